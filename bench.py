@@ -1,0 +1,353 @@
+#!/usr/bin/env python
+"""Benchmark of the semi-naive transitive-closure fixpoint on B200.
+
+Workload: the TC program ``path(x, y) :- edge(x, y). path(x, z) :- path(x, y),
+edge(y, z).`` on a seeded subcritical directed Erdos-Renyi graph with
+16,777,216 nodes and 14,680,064 edges (mean out-degree 0.875), run to its
+fixpoint through the device-resident RelationStore / RecursiveExecutor.
+
+Metric: derived TC tuples per second, i.e. the executor's total_new_rows
+(|FULL at the fixpoint| - |seed|) divided by the time of the fixpoint.
+
+* ``value``: inputs already resident in HBM; one step = fresh store from the
+  device-resident edges + compile + run to the fixpoint; K steps timed with
+  CUDA events, barrier + synchronize on both sides, max over ranks.
+* ``e2e``: the same through the public API from pinned host buffers: every
+  step uploads the edges (static EDB and seed), runs, and reads FULL back.
+* ``roofline``: the dominant kernel class of one profiled step (CUDA events
+  on the executor's stream around every kernel class, algorithmic bytes =
+  each input row read once and each output row written once).
+* ``cpu_baseline``: the oracle's restatement of the reference's parallel CPU
+  operators (run_with_stream(None) with the *_cpu_parallel operators) on a
+  bounded sample: the first rounds of the same fixpoint.
+
+Multi-GPU (torchrun): ranks split the nodes into contiguous x ranges; each
+rank closes the paths starting in its range against the replicated EDB. The
+join output keeps x, so every operator stays partition-local and no data
+crosses ranks; a final all-reduce combines iteration counts (max) and new
+rows (sum). ``--impl reference`` times the CPU oracle alone (rank 0).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    # name: (nodes, edges, seed)
+    "er_16m_14_68m": (16_777_216, 14_680_064, 2),
+    "er_2000_8000": (2_000, 8_000, 1),
+}
+# Rounds of the fixpoint run by one CPU-baseline sample.
+CPU_SAMPLE_ROUNDS = {"er_16m_14_68m": 4, "er_2000_8000": 13}
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--workload", choices=sorted(WORKLOADS), default="er_16m_14_68m")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def measured_peaks():
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        d = json.loads(f.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def partition(src, dst, nodes, rank, world):
+    """Seed rows whose x lies in this rank's contiguous node range."""
+    lo = nodes * rank // world
+    hi = nodes * (rank + 1) // world
+    a = np.searchsorted(src, lo, side="left")
+    b = np.searchsorted(src, hi, side="left")
+    return src[a:b], dst[a:b]
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
+                 "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        self.file.flush()
+        rows = []
+        for line in Path(self.file.name).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1].split()[0]), float(parts[2].split()[0]), parts[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v == "Active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(workload, edges_cols=None, threads=None):
+    """Times the oracle's parallel CPU pipeline on the first rounds of the fixpoint."""
+    import oracle
+    from sparkalog_b200 import generators
+
+    nodes, edges, seed = WORKLOADS[workload]
+    rounds = CPU_SAMPLE_ROUNDS[workload]
+    src, dst = edges_cols if edges_cols is not None else generators.er_edges(nodes, edges, seed)
+    cores = threads or os.cpu_count() or 1
+    st = oracle.Store()
+    st.insert_static(0, (src, dst))
+    st.insert_recursive(1, (src, dst), (src, dst))
+    t0 = time.perf_counter()
+    it, new, _ = st.run_scc_bounded([1], [oracle.tc_rule(1, 0)], rounds, cores)
+    dt = time.perf_counter() - t0
+    return {"value": new / dt, "unit": "tuples/s", "cores": cores, "kind": "port",
+            "sample": f"first {it} rounds of the same fixpoint ({new} derived tuples in {dt:.2f} s); "
+                      f"restatement of the reference's *_cpu_parallel operators inside RecursiveExecutor::run"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from sparkalog_b200 import generators
+
+    nodes, edges, seed = WORKLOADS[args.workload]
+    cols = generators.er_edges(nodes, edges, seed)
+    samples = []
+    base = None
+    for i in range(args.warmup + args.steps):
+        b = cpu_baseline(args.workload, cols)
+        if i >= args.warmup:
+            samples.append(b["value"])
+            base = b
+    value = statistics.median(samples)
+    nodes, edges, _ = WORKLOADS[args.workload]
+    line = {
+        "impl": "reference", "metric": "TC derived tuples/s", "value": value, "unit": "tuples/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded ER)",
+        "config": {"workload": args.workload, "nodes": nodes, "edges": edges},
+        "cpu_baseline": {"value": value, "unit": "tuples/s", "cores": base["cores"], "kind": base["kind"],
+                         "sample": base["sample"]},
+        "e2e": {"value": value, "unit": "tuples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    from sparkalog_b200 import generators
+    from sparkalog_b200.recursion import DELTA, FULL, RecursiveExecutor, RelationStore, transitive_closure_scc
+    from sparkalog_b200.relational import RelationId
+
+    nodes, edges, seed = WORKLOADS[args.workload]
+    src, dst = generators.er_edges(nodes, edges, seed)
+    ps, pd = partition(src, dst, nodes, rank, world)
+    stream = torch.cuda.current_stream()
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).cuda()
+    e0, e1, s0, s1 = dev(src), dev(dst), dev(ps), dev(pd)
+    path, edge = RelationId(1), RelationId(0)
+    plan = transitive_closure_scc(path, edge)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def step(profile=False):
+        store = RelationStore(stream)
+        store.insert_static(0, (e0, e1))
+        store.insert_recursive(1, (s0, s1), (s0, s1))
+        ex = RecursiveExecutor.compile(plan, store)
+        if profile:
+            ex.set_profiling(True)
+        summary = ex.run(store)
+        stats = ex.stats()
+        ex.close()
+        store.close()
+        return summary, stats
+
+    for _ in range(args.warmup):
+        summary, _ = step()
+
+    timer_start = torch.cuda.Event(enable_timing=True)
+    timer_end = torch.cuda.Event(enable_timing=True)
+    launches = 0
+    with ClockSampler(local_rank) as clocks:
+        barrier()
+        timer_start.record(stream)
+        for _ in range(args.steps):
+            summary, stats = step()
+            launches += stats["total_launches"]
+        timer_end.record(stream)
+        barrier()
+    ms = timer_start.elapsed_time(timer_end)
+    local = [ms, float(summary.total_new_rows), float(summary.iterations)]
+    if dist is not None:
+        t = torch.tensor(local, dtype=torch.float64, device="cuda")
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = t.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        ms, iterations, new_rows = float(mx[0]), int(mx[2]), int(sm[1])
+    else:
+        new_rows, iterations = int(local[1]), int(local[2])
+    value = new_rows * args.steps / (ms / 1e3)
+
+    # Roofline: one profiled step right after the timed ones.
+    _, pstats = step(profile=True)
+    classes = pstats["classes"]
+    dominant = max(classes, key=lambda k: classes[k]["ms"])
+    dom = classes[dominant]
+    peak, peak_kind = measured_peaks()
+    per_launch_ms = dom["ms"] / max(dom["launches"], 1)
+    per_launch_bytes = dom["bytes"] / max(dom["launches"], 1)
+    achieved = per_launch_bytes / (per_launch_ms / 1e3) / 1e9 if per_launch_ms > 0 else 0.0
+
+    # End to end through the public API: pinned host buffers, H2D + run + D2H.
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    h_src, h_dst, h_ps, h_pd = pin(src), pin(dst), pin(ps), pin(pd)
+    full_rows = None
+    out0 = out1 = None
+    e2e_ms = []
+    for i in range(2 + args.steps):
+        barrier()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        store = RelationStore(stream)
+        store.insert_static(0, (h_src, h_dst))
+        store.insert_recursive(1, (h_ps, h_pd), (h_ps, h_pd))
+        ex = RecursiveExecutor.compile(plan, store)
+        ex.run(store)
+        n = store.rows(1, FULL)
+        if out0 is None or len(out0) < n:
+            out0 = torch.empty(n, dtype=torch.int32).pin_memory()
+            out1 = torch.empty(n, dtype=torch.int32).pin_memory()
+        store.read_into(1, FULL, out0, out1)
+        b.record(stream)
+        barrier()
+        ex.close()
+        store.close()
+        full_rows = n
+        if i >= 2:
+            e2e_ms.append(a.elapsed_time(b))
+    e2e_local = statistics.median(e2e_ms)
+    if dist is not None:
+        t = torch.tensor([e2e_local], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_local = float(t[0])
+    e2e_value = new_rows / (e2e_local / 1e3)
+    h2d = (len(h_src) + 2 * len(h_ps)) * 8
+    d2h = full_rows * 8
+
+    clock = clocks.summary()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.workload, (src, dst))
+    if rank == 0:
+        line = {
+            "metric": "TC derived tuples/s",
+            "value": value,
+            "unit": "tuples/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "strong",
+            "vs_baseline": None,
+            "dtype": "u32",
+            "data": "synthetic (seeded ER, splitmix64)",
+            "config": {"workload": args.workload, "nodes": nodes, "edges": edges, "seed": seed,
+                       "derived_tuples": new_rows, "iterations": iterations,
+                       "parallelism": f"x-range partition x{world}" if world > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (FULL ~1 GB, candidates ~100 MB per round)"},
+            "e2e": {"value": e2e_value, "unit": "tuples/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": e2e_local},
+            "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved / 1.0, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "peak_kind": peak_kind,
+                         "per_launch_ms": per_launch_ms, "per_launch_algorithmic_bytes": per_launch_bytes,
+                         "classes": {k: {"ms": v["ms"], "launches": v["launches"],
+                                         "gbs": (v["bytes"] / (v["ms"] / 1e3) / 1e9) if v["ms"] > 0 else 0.0}
+                                     for k, v in classes.items()}},
+            "gpu_launches": launches,
+            "clocks": clock,
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

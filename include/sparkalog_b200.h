@@ -1,0 +1,231 @@
+/*
+ * sparkalog_b200 — B200-native (sm_100a) binary recursive operator pipeline.
+ *
+ * C ABI of libsparkalog_b200.so. Plain pointers and sizes only.
+ *
+ * Tier A: the reference's own FFI for the pipeline's operators, with the same
+ * names, signatures, argument meaning, null-pointer checks and empty-input
+ * behaviour as the launchers in crates/sparkalog-execution/native/column_ops.cu
+ * (bound from Rust at crates/sparkalog-execution/src/lib.rs:28-169). A build of
+ * the reference links this library in place of its libsparkalog_cuda.a.
+ * Return values are cudaError_t codes (0 = success); counts are written to
+ * device (or managed) memory asynchronously on `stream`.
+ *
+ * Tier B: a device-resident RelationStore / RecursiveExecutor
+ * (crates/sparkalog-recursion/src/generic.rs:16-525) that keeps FULL, DELTA
+ * and NEWT on the device as packed 64-bit rows and runs the whole semi-naive
+ * loop without copying relations back to the host. Return values are 0 on
+ * success, a positive cudaError_t, or a negative SPARKALOG_E_* code;
+ * sparkalog_last_error() describes the last failure of the calling thread.
+ */
+#ifndef SPARKALOG_B200_H
+#define SPARKALOG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define SPARKALOG_API __attribute__((visibility("default")))
+#else
+#define SPARKALOG_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Tier A: reference-compatible operator entry points                        */
+/* ------------------------------------------------------------------------ */
+
+/* column_ops.cu:248-250; lib.rs:32. */
+SPARKALOG_API int sparkalog_stream_synchronize(void* stream);
+
+/* Scratch size for the join's count stage. column_ops.cu:339-355; lib.rs:59-65. */
+SPARKALOG_API int sparkalog_join_u32_temporary_bytes(const uint64_t* counts, uint64_t* offsets, size_t left_rows,
+                                                     size_t* temporary_bytes, void* stream);
+
+/* Per left row match counts, their exclusive scan and the total.
+ * column_ops.cu:357-401; lib.rs:66-78. */
+SPARKALOG_API int sparkalog_join_u32_count(const uint32_t* left_keys, size_t left_rows, const uint32_t* index_keys,
+                                           const uint32_t* index_starts, size_t unique_keys, uint64_t* counts,
+                                           uint64_t* offsets, uint64_t* total, void* temporary,
+                                           size_t temporary_bytes, void* stream);
+
+/* Projected join output, left-row-major, matches in index order.
+ * A side value of 0 selects the left row, 1 the right row.
+ * column_ops.cu:403-444; lib.rs:79-94. */
+SPARKALOG_API int sparkalog_join_u32_emit(const uint32_t* left_keys, size_t left_rows, const uint32_t* index_keys,
+                                          const uint32_t* index_starts, const uint32_t* index_rows,
+                                          size_t unique_keys, const uint32_t* projection0,
+                                          uint32_t projection0_side, const uint32_t* projection1,
+                                          uint32_t projection1_side, const uint64_t* offsets, uint32_t* output0,
+                                          uint32_t* output1, void* stream);
+
+/* column_ops.cu:446-487; lib.rs:95-102. */
+SPARKALOG_API int sparkalog_distinct_u32_temporary_bytes(uint64_t* packed, uint64_t* scratch, uint64_t* unique_rows,
+                                                         size_t rows, size_t* temporary_bytes, void* stream);
+
+/* Sort and deduplicate (first, second) pairs; sorted unique output and its
+ * u64 count. `packed`/`scratch` (rows u64 each) are the sort's buffers.
+ * column_ops.cu:489-549; lib.rs:103-115. */
+SPARKALOG_API int sparkalog_distinct_u32(const uint32_t* first, const uint32_t* second, size_t rows,
+                                         uint64_t* packed, uint64_t* scratch, uint64_t* unique_rows,
+                                         uint32_t* output_first, uint32_t* output_second, void* temporary,
+                                         size_t temporary_bytes, void* stream);
+
+/* column_ops.cu:551-574; lib.rs:116-123. */
+SPARKALOG_API int sparkalog_anti_join_u32_temporary_bytes(const uint32_t* flags, uint32_t* selected,
+                                                          uint32_t* selected_rows, size_t left_rows,
+                                                          size_t* temporary_bytes, void* stream);
+
+/* Stable left - right over lexicographically sorted pairs. flags[row] = 1 for
+ * kept rows, selected[] = kept row ids, *selected_rows = u32 count.
+ * column_ops.cu:576-641; lib.rs:124-139. */
+SPARKALOG_API int sparkalog_anti_join_u32(const uint32_t* left_first, const uint32_t* left_second, size_t left_rows,
+                                          const uint32_t* right_first, const uint32_t* right_second,
+                                          size_t right_rows, uint32_t* flags, uint32_t* selected,
+                                          uint32_t* selected_rows, uint32_t* output_first, uint32_t* output_second,
+                                          void* temporary, size_t temporary_bytes, void* stream);
+
+/* column_ops.cu:643-690; lib.rs:140-150. */
+SPARKALOG_API int sparkalog_union_u32_temporary_bytes(const uint64_t* left, size_t left_rows, const uint64_t* right,
+                                                      size_t right_rows, uint64_t* merged, uint64_t* unique,
+                                                      uint64_t* unique_rows, size_t* temporary_bytes, void* stream);
+
+/* Merge two sorted pair lists and deduplicate; sorted output and u64 count.
+ * column_ops.cu:692-775; lib.rs:151-168. */
+SPARKALOG_API int sparkalog_union_u32(const uint32_t* left_first, const uint32_t* left_second, size_t left_rows,
+                                      const uint32_t* right_first, const uint32_t* right_second, size_t right_rows,
+                                      uint64_t* left, uint64_t* right, uint64_t* merged, uint64_t* unique,
+                                      uint64_t* unique_rows, uint32_t* output_first, uint32_t* output_second,
+                                      void* temporary, size_t temporary_bytes, void* stream);
+
+/* Asynchronous error bits of this device's Tier A kernels (a decoupled
+ * look-back that hit its spin cap). No counterpart in the reference, whose
+ * CUB kernels have no such wait. reset != 0 clears the bits. */
+SPARKALOG_API int sparkalog_b200_device_error(uint32_t* bits, int reset);
+
+/* ------------------------------------------------------------------------ */
+/* Tier B: device-resident store and executor                                */
+/* ------------------------------------------------------------------------ */
+
+enum {
+    SPARKALOG_E_MISSING = -1,              /* RelationStoreError::Missing */
+    SPARKALOG_E_DUPLICATE = -2,            /* RelationStoreError::Duplicate */
+    SPARKALOG_E_NOT_RECURSIVE = -3,        /* RelationStoreError::NotRecursive */
+    SPARKALOG_E_EMPTY_SCC = -4,            /* GenericExecutionError::EmptyScc */
+    SPARKALOG_E_DUPLICATE_SCC_RELATION = -5,
+    SPARKALOG_E_DELTA_OUTSIDE_SCC = -6,
+    SPARKALOG_E_TARGET_OUTSIDE_SCC = -7,
+    SPARKALOG_E_INCOMPATIBLE_TARGET_PLANS = -8,
+    SPARKALOG_E_MISSING_RULE_TARGET = -9,
+    SPARKALOG_E_ITERATION_LIMIT = -10,
+    SPARKALOG_E_TOO_MANY_ROWS = -11,       /* execution::Error::TooManyRows */
+    SPARKALOG_E_MISSING_COLUMN = -12,      /* MissingPlanColumn / MissingColumn */
+    SPARKALOG_E_DEVICE_FAULT = -20,        /* a kernel reported an error bit */
+    SPARKALOG_E_INVALID_ARGUMENT = -21,
+    SPARKALOG_E_UNSORTED_FULL = -22,       /* FULL must be sorted for anti-join/union */
+};
+
+/* JoinInput: 0 = Left (the DELTA side), 1 = Right. */
+typedef struct sparkalog_rule_plan {
+    uint32_t target;          /* RecursiveRulePlan::target, relational/src/lib.rs:74-82 */
+    uint32_t delta_input;
+    uint32_t right_input;
+    uint32_t left_key;        /* BinaryEqualityJoin, relational/src/lib.rs:46-50 */
+    uint32_t right_key;
+    uint32_t proj_side[2];
+    uint32_t proj_col[2];
+    uint32_t distinct_cols[2];   /* BinaryDistinct */
+    uint32_t anti_left[2];       /* SortedBinaryAntiJoin */
+    uint32_t anti_right[2];
+    uint32_t union_left[2];      /* SortedBinaryUnion */
+    uint32_t union_right[2];
+} sparkalog_rule_plan;
+
+/* SccSummary, recursion/src/generic.rs:536-542 (placements omitted: every
+ * operator runs on the GPU). relation_rows has one entry per SCC relation, in
+ * plan order; the caller provides room for relation_count entries. */
+typedef struct sparkalog_scc_summary {
+    uint64_t iterations;
+    uint64_t total_new_rows;
+    uint64_t relation_count;
+    uint32_t* relation_ids;
+    uint64_t* relation_rows;
+} sparkalog_scc_summary;
+
+typedef struct sparkalog_store sparkalog_store;
+typedef struct sparkalog_executor sparkalog_executor;
+
+/* Location of caller buffers: host memory (pageable or pinned) or device. */
+enum { SPARKALOG_HOST = 0, SPARKALOG_DEVICE = 1 };
+/* Relation versions, RelationVersion (relational/src/lib.rs:10-14). */
+enum { SPARKALOG_FULL = 0, SPARKALOG_DELTA = 1 };
+
+/* RelationStore::new, generic.rs:29-34. Work runs on `stream` (0 = legacy). */
+SPARKALOG_API int sparkalog_store_create(void* stream, sparkalog_store** out);
+SPARKALOG_API void sparkalog_store_destroy(sparkalog_store* store);
+
+/* RelationStore::insert_static, generic.rs:36-51. */
+SPARKALOG_API int sparkalog_store_insert_static(sparkalog_store* store, uint32_t id, const uint32_t* first,
+                                                const uint32_t* second, size_t rows, int location);
+
+/* RelationStore::insert_recursive, generic.rs:53-79. */
+SPARKALOG_API int sparkalog_store_insert_recursive(sparkalog_store* store, uint32_t id, const uint32_t* full_first,
+                                                   const uint32_t* full_second, size_t full_rows,
+                                                   const uint32_t* delta_first, const uint32_t* delta_second,
+                                                   size_t delta_rows, int location);
+
+/* Row count of FULL or DELTA (RelationStore::full/delta, generic.rs:81-92). */
+SPARKALOG_API int sparkalog_store_rows(sparkalog_store* store, uint32_t id, int version, size_t* rows);
+
+/* Copies FULL or DELTA out as two u32 columns (sorted for FULL of recursive
+ * relations after a run, as the reference's RelationBuffer is). */
+SPARKALOG_API int sparkalog_store_read(sparkalog_store* store, uint32_t id, int version, uint32_t* first,
+                                       uint32_t* second, int location);
+
+/* RecursiveExecutor::compile, generic.rs:407-470. */
+SPARKALOG_API int sparkalog_executor_compile(sparkalog_store* store, const uint32_t* relations,
+                                             size_t relation_count, const sparkalog_rule_plan* rules,
+                                             size_t rule_count, sparkalog_executor** out);
+SPARKALOG_API void sparkalog_executor_destroy(sparkalog_executor* executor);
+
+/* RecursiveExecutor::run, generic.rs:472-516. */
+SPARKALOG_API int sparkalog_executor_run(sparkalog_executor* executor, sparkalog_store* store,
+                                         size_t max_iterations, sparkalog_scc_summary* summary);
+
+/* Per-kernel-class statistics of an executor, measured with CUDA events on
+ * the executor's stream while profiling is enabled. No counterpart in the
+ * reference (which has no tracing); used to report achieved HBM bandwidth.
+ * bytes[] are algorithmic bytes: each input row read once, each output row
+ * written once (8 bytes per packed pair). launches[] counts every kernel of
+ * the class; total_launches counts every kernel the executor launched. */
+enum {
+    SPARKALOG_K_JOIN = 0,        /* fused count/scan/emit join */
+    SPARKALOG_K_SORT_HIST = 1,   /* radix histogram + plan */
+    SPARKALOG_K_SORT_PASS = 2,   /* radix scatter passes (active ones) */
+    SPARKALOG_K_ANTI_JOIN = 3,   /* unique + anti-join against the FULL levels */
+    SPARKALOG_K_MERGE = 4,       /* merge of NEWT / levels */
+    SPARKALOG_K_INDEX = 5,       /* right-relation index build */
+    SPARKALOG_K_CLASSES = 8
+};
+typedef struct sparkalog_kernel_stats {
+    uint64_t launches[SPARKALOG_K_CLASSES];
+    double milliseconds[SPARKALOG_K_CLASSES];
+    double bytes[SPARKALOG_K_CLASSES];
+    uint64_t total_launches;
+    uint64_t rounds;
+} sparkalog_kernel_stats;
+
+SPARKALOG_API int sparkalog_executor_set_profiling(sparkalog_executor* executor, int enable);
+SPARKALOG_API int sparkalog_executor_stats(sparkalog_executor* executor, sparkalog_kernel_stats* out, int reset);
+
+/* Thread-local description of the last failure. */
+SPARKALOG_API const char* sparkalog_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPARKALOG_B200_H */

@@ -1,0 +1,161 @@
+"""ctypes bindings of ``lib/libsparkalog_b200.so`` (declared in include/sparkalog_b200.h).
+
+The library is the product: every operator and the fixpoint loop run in it on
+the GPU. There is no CPU fallback; importing this module without the built
+library raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libsparkalog_b200.so"
+
+c_u32p = ctypes.POINTER(ctypes.c_uint32)
+c_u64p = ctypes.POINTER(ctypes.c_uint64)
+c_sizep = ctypes.POINTER(ctypes.c_size_t)
+vp = ctypes.c_void_p
+
+# Symbols of include/sparkalog_b200.h, in declaration order.
+TIER_A = [
+    "sparkalog_stream_synchronize",
+    "sparkalog_join_u32_temporary_bytes",
+    "sparkalog_join_u32_count",
+    "sparkalog_join_u32_emit",
+    "sparkalog_distinct_u32_temporary_bytes",
+    "sparkalog_distinct_u32",
+    "sparkalog_anti_join_u32_temporary_bytes",
+    "sparkalog_anti_join_u32",
+    "sparkalog_union_u32_temporary_bytes",
+    "sparkalog_union_u32",
+    "sparkalog_b200_device_error",
+]
+TIER_B = [
+    "sparkalog_store_create",
+    "sparkalog_store_destroy",
+    "sparkalog_store_insert_static",
+    "sparkalog_store_insert_recursive",
+    "sparkalog_store_rows",
+    "sparkalog_store_read",
+    "sparkalog_executor_compile",
+    "sparkalog_executor_destroy",
+    "sparkalog_executor_run",
+    "sparkalog_executor_set_profiling",
+    "sparkalog_executor_stats",
+    "sparkalog_last_error",
+]
+EXPORTED = TIER_A + TIER_B
+
+
+class RulePlanC(ctypes.Structure):
+    """sparkalog_rule_plan."""
+
+    _fields_ = [
+        ("target", ctypes.c_uint32),
+        ("delta_input", ctypes.c_uint32),
+        ("right_input", ctypes.c_uint32),
+        ("left_key", ctypes.c_uint32),
+        ("right_key", ctypes.c_uint32),
+        ("proj_side", ctypes.c_uint32 * 2),
+        ("proj_col", ctypes.c_uint32 * 2),
+        ("distinct_cols", ctypes.c_uint32 * 2),
+        ("anti_left", ctypes.c_uint32 * 2),
+        ("anti_right", ctypes.c_uint32 * 2),
+        ("union_left", ctypes.c_uint32 * 2),
+        ("union_right", ctypes.c_uint32 * 2),
+    ]
+
+
+class SccSummaryC(ctypes.Structure):
+    """sparkalog_scc_summary."""
+
+    _fields_ = [
+        ("iterations", ctypes.c_uint64),
+        ("total_new_rows", ctypes.c_uint64),
+        ("relation_count", ctypes.c_uint64),
+        ("relation_ids", c_u32p),
+        ("relation_rows", c_u64p),
+    ]
+
+
+KERNEL_CLASSES = ["join", "sort_histogram", "sort_pass", "anti_join", "merge", "index"]
+
+
+class KernelStatsC(ctypes.Structure):
+    """sparkalog_kernel_stats."""
+
+    _fields_ = [
+        ("launches", ctypes.c_uint64 * 8),
+        ("milliseconds", ctypes.c_double * 8),
+        ("bytes", ctypes.c_double * 8),
+        ("total_launches", ctypes.c_uint64),
+        ("rounds", ctypes.c_uint64),
+    ]
+
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Loads the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -m sparkalog_b200.build` "
+            "(sparkalog_b200 has no CPU fallback)")
+    L = ctypes.CDLL(str(LIB_PATH))
+    i = ctypes.c_int
+    L.sparkalog_stream_synchronize.argtypes = [vp]
+    L.sparkalog_join_u32_temporary_bytes.argtypes = [vp, vp, ctypes.c_size_t, c_sizep, vp]
+    L.sparkalog_join_u32_count.argtypes = [vp, ctypes.c_size_t, vp, vp, ctypes.c_size_t, vp, vp, vp, vp,
+                                           ctypes.c_size_t, vp]
+    L.sparkalog_join_u32_emit.argtypes = [vp, ctypes.c_size_t, vp, vp, vp, ctypes.c_size_t, vp, ctypes.c_uint32,
+                                          vp, ctypes.c_uint32, vp, vp, vp, vp]
+    L.sparkalog_distinct_u32_temporary_bytes.argtypes = [vp, vp, vp, ctypes.c_size_t, c_sizep, vp]
+    L.sparkalog_distinct_u32.argtypes = [vp, vp, ctypes.c_size_t, vp, vp, vp, vp, vp, vp, ctypes.c_size_t, vp]
+    L.sparkalog_anti_join_u32_temporary_bytes.argtypes = [vp, vp, vp, ctypes.c_size_t, c_sizep, vp]
+    L.sparkalog_anti_join_u32.argtypes = [vp, vp, ctypes.c_size_t, vp, vp, ctypes.c_size_t, vp, vp, vp, vp, vp, vp,
+                                          ctypes.c_size_t, vp]
+    L.sparkalog_union_u32_temporary_bytes.argtypes = [vp, ctypes.c_size_t, vp, ctypes.c_size_t, vp, vp, vp, c_sizep,
+                                                      vp]
+    L.sparkalog_union_u32.argtypes = [vp, vp, ctypes.c_size_t, vp, vp, ctypes.c_size_t, vp, vp, vp, vp, vp, vp, vp,
+                                      vp, ctypes.c_size_t, vp]
+    L.sparkalog_b200_device_error.argtypes = [c_u32p, i]
+    for name in TIER_A:
+        getattr(L, name).restype = i
+    L.sparkalog_store_create.argtypes = [vp, ctypes.POINTER(vp)]
+    L.sparkalog_store_create.restype = i
+    L.sparkalog_store_destroy.argtypes = [vp]
+    L.sparkalog_store_destroy.restype = None
+    L.sparkalog_store_insert_static.argtypes = [vp, ctypes.c_uint32, vp, vp, ctypes.c_size_t, i]
+    L.sparkalog_store_insert_static.restype = i
+    L.sparkalog_store_insert_recursive.argtypes = [vp, ctypes.c_uint32, vp, vp, ctypes.c_size_t, vp, vp,
+                                                   ctypes.c_size_t, i]
+    L.sparkalog_store_insert_recursive.restype = i
+    L.sparkalog_store_rows.argtypes = [vp, ctypes.c_uint32, i, c_sizep]
+    L.sparkalog_store_rows.restype = i
+    L.sparkalog_store_read.argtypes = [vp, ctypes.c_uint32, i, vp, vp, i]
+    L.sparkalog_store_read.restype = i
+    L.sparkalog_executor_compile.argtypes = [vp, c_u32p, ctypes.c_size_t, ctypes.POINTER(RulePlanC), ctypes.c_size_t,
+                                             ctypes.POINTER(vp)]
+    L.sparkalog_executor_compile.restype = i
+    L.sparkalog_executor_destroy.argtypes = [vp]
+    L.sparkalog_executor_destroy.restype = None
+    L.sparkalog_executor_run.argtypes = [vp, vp, ctypes.c_size_t, ctypes.POINTER(SccSummaryC)]
+    L.sparkalog_executor_run.restype = i
+    L.sparkalog_executor_set_profiling.argtypes = [vp, i]
+    L.sparkalog_executor_set_profiling.restype = i
+    L.sparkalog_executor_stats.argtypes = [vp, ctypes.POINTER(KernelStatsC), i]
+    L.sparkalog_executor_stats.restype = i
+    L.sparkalog_last_error.argtypes = []
+    L.sparkalog_last_error.restype = ctypes.c_char_p
+    _lib = L
+    return L
+
+
+def last_error() -> str:
+    msg = load().sparkalog_last_error()
+    return msg.decode() if msg else ""

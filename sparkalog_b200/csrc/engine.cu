@@ -1,0 +1,1038 @@
+// Device-resident RelationStore / RecursiveExecutor (the Tier B C ABI).
+//
+// Semantics follow crates/sparkalog-recursion/src/generic.rs:
+//   RelationStore            :16-121   (FULL / DELTA / NEWT per relation)
+//   RuleRuntime::evaluate    :197-259  (cached right index, join, distinct)
+//   TargetRuntime::combine   :299-358  (union of clause outputs, anti-join)
+//   TargetRuntime::apply     :360-397  (FULL u= NEWT, DELTA <- NEWT)
+//   RecursiveExecutor::run   :472-525  (loop while any DELTA is non-empty,
+//                                       counting every executed round)
+//
+// B200 layout: every relation lives on the device as packed 64-bit rows
+// (first << 32 | second), so lexicographic pair order is u64 order. One round
+// of the loop is a fixed sequence of kernels on one stream:
+//   join (fused count/scan/emit)  ->  radix sort of the candidates
+//   ->  unique + anti-join against the FULL levels (one fused pass)  ->  NEWT
+//   ->  merge NEWT into the levels  ->  DELTA <- NEWT
+// with one small device-to-host copy of the round's counts per round.
+//
+// Clause outputs of one target are appended into one candidate buffer and
+// sorted once: unique(A ++ B) equals the reference's union of the two
+// distinct outputs (generic.rs:317-336).
+
+#include "sparkalog_b200.h"
+#include "spk_common.cuh"
+#include "spk_engine_kernels.cuh"
+#include "spk_host.h"
+#include "spk_join.cuh"
+#include "spk_radix.cuh"
+#include "spk_setops.cuh"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+using spk::u32;
+using spk::u64;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& message) {
+    g_last_error = message;
+    return code;
+}
+
+int cuda_fail(cudaError_t st, const char* what) {
+    g_last_error = std::string(what) + " failed with CUDA error " + std::to_string(static_cast<int>(st)) + " (" +
+                   cudaGetErrorString(st) + ")";
+    return static_cast<int>(st);
+}
+
+#define SPK_CUDA(expr, what)                         \
+    do {                                             \
+        cudaError_t _st = (expr);                    \
+        if (_st != cudaSuccess) return cuda_fail(_st, what); \
+    } while (0)
+
+constexpr int kThreads = 256;
+constexpr int kSetItems = 8;
+constexpr int kSetTile = kThreads * kSetItems;
+constexpr int kJoinItems = 8;
+constexpr int kJoinTile = kThreads * kJoinItems;
+constexpr int kMergeItems = 8;
+constexpr int kMergeTile = kThreads * kMergeItems;
+constexpr int kSortThreads = spk::RadixSortConfig::kThreads;
+constexpr int kSortItems = spk::RadixSortConfig::kItems;
+constexpr int kSortTile = spk::RadixSortConfig::kTile;
+// A level is merged into the next larger one once it holds more than
+// 1/kLevelRatio of that level's rows.
+constexpr u64 kLevelRatio = 4;
+
+// A stream-ordered device allocation that only grows.
+struct DevArray {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+
+    template <class T>
+    T* as() const { return static_cast<T*>(ptr); }
+
+    // Grows to at least `need` bytes. With keep_bytes > 0 the first keep_bytes
+    // bytes are preserved.
+    cudaError_t ensure(size_t need, cudaStream_t s, size_t keep_bytes = 0) {
+        if (need <= bytes && ptr) return cudaSuccess;
+        size_t cap = std::max<size_t>(need, 4096);
+        cap = std::max(cap, bytes + bytes / 2);
+        cap = spk::align_up(cap, 256);
+        void* fresh = nullptr;
+        cudaError_t st = cudaMallocAsync(&fresh, cap, s);
+        if (st != cudaSuccess) return st;
+        if (keep_bytes && ptr) {
+            st = cudaMemcpyAsync(fresh, ptr, std::min(keep_bytes, bytes), cudaMemcpyDeviceToDevice, s);
+            if (st != cudaSuccess) return st;
+        }
+        if (ptr) cudaFreeAsync(ptr, s);
+        ptr = fresh;
+        bytes = cap;
+        return cudaSuccess;
+    }
+
+    void release(cudaStream_t s) {
+        if (ptr) cudaFreeAsync(ptr, s);
+        ptr = nullptr;
+        bytes = 0;
+    }
+};
+
+void swap_arrays(DevArray& a, DevArray& b) {
+    std::swap(a.ptr, b.ptr);
+    std::swap(a.bytes, b.bytes);
+}
+
+struct RelState {
+    bool recursive = false;
+    u64 version = 0;
+    bool sorted = true;     // level[0] as inserted is non-decreasing
+    bool has_dups = false;  // level[0] as inserted has adjacent duplicates
+    DevArray level[spk::kMaxLevels];
+    u64 level_n[spk::kMaxLevels] = {0, 0, 0};
+    DevArray spare;         // merge destination, swapped with a level after a merge
+    DevArray delta, newt;
+    u64 delta_n = 0;
+
+    u64 full_rows() const {
+        u64 n = 0;
+        for (int l = 0; l < spk::kMaxLevels; ++l) n += level_n[l];
+        return n;
+    }
+};
+
+}  // namespace
+
+struct sparkalog_store {
+    cudaStream_t stream = nullptr;
+    std::map<u32, RelState> relations;
+    DevArray scratch_u32[2];   // staging columns for host inserts / reads
+    DevArray flags;            // device flag words
+    u32* pinned = nullptr;     // small pinned host buffer
+
+    RelState* find(u32 id) {
+        auto it = relations.find(id);
+        return it == relations.end() ? nullptr : &it->second;
+    }
+};
+
+namespace {
+
+unsigned grid_for(const void* kernel, int threads, size_t tiles) {
+    return spk::persistent_grid(kernel, threads, 0, tiles);
+}
+
+unsigned simple_grid(size_t n) {
+    size_t blocks = (n + 255) / 256;
+    size_t cap = static_cast<size_t>(spk::device_sm_count()) * 8;
+    return static_cast<unsigned>(std::max<size_t>(1, std::min(blocks, cap)));
+}
+
+// Merge of two disjoint sorted runs into `out` (capacity checked by caller).
+cudaError_t launch_merge(const u64* a, u64 na, const u64* b, u64 nb, u64* out, cudaStream_t s) {
+    const u64 total = na + nb;
+    if (total == 0) return cudaSuccess;
+    if (nb == 0) return cudaMemcpyAsync(out, a, na * 8, cudaMemcpyDeviceToDevice, s);
+    if (na == 0) return cudaMemcpyAsync(out, b, nb * 8, cudaMemcpyDeviceToDevice, s);
+    auto kernel = spk::merge_disjoint_kernel<kThreads, kMergeItems>;
+    const size_t tiles = (total + kMergeTile - 1) / kMergeTile;
+    kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, tiles), kThreads, 0, s>>>(a, na, b, nb, out);
+    return cudaGetLastError();
+}
+
+// Collapses all levels of a relation into level[0] (a single sorted run).
+int materialize(RelState& r, cudaStream_t s) {
+    for (int l = 1; l < spk::kMaxLevels; ++l) {
+        if (r.level_n[l] == 0) continue;
+        const u64 total = r.level_n[0] + r.level_n[l];
+        SPK_CUDA(r.spare.ensure(total * 8, s), "cudaMallocAsync");
+        SPK_CUDA(launch_merge(r.level[0].as<u64>(), r.level_n[0], r.level[l].as<u64>(), r.level_n[l],
+                              r.spare.as<u64>(), s),
+                 "merge_disjoint_kernel");
+        swap_arrays(r.level[0], r.spare);
+        r.level_n[0] = total;
+        r.level_n[l] = 0;
+    }
+    return 0;
+}
+
+// Uploads (or adopts device) columns and packs them into `dst`.
+int pack_columns(sparkalog_store* st, const u32* c0, const u32* c1, size_t rows, int location, DevArray& dst,
+                 bool* sorted, bool* has_dups) {
+    cudaStream_t s = st->stream;
+    *sorted = true;
+    *has_dups = false;
+    SPK_CUDA(dst.ensure(std::max<size_t>(rows, 1) * 8, s), "cudaMallocAsync");
+    if (rows == 0) return 0;
+    if (c0 == nullptr || c1 == nullptr) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null column pointer");
+    const u32* d0 = c0;
+    const u32* d1 = c1;
+    if (location == SPARKALOG_HOST) {
+        SPK_CUDA(st->scratch_u32[0].ensure(rows * 4, s), "cudaMallocAsync");
+        SPK_CUDA(st->scratch_u32[1].ensure(rows * 4, s), "cudaMallocAsync");
+        SPK_CUDA(cudaMemcpyAsync(st->scratch_u32[0].ptr, c0, rows * 4, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
+        SPK_CUDA(cudaMemcpyAsync(st->scratch_u32[1].ptr, c1, rows * 4, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
+        d0 = st->scratch_u32[0].as<u32>();
+        d1 = st->scratch_u32[1].as<u32>();
+    }
+    u32* flags = st->flags.as<u32>();
+    SPK_CUDA(cudaMemsetAsync(flags, 0, 4, s), "cudaMemsetAsync");
+    spk::pack_rows_kernel<<<simple_grid(rows), 256, 0, s>>>(d0, d1, rows, dst.as<u64>(), flags);
+    SPK_CUDA(cudaGetLastError(), "pack_rows_kernel");
+    SPK_CUDA(cudaMemcpyAsync(st->pinned, flags, 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+    SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    *sorted = (st->pinned[0] & 1u) == 0;
+    *has_dups = (st->pinned[0] & 2u) != 0;
+    return 0;
+}
+
+struct SortScratch {
+    DevArray plan;     // RadixPlan
+    DevArray status;   // look-back words
+};
+
+struct IndexCache {
+    bool valid = false;
+    u32 relation = 0;
+    u64 version = 0;
+    u32 column = 0;
+    DevArray offsets;   // u32[num_keys + 1]
+    DevArray rows;      // u32[n] (empty when identity)
+    bool identity = true;
+    u64 num_keys = 0;
+    u32 max_degree = 0;
+};
+
+struct TargetRT {
+    u32 id = 0;
+    std::vector<size_t> rules;
+    DevArray j_a, j_b;     // candidate buffers (sort ping-pong)
+    u64 j_cap = 0;         // elements
+    SortScratch sort;
+};
+
+}  // namespace
+
+struct sparkalog_executor {
+    std::vector<u32> relations;
+    std::vector<sparkalog_rule_plan> rules;
+    std::vector<TargetRT> targets;
+    std::vector<IndexCache> index;
+    DevArray counts;       // device: per target [rules+1] join counts, sort count, newt count
+    DevArray counters;     // device: tile counters, error word
+    DevArray status;       // shared look-back words for join / anti-join
+    u64* host_counts = nullptr;  // pinned mirror of `counts`
+    DevArray rule_delta;         // device: DELTA row count of each rule's delta input
+    u64* host_rule_delta = nullptr;
+    size_t counts_words = 0;
+    u32 epoch = 1;
+    SortScratch index_sort;
+    DevArray index_pairs[2];
+    u32* host_active = nullptr;  // pinned: radix pass activity per target (8 words each)
+
+    // Profiling: CUDA events around each kernel class on the executor's stream.
+    struct Timing {
+        int cls;
+        cudaEvent_t a, b;
+        double bytes;
+        u64 launches;
+    };
+    bool profiling = false;
+    std::vector<cudaEvent_t> free_events;
+    std::vector<Timing> timings;
+    sparkalog_kernel_stats stats{};
+
+    cudaEvent_t take_event() {
+        if (free_events.empty()) {
+            cudaEvent_t e = nullptr;
+            cudaEventCreate(&e);
+            return e;
+        }
+        cudaEvent_t e = free_events.back();
+        free_events.pop_back();
+        return e;
+    }
+    // Opens a timed section; returns its index or -1 when not profiling.
+    int begin(int cls, cudaStream_t s) {
+        if (!profiling) return -1;
+        Timing t{cls, take_event(), take_event(), 0.0, 0};
+        cudaEventRecord(t.a, s);
+        timings.push_back(t);
+        return static_cast<int>(timings.size()) - 1;
+    }
+    void end(int idx, cudaStream_t s, double bytes, u64 launches) {
+        if (idx < 0) return;
+        cudaEventRecord(timings[idx].b, s);
+        timings[idx].bytes = bytes;
+        timings[idx].launches = launches;
+    }
+    // Folds completed sections into the statistics (call after a stream sync).
+    void collect() {
+        for (auto& t : timings) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, t.a, t.b) == cudaSuccess) {
+                stats.milliseconds[t.cls] += ms;
+                stats.bytes[t.cls] += t.bytes;
+                stats.launches[t.cls] += t.launches;
+            }
+            free_events.push_back(t.a);
+            free_events.push_back(t.b);
+        }
+        timings.clear();
+    }
+};
+
+namespace {
+
+// Radix sort of *n_dev keys (or n_host_bound keys when n_dev is null) held in
+// buffers a/b; n_host_bound sizes the grids and the look-back buffer. The
+// sorted keys end in a or b as RadixPlan::final_sel says.
+int radix_sort(u64* a, u64* b, const u64* n_dev, u64 n_host_bound, SortScratch& sc, sparkalog_executor* ex,
+               u32* err, cudaStream_t s, int* hist_timing, int* pass_timing) {
+    SPK_CUDA(sc.plan.ensure(sizeof(spk::RadixPlan), s), "cudaMallocAsync");
+    SPK_CUDA(sc.status.ensure(spk::radix_status_words(n_host_bound) * 8, s), "cudaMallocAsync");
+    spk::RadixPlan* plan = sc.plan.as<spk::RadixPlan>();
+    const int th = ex->begin(SPARKALOG_K_SORT_HIST, s);
+    SPK_CUDA(cudaMemsetAsync(plan, 0, spk::kRadixPlanClearBytes, s), "cudaMemsetAsync");
+    constexpr int kPasses = 8;
+    {
+        auto kernel = spk::radix_histogram<kThreads>;
+        kernel<<<simple_grid(n_host_bound), kThreads, 0, s>>>(a, n_dev, n_host_bound, plan, 0, kPasses);
+        SPK_CUDA(cudaGetLastError(), "radix_histogram");
+    }
+    spk::radix_plan<<<1, spk::kRadix, 0, s>>>(plan, n_dev, n_host_bound, kPasses);
+    SPK_CUDA(cudaGetLastError(), "radix_plan");
+    ex->end(th, s, 0.0, 2);
+    ex->stats.total_launches += 2;
+    const int tp = ex->begin(SPARKALOG_K_SORT_PASS, s);
+    auto kernel = spk::radix_pass<kSortThreads, kSortItems>;
+    const size_t tiles = (n_host_bound + kSortTile - 1) / kSortTile;
+    const unsigned grid = grid_for(reinterpret_cast<const void*>(kernel), kSortThreads, std::max<size_t>(tiles, 1));
+    for (int p = 0; p < kPasses; ++p) {
+        kernel<<<grid, kSortThreads, 0, s>>>(a, b, plan, plan, p, p * spk::kRadixBits, sc.status.as<u64>(), nullptr,
+                                             ex->epoch++, err);
+        SPK_CUDA(cudaGetLastError(), "radix_pass");
+    }
+    ex->end(tp, s, 0.0, 0);
+    ex->stats.total_launches += kPasses;
+    if (hist_timing) *hist_timing = th;
+    if (pass_timing) *pass_timing = tp;
+    return 0;
+}
+
+constexpr size_t kCounterWords = 1024;  // per-round tile counters
+constexpr size_t kErrWord = kCounterWords;
+
+size_t target_count_base(const sparkalog_executor* ex, size_t t) {
+    // Layout per target: [rules + 1 join counts][newt count]
+    size_t base = 0;
+    for (size_t i = 0; i < t; ++i) base += ex->targets[i].rules.size() + 2;
+    return base;
+}
+
+int build_index_impl(sparkalog_executor* ex, sparkalog_store* st, IndexCache& ic, u32 relation, u32 column);
+
+// Builds a rule's right index; its kernels are counted as launches but kept
+// out of the per-class timings of the round's operators.
+int build_index(sparkalog_executor* ex, sparkalog_store* st, IndexCache& ic, u32 relation, u32 column) {
+    const bool profiling = ex->profiling;
+    ex->profiling = false;
+    const int rc = build_index_impl(ex, st, ic, relation, column);
+    ex->profiling = profiling;
+    return rc;
+}
+
+int build_index_impl(sparkalog_executor* ex, sparkalog_store* st, IndexCache& ic, u32 relation, u32 column) {
+    cudaStream_t s = st->stream;
+    RelState* r = st->find(relation);
+    if (!r) return fail(SPARKALOG_E_MISSING, "relation " + std::to_string(relation) + " is not registered");
+    if (r->recursive) {
+        int rc = materialize(*r, s);
+        if (rc) return rc;
+    }
+    const u64 n = r->level_n[0];
+    const u64* rows = r->level[0].as<u64>();
+    const u64* sorted_keys = rows;
+    ic.identity = (column == 0 && r->sorted);
+    if (!ic.identity) {
+        // Index rows ordered by (key value, row id): sort (key << 32 | row).
+        SPK_CUDA(ex->index_pairs[0].ensure(std::max<u64>(n, 1) * 8, s), "cudaMallocAsync");
+        SPK_CUDA(ex->index_pairs[1].ensure(std::max<u64>(n, 1) * 8, s), "cudaMallocAsync");
+        if (n) {
+            spk::key_row_pairs_kernel<<<simple_grid(n), 256, 0, s>>>(rows, n, column, ex->index_pairs[0].as<u64>());
+            SPK_CUDA(cudaGetLastError(), "key_row_pairs_kernel");
+            u32* err = ex->counters.as<u32>() + kErrWord;
+            int rc = radix_sort(ex->index_pairs[0].as<u64>(), ex->index_pairs[1].as<u64>(), nullptr, n, ex->index_sort,
+                                ex, err, s, nullptr, nullptr);
+            if (rc) return rc;
+            // Bring the sorted pairs to buffer 0 regardless of pass parity.
+            u32 sel = 0;
+            SPK_CUDA(cudaMemcpyAsync(&sel, &ex->index_sort.plan.as<spk::RadixPlan>()->final_sel, 4,
+                                     cudaMemcpyDeviceToHost, s),
+                     "cudaMemcpyAsync");
+            SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+            if (sel) swap_arrays(ex->index_pairs[0], ex->index_pairs[1]);
+        }
+        sorted_keys = ex->index_pairs[0].as<u64>();
+        SPK_CUDA(ic.rows.ensure(std::max<u64>(n, 1) * 4, s), "cudaMallocAsync");
+        if (n) {
+            spk::low_words_kernel<<<simple_grid(n), 256, 0, s>>>(sorted_keys, n, ic.rows.as<u32>());
+            SPK_CUDA(cudaGetLastError(), "low_words_kernel");
+        }
+    }
+    // Key domain: [0, max key]. The keys are the high words of sorted_keys.
+    u64 last = 0;
+    if (n) {
+        SPK_CUDA(cudaMemcpyAsync(&last, sorted_keys + (n - 1), 8, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+        SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    }
+    ic.num_keys = n ? (last >> 32) + 1 : 0;
+    SPK_CUDA(ic.offsets.ensure((ic.num_keys + 1) * 4, s), "cudaMallocAsync");
+    u32* maxdeg = ex->counters.as<u32>() + kErrWord + 1;
+    SPK_CUDA(cudaMemsetAsync(maxdeg, 0, 4, s), "cudaMemsetAsync");
+    if (n) {
+        spk::dense_offsets_kernel<<<simple_grid(n), 256, 0, s>>>(sorted_keys, n, ic.num_keys, ic.offsets.as<u32>(),
+                                                                 maxdeg);
+        SPK_CUDA(cudaGetLastError(), "dense_offsets_kernel");
+        ex->stats.total_launches += ic.identity ? 1 : 3;
+    } else {
+        SPK_CUDA(cudaMemsetAsync(ic.offsets.ptr, 0, 4, s), "cudaMemsetAsync");
+    }
+    u32 md = 0;
+    SPK_CUDA(cudaMemcpyAsync(&md, maxdeg, 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+    SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    ic.max_degree = md;
+    ic.valid = true;
+    ic.relation = relation;
+    ic.version = r->version;
+    ic.column = column;
+    return 0;
+}
+
+bool valid_cols(const u32 c[2]) { return c[0] <= 1 && c[1] <= 1; }
+
+}  // namespace
+
+extern "C" {
+
+const char* sparkalog_last_error(void) { return g_last_error.c_str(); }
+
+int sparkalog_store_create(void* stream, sparkalog_store** out) {
+    if (!out) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null output pointer");
+    auto* st = new sparkalog_store();
+    st->stream = static_cast<cudaStream_t>(stream);
+    {
+        // Relations grow and shrink every round through cudaMallocAsync; keep
+        // freed blocks in the device's pool instead of returning them at
+        // every synchronisation.
+        int dev = 0;
+        cudaMemPool_t pool;
+        if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            uint64_t threshold = ~0ull;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+        }
+    }
+    cudaError_t e = st->flags.ensure(256, st->stream);
+    if (e == cudaSuccess) e = cudaMallocHost(&st->pinned, 256);
+    if (e != cudaSuccess) {
+        delete st;
+        return cuda_fail(e, "sparkalog_store_create");
+    }
+    *out = st;
+    return 0;
+}
+
+void sparkalog_store_destroy(sparkalog_store* st) {
+    if (!st) return;
+    cudaStream_t s = st->stream;
+    for (auto& kv : st->relations) {
+        for (auto& l : kv.second.level) l.release(s);
+        kv.second.spare.release(s);
+        kv.second.delta.release(s);
+        kv.second.newt.release(s);
+    }
+    st->scratch_u32[0].release(s);
+    st->scratch_u32[1].release(s);
+    st->flags.release(s);
+    cudaStreamSynchronize(s);
+    if (st->pinned) cudaFreeHost(st->pinned);
+    delete st;
+}
+
+int sparkalog_store_insert_static(sparkalog_store* st, u32 id, const u32* first, const u32* second, size_t rows,
+                                  int location) {
+    if (!st) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null store");
+    if (st->find(id)) return fail(SPARKALOG_E_DUPLICATE, "relation " + std::to_string(id) + " is already registered");
+    if (rows > 0xffffffffull) return fail(SPARKALOG_E_TOO_MANY_ROWS, "too many rows for u32 row ids");
+    RelState r;
+    int rc = pack_columns(st, first, second, rows, location, r.level[0], &r.sorted, &r.has_dups);
+    if (rc) return rc;
+    r.level_n[0] = rows;
+    st->relations[id] = std::move(r);
+    return 0;
+}
+
+int sparkalog_store_insert_recursive(sparkalog_store* st, u32 id, const u32* full_first, const u32* full_second,
+                                     size_t full_rows, const u32* delta_first, const u32* delta_second,
+                                     size_t delta_rows, int location) {
+    if (!st) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null store");
+    if (st->find(id)) return fail(SPARKALOG_E_DUPLICATE, "relation " + std::to_string(id) + " is already registered");
+    if (full_rows > 0xffffffffull || delta_rows > 0xffffffffull)
+        return fail(SPARKALOG_E_TOO_MANY_ROWS, "too many rows for u32 row ids");
+    RelState r;
+    r.recursive = true;
+    int rc = pack_columns(st, full_first, full_second, full_rows, location, r.level[0], &r.sorted, &r.has_dups);
+    if (rc) return rc;
+    r.level_n[0] = full_rows;
+    if (delta_first == full_first && delta_second == full_second && delta_rows == full_rows) {
+        // DELTA = FULL (how execute_binary seeds every recursive relation,
+        // datalog/src/subset.rs:406-408): copy on the device, upload once.
+        SPK_CUDA(r.delta.ensure(std::max<size_t>(full_rows, 1) * 8, st->stream), "cudaMallocAsync");
+        if (full_rows)
+            SPK_CUDA(cudaMemcpyAsync(r.delta.ptr, r.level[0].ptr, full_rows * 8, cudaMemcpyDeviceToDevice,
+                                     st->stream),
+                     "cudaMemcpyAsync");
+    } else {
+        bool dsorted, ddups;
+        rc = pack_columns(st, delta_first, delta_second, delta_rows, location, r.delta, &dsorted, &ddups);
+        if (rc) return rc;
+    }
+    r.delta_n = delta_rows;
+    SPK_CUDA(r.newt.ensure(4096, st->stream), "cudaMallocAsync");
+    st->relations[id] = std::move(r);
+    return 0;
+}
+
+int sparkalog_store_rows(sparkalog_store* st, u32 id, int version, size_t* rows) {
+    if (!st || !rows) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null argument");
+    RelState* r = st->find(id);
+    if (!r) return fail(SPARKALOG_E_MISSING, "relation " + std::to_string(id) + " is not registered");
+    if (version == SPARKALOG_FULL) {
+        *rows = r->full_rows();
+        return 0;
+    }
+    if (!r->recursive) return fail(SPARKALOG_E_NOT_RECURSIVE, "relation has no DELTA/NEWT state");
+    *rows = r->delta_n;
+    return 0;
+}
+
+int sparkalog_store_read(sparkalog_store* st, u32 id, int version, u32* first, u32* second, int location) {
+    if (!st) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null store");
+    RelState* r = st->find(id);
+    if (!r) return fail(SPARKALOG_E_MISSING, "relation " + std::to_string(id) + " is not registered");
+    cudaStream_t s = st->stream;
+    const u64* src;
+    u64 n;
+    if (version == SPARKALOG_FULL) {
+        if (r->recursive) {
+            int rc = materialize(*r, s);
+            if (rc) return rc;
+        }
+        src = r->level[0].as<u64>();
+        n = r->level_n[0];
+    } else {
+        if (!r->recursive) return fail(SPARKALOG_E_NOT_RECURSIVE, "relation has no DELTA/NEWT state");
+        src = r->delta.as<u64>();
+        n = r->delta_n;
+    }
+    if (n == 0) return 0;
+    if (!first || !second) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null output column");
+    u32* d0 = first;
+    u32* d1 = second;
+    if (location == SPARKALOG_HOST) {
+        SPK_CUDA(st->scratch_u32[0].ensure(n * 4, s), "cudaMallocAsync");
+        SPK_CUDA(st->scratch_u32[1].ensure(n * 4, s), "cudaMallocAsync");
+        d0 = st->scratch_u32[0].as<u32>();
+        d1 = st->scratch_u32[1].as<u32>();
+    }
+    spk::unpack_rows_kernel<<<simple_grid(n), 256, 0, s>>>(src, n, d0, d1);
+    SPK_CUDA(cudaGetLastError(), "unpack_rows_kernel");
+    if (location == SPARKALOG_HOST) {
+        SPK_CUDA(cudaMemcpyAsync(first, d0, n * 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+        SPK_CUDA(cudaMemcpyAsync(second, d1, n * 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+    }
+    SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    return 0;
+}
+
+int sparkalog_executor_compile(sparkalog_store* st, const u32* relations, size_t relation_count,
+                               const sparkalog_rule_plan* rules, size_t rule_count, sparkalog_executor** out) {
+    if (!st || !out || (relation_count && !relations) || (rule_count && !rules))
+        return fail(SPARKALOG_E_INVALID_ARGUMENT, "null argument");
+    if (relation_count == 0) return fail(SPARKALOG_E_EMPTY_SCC, "recursive SCC has no relations");
+    for (size_t i = 0; i < relation_count; ++i) {
+        for (size_t j = 0; j < i; ++j)
+            if (relations[j] == relations[i])
+                return fail(SPARKALOG_E_DUPLICATE_SCC_RELATION,
+                            "relation " + std::to_string(relations[i]) + " occurs twice in its SCC");
+        RelState* r = st->find(relations[i]);
+        if (!r) return fail(SPARKALOG_E_MISSING, "relation " + std::to_string(relations[i]) + " is not registered");
+        if (!r->recursive)
+            return fail(SPARKALOG_E_NOT_RECURSIVE,
+                        "relation " + std::to_string(relations[i]) + " has no DELTA/NEWT state");
+    }
+    auto in_scc = [&](u32 id) {
+        for (size_t i = 0; i < relation_count; ++i)
+            if (relations[i] == id) return true;
+        return false;
+    };
+    for (size_t k = 0; k < rule_count; ++k) {
+        const sparkalog_rule_plan& p = rules[k];
+        if (!st->find(p.delta_input))
+            return fail(SPARKALOG_E_MISSING, "relation " + std::to_string(p.delta_input) + " is not registered");
+        if (!st->find(p.right_input))
+            return fail(SPARKALOG_E_MISSING, "relation " + std::to_string(p.right_input) + " is not registered");
+        if (!in_scc(p.delta_input))
+            return fail(SPARKALOG_E_DELTA_OUTSIDE_SCC,
+                        "DELTA relation " + std::to_string(p.delta_input) + " is outside its SCC");
+        if (!in_scc(p.target))
+            return fail(SPARKALOG_E_TARGET_OUTSIDE_SCC,
+                        "rule target " + std::to_string(p.target) + " is outside its SCC");
+    }
+    auto* ex = new sparkalog_executor();
+    ex->relations.assign(relations, relations + relation_count);
+    ex->rules.assign(rules, rules + rule_count);
+    for (size_t t = 0; t < relation_count; ++t) {
+        TargetRT trt;
+        trt.id = relations[t];
+        for (size_t k = 0; k < rule_count; ++k)
+            if (rules[k].target == relations[t]) trt.rules.push_back(k);
+        if (trt.rules.empty()) {
+            delete ex;
+            return fail(SPARKALOG_E_MISSING_RULE_TARGET,
+                        "relation " + std::to_string(relations[t]) + " has no recursive rule");
+        }
+        const sparkalog_rule_plan& first = rules[trt.rules[0]];
+        for (size_t k : trt.rules) {
+            const sparkalog_rule_plan& p = rules[k];
+            if (std::memcmp(p.anti_left, first.anti_left, 8) || std::memcmp(p.anti_right, first.anti_right, 8) ||
+                std::memcmp(p.union_left, first.union_left, 8) || std::memcmp(p.union_right, first.union_right, 8)) {
+                delete ex;
+                return fail(SPARKALOG_E_INCOMPATIBLE_TARGET_PLANS,
+                            "clauses for relation " + std::to_string(relations[t]) +
+                                " use incompatible set plans");
+            }
+        }
+        ex->targets.push_back(std::move(trt));
+    }
+    ex->index.resize(rule_count);
+    ex->counts_words = 0;
+    for (auto& t : ex->targets) ex->counts_words += t.rules.size() + 2;
+    cudaStream_t s = st->stream;
+    cudaError_t e = ex->counts.ensure(ex->counts_words * 8, s);
+    if (e == cudaSuccess) e = ex->counters.ensure((kCounterWords + 64) * 4, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ex->counters.ptr, 0, (kCounterWords + 64) * 4, s);
+    if (e == cudaSuccess) e = cudaMallocHost(&ex->host_counts, ex->counts_words * 8 + 64);
+    if (e == cudaSuccess) e = ex->rule_delta.ensure(std::max<size_t>(rule_count, 1) * 8, s);
+    if (e == cudaSuccess) e = cudaMallocHost(&ex->host_rule_delta, std::max<size_t>(rule_count, 1) * 8);
+    if (e == cudaSuccess) e = cudaMallocHost(&ex->host_active, relation_count * spk::kMaxPasses * 4 + 64);
+    if (e != cudaSuccess) {
+        delete ex;
+        return cuda_fail(e, "sparkalog_executor_compile");
+    }
+    *out = ex;
+    return 0;
+}
+
+void sparkalog_executor_destroy(sparkalog_executor* ex) {
+    if (!ex) return;
+    cudaStream_t s = nullptr;
+    for (auto& t : ex->targets) {
+        t.j_a.release(s);
+        t.j_b.release(s);
+        t.sort.plan.release(s);
+        t.sort.status.release(s);
+    }
+    for (auto& ic : ex->index) {
+        ic.offsets.release(s);
+        ic.rows.release(s);
+    }
+    ex->counts.release(s);
+    ex->rule_delta.release(s);
+    ex->counters.release(s);
+    ex->status.release(s);
+    ex->index_sort.plan.release(s);
+    ex->index_sort.status.release(s);
+    ex->index_pairs[0].release(s);
+    ex->index_pairs[1].release(s);
+    cudaDeviceSynchronize();
+    if (ex->host_counts) cudaFreeHost(ex->host_counts);
+    if (ex->host_rule_delta) cudaFreeHost(ex->host_rule_delta);
+    if (ex->host_active) cudaFreeHost(ex->host_active);
+    for (auto& t : ex->timings) {
+        cudaEventDestroy(t.a);
+        cudaEventDestroy(t.b);
+    }
+    for (cudaEvent_t e : ex->free_events) cudaEventDestroy(e);
+    delete ex;
+}
+
+int sparkalog_executor_set_profiling(sparkalog_executor* ex, int enable) {
+    if (!ex) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null executor");
+    ex->profiling = enable != 0;
+    return 0;
+}
+
+int sparkalog_executor_stats(sparkalog_executor* ex, sparkalog_kernel_stats* out, int reset) {
+    if (!ex || !out) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null argument");
+    *out = ex->stats;
+    if (reset) ex->stats = sparkalog_kernel_stats{};
+    return 0;
+}
+
+int sparkalog_executor_run(sparkalog_executor* ex, sparkalog_store* st, size_t max_iterations,
+                           sparkalog_scc_summary* summary) {
+    if (!ex || !st) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null argument");
+    cudaStream_t s = st->stream;
+    for (const auto& p : ex->rules) {
+        if (p.left_key > 1 || p.right_key > 1 || !valid_cols(p.proj_col) || !valid_cols(p.distinct_cols) ||
+            !valid_cols(p.anti_left) || !valid_cols(p.anti_right) || !valid_cols(p.union_left) ||
+            !valid_cols(p.union_right) || p.proj_side[0] > 1 || p.proj_side[1] > 1)
+            return fail(SPARKALOG_E_MISSING_COLUMN, "plan names a column outside a binary relation");
+        // The device pipeline keeps rows packed in (first, second) order, which
+        // is the only set-operator column order the binary lowering produces
+        // (datalog/src/subset.rs:226-237).
+        if (p.distinct_cols[0] != 0 || p.distinct_cols[1] != 1 || p.anti_left[0] != 0 || p.anti_left[1] != 1 ||
+            p.anti_right[0] != 0 || p.anti_right[1] != 1 || p.union_left[0] != 0 || p.union_left[1] != 1 ||
+            p.union_right[0] != 0 || p.union_right[1] != 1)
+            return fail(SPARKALOG_E_INVALID_ARGUMENT, "set operators must use columns [0, 1]");
+    }
+    u32* counters = ex->counters.as<u32>();
+    u32* err = counters + kErrWord;
+    u64* counts = ex->counts.as<u64>();
+
+    // FULL of each SCC relation must be a sorted run before the first merge;
+    // duplicates inside it are removed the way the reference's first union
+    // would remove them (only when a round will run).
+    bool any_delta = false;
+    for (u32 id : ex->relations) any_delta |= st->find(id)->delta_n != 0;
+    if (any_delta) {
+        for (u32 id : ex->relations) {
+            RelState& r = *st->find(id);
+            int rc = materialize(r, s);
+            if (rc) return rc;
+            if (!r.sorted)
+                return fail(SPARKALOG_E_UNSORTED_FULL,
+                            "FULL of relation " + std::to_string(id) + " is not sorted by (first, second)");
+            if (r.has_dups && r.level_n[0] > 0) {
+                const u64 n = r.level_n[0];
+                SPK_CUDA(r.spare.ensure(n * 8, s), "cudaMallocAsync");
+                SPK_CUDA(ex->status.ensure(((n + kSetTile - 1) / kSetTile + 1) * 8, s), "cudaMallocAsync");
+                SPK_CUDA(cudaMemsetAsync(counters, 0, kCounterWords * 4, s), "cudaMemsetAsync");
+                SPK_CUDA(cudaMemsetAsync(counts, 0, 8, s), "cudaMemsetAsync");
+                // unique over the packed run: anti-join against no levels.
+                spk::Levels none{};
+                none.n = 0;
+                u64* nptr = counts + 1;
+                SPK_CUDA(cudaMemcpyAsync(nptr, &r.level_n[0], 8, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
+                auto kernel = spk::anti_join_levels_kernel<kThreads, kSetItems>;
+                const size_t tiles = (n + kSetTile - 1) / kSetTile;
+                kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, tiles), kThreads, 0, s>>>(
+                    r.level[0].as<u64>(), r.level[0].as<u64>(), nullptr, nptr, none, r.spare.as<u64>(), counts,
+                    ex->status.as<u64>(), counters, ex->epoch++, err);
+                SPK_CUDA(cudaGetLastError(), "anti_join_levels_kernel");
+                ex->stats.total_launches += 1;
+                SPK_CUDA(cudaMemcpyAsync(ex->host_counts, counts, 8, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+                SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+                swap_arrays(r.level[0], r.spare);
+                r.level_n[0] = ex->host_counts[0];
+                r.has_dups = false;
+            }
+        }
+    }
+
+    u64 iterations = 0, total_new = 0;
+    for (;;) {
+        bool has_delta = false;
+        u64 remaining = 0;
+        for (u32 id : ex->relations) {
+            has_delta |= st->find(id)->delta_n != 0;
+            remaining += st->find(id)->delta_n;
+        }
+        if (!has_delta) break;
+        if (iterations >= max_iterations) {
+            if (summary) {
+                summary->iterations = iterations;
+                summary->total_new_rows = total_new;
+            }
+            return fail(SPARKALOG_E_ITERATION_LIMIT, "recursive SCC did not converge within " +
+                                                         std::to_string(max_iterations) + " iterations; " +
+                                                         std::to_string(remaining) + " delta rows remain");
+        }
+        if (ex->epoch > spk::kEpochMask - 4096) {
+            // Epoch wrap: clear every look-back buffer so stale words never match.
+            if (ex->status.ptr) SPK_CUDA(cudaMemsetAsync(ex->status.ptr, 0, ex->status.bytes, s), "cudaMemsetAsync");
+            for (auto& t : ex->targets)
+                if (t.sort.status.ptr)
+                    SPK_CUDA(cudaMemsetAsync(t.sort.status.ptr, 0, t.sort.status.bytes, s), "cudaMemsetAsync");
+            if (ex->index_sort.status.ptr)
+                SPK_CUDA(cudaMemsetAsync(ex->index_sort.status.ptr, 0, ex->index_sort.status.bytes, s),
+                         "cudaMemsetAsync");
+            ex->epoch = 1;
+        }
+
+        // RuleRuntime::evaluate's index cache (generic.rs:217-229).
+        for (size_t k = 0; k < ex->rules.size(); ++k) {
+            const sparkalog_rule_plan& p = ex->rules[k];
+            RelState* right = st->find(p.right_input);
+            IndexCache& ic = ex->index[k];
+            if (!ic.valid || ic.relation != p.right_input || ic.version != right->version ||
+                ic.column != p.right_key) {
+                int rc = build_index(ex, st, ic, p.right_input, p.right_key);
+                if (rc) return rc;
+            }
+        }
+
+        // Size the candidate buffers: |J| <= sum over rules of |DELTA| * max degree,
+        // so the capacity flag below only fires if that bound is not met.
+        size_t max_status_words = 64;
+        for (size_t k = 0; k < ex->rules.size(); ++k) {
+            const u64 dn = st->find(ex->rules[k].delta_input)->delta_n;
+            ex->host_rule_delta[k] = dn;
+            max_status_words = std::max<size_t>(max_status_words, (dn + kJoinTile - 1) / kJoinTile + 1);
+        }
+        for (auto& t : ex->targets) {
+            u64 bound = 0;
+            for (size_t k : t.rules)
+                bound += ex->host_rule_delta[k] * static_cast<u64>(std::max<u32>(ex->index[k].max_degree, 1));
+            const u64 want = std::max<u64>(bound, 1024);
+            if (t.j_cap < want) {
+                const u64 cap = want + want / 4;
+                SPK_CUDA(t.j_a.ensure(cap * 8, s), "cudaMallocAsync");
+                SPK_CUDA(t.j_b.ensure(cap * 8, s), "cudaMallocAsync");
+                t.j_cap = cap;
+            }
+        }
+        SPK_CUDA(cudaMemcpyAsync(ex->rule_delta.ptr, ex->host_rule_delta, ex->rules.size() * 8,
+                                 cudaMemcpyHostToDevice, s),
+                 "cudaMemcpyAsync");
+
+        for (;;) {
+            for (auto& t : ex->targets) {
+                SPK_CUDA(st->find(t.id)->newt.ensure(t.j_cap * 8, s), "cudaMallocAsync");
+                max_status_words = std::max<size_t>(max_status_words, (t.j_cap + kSetTile - 1) / kSetTile + 1);
+            }
+            SPK_CUDA(ex->status.ensure(max_status_words * 8, s), "cudaMallocAsync");
+            SPK_CUDA(cudaMemsetAsync(counters, 0, (kCounterWords + 1) * 4, s), "cudaMemsetAsync");
+            SPK_CUDA(cudaMemsetAsync(counts, 0, ex->counts_words * 8, s), "cudaMemsetAsync");
+            size_t counter_slot = 0;
+            const int join_timing = ex->begin(SPARKALOG_K_JOIN, s);
+            // Joins: every rule appends into its target's candidate buffer.
+            for (size_t ti = 0; ti < ex->targets.size(); ++ti) {
+                TargetRT& t = ex->targets[ti];
+                u64* tc = counts + target_count_base(ex, ti);
+                for (size_t pos = 0; pos < t.rules.size(); ++pos) {
+                    const size_t k = t.rules[pos];
+                    const sparkalog_rule_plan& p = ex->rules[k];
+                    RelState& d = *st->find(p.delta_input);
+                    RelState& right = *st->find(p.right_input);
+                    IndexCache& ic = ex->index[k];
+                    spk::FusedJoinArgs a{};
+                    a.delta = d.delta.as<u64>();
+                    a.delta_count = ex->rule_delta.as<u64>() + k;
+                    a.left_key = p.left_key;
+                    a.dense_offsets = ic.offsets.as<u32>();
+                    a.dense_keys = ic.num_keys;
+                    a.rows = ic.identity ? nullptr : ic.rows.as<u32>();
+                    a.right = right.level[0].as<u64>();
+                    a.side[0] = p.proj_side[0];
+                    a.side[1] = p.proj_side[1];
+                    a.col[0] = p.proj_col[0];
+                    a.col[1] = p.proj_col[1];
+                    a.out = t.j_a.as<u64>();
+                    a.capacity = t.j_cap;
+                    a.count_in = tc + pos;
+                    a.count_out = tc + pos + 1;
+                    a.status = ex->status.as<u64>();
+                    a.tile_counter = counters + counter_slot++;
+                    a.epoch_ptr = nullptr;
+                    a.epoch_add = ex->epoch++;
+                    a.err = err;
+                    auto kernel = spk::join_fused_kernel<kThreads, kJoinItems>;
+                    const size_t tiles = (ex->host_rule_delta[k] + kJoinTile - 1) / kJoinTile;
+                    kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, std::max<size_t>(tiles, 1)),
+                             kThreads, 0, s>>>(a);
+                    SPK_CUDA(cudaGetLastError(), "join_fused_kernel");
+                    ex->stats.total_launches += 1;
+                }
+            }
+            ex->end(join_timing, s, 0.0, ex->rules.size());
+            std::vector<int> hist_t(ex->targets.size(), -1), pass_t(ex->targets.size(), -1),
+                anti_t(ex->targets.size(), -1);
+            // Distinct (radix sort) + unique/anti-join per target. The sort
+            // reads the clamped candidate count from the device.
+            for (size_t ti = 0; ti < ex->targets.size(); ++ti) {
+                TargetRT& t = ex->targets[ti];
+                u64* tc = counts + target_count_base(ex, ti);
+                u64* jn = tc + t.rules.size();
+                int rc = radix_sort(t.j_a.as<u64>(), t.j_b.as<u64>(), jn, t.j_cap, t.sort, ex, err, s, &hist_t[ti],
+                                    &pass_t[ti]);
+                if (rc) return rc;
+                RelState& tr = *st->find(t.id);
+                spk::Levels lv{};
+                lv.n = 0;
+                for (int l = 0; l < spk::kMaxLevels; ++l) {
+                    if (tr.level_n[l] == 0) continue;
+                    lv.keys[lv.n] = tr.level[l].as<u64>();
+                    lv.count[lv.n] = tr.level_n[l];
+                    ++lv.n;
+                }
+                auto kernel = spk::anti_join_levels_kernel<kThreads, kSetItems>;
+                const size_t tiles = (t.j_cap + kSetTile - 1) / kSetTile;
+                anti_t[ti] = ex->begin(SPARKALOG_K_ANTI_JOIN, s);
+                kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, std::max<size_t>(tiles, 1)),
+                         kThreads, 0, s>>>(t.j_a.as<u64>(), t.j_b.as<u64>(),
+                                           &t.sort.plan.as<spk::RadixPlan>()->final_sel, jn, lv, tr.newt.as<u64>(),
+                                           tc + t.rules.size() + 1, ex->status.as<u64>(), counters + counter_slot++,
+                                           ex->epoch++, err);
+                SPK_CUDA(cudaGetLastError(), "anti_join_levels_kernel");
+                ex->end(anti_t[ti], s, 0.0, 1);
+                ex->stats.total_launches += 1;
+                SPK_CUDA(cudaMemcpyAsync(ex->host_active + ti * spk::kMaxPasses, t.sort.plan.as<spk::RadixPlan>()->active,
+                                         spk::kMaxPasses * 4, cudaMemcpyDeviceToHost, s),
+                         "cudaMemcpyAsync");
+            }
+            // The round's only host synchronisation: counts and error bits.
+            SPK_CUDA(cudaMemcpyAsync(ex->host_counts, counts, ex->counts_words * 8, cudaMemcpyDeviceToHost, s),
+                     "cudaMemcpyAsync");
+            SPK_CUDA(cudaMemcpyAsync(ex->host_counts + ex->counts_words, err, 4, cudaMemcpyDeviceToHost, s),
+                     "cudaMemcpyAsync");
+            SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+            const u32 bits = static_cast<u32>(ex->host_counts[ex->counts_words] & 0xffffffffu);
+            if (ex->profiling) {
+                // Algorithmic bytes (each input row read once, each output written once).
+                double join_bytes = 0.0;
+                for (size_t k = 0; k < ex->rules.size(); ++k) join_bytes += 16.0 * ex->host_rule_delta[k];
+                for (size_t ti = 0; ti < ex->targets.size(); ++ti) {
+                    const TargetRT& t = ex->targets[ti];
+                    const double jn = static_cast<double>(ex->host_counts[target_count_base(ex, ti) + t.rules.size()]);
+                    const double nn =
+                        static_cast<double>(ex->host_counts[target_count_base(ex, ti) + t.rules.size() + 1]);
+                    join_bytes += 12.0 * jn;
+                    u64 active = 0;
+                    for (int p = 0; p < spk::kMaxPasses; ++p) active += ex->host_active[ti * spk::kMaxPasses + p] ? 1 : 0;
+                    if (hist_t[ti] >= 0) ex->timings[hist_t[ti]].bytes = 8.0 * jn;
+                    if (pass_t[ti] >= 0) {
+                        ex->timings[pass_t[ti]].bytes = 16.0 * jn * static_cast<double>(active);
+                        ex->timings[pass_t[ti]].launches = active;
+                    }
+                    if (anti_t[ti] >= 0) ex->timings[anti_t[ti]].bytes = 8.0 * jn + 8.0 * nn;
+                }
+                if (join_timing >= 0) ex->timings[join_timing].bytes = join_bytes;
+                ex->collect();
+            }
+            if (!(bits & spk::kErrCapacity)) break;
+            // A candidate buffer overflowed: grow it and redo the round (no
+            // relation state has changed yet).
+            for (auto& t : ex->targets) {
+                const u64 cap = t.j_cap * 2;
+                SPK_CUDA(t.j_a.ensure(cap * 8, s), "cudaMallocAsync");
+                SPK_CUDA(t.j_b.ensure(cap * 8, s), "cudaMallocAsync");
+                t.j_cap = cap;
+            }
+            SPK_CUDA(cudaMemsetAsync(err, 0, 4, s), "cudaMemsetAsync");
+        }
+
+        const u32 err_bits = static_cast<u32>(ex->host_counts[ex->counts_words] & 0xffffffffu);
+        if (err_bits & ~spk::kErrCapacity)
+            return fail(SPARKALOG_E_DEVICE_FAULT, "device error bits " + std::to_string(err_bits));
+
+        // TargetRuntime::apply: FULL u= NEWT (into the levels), DELTA <- NEWT.
+        for (size_t ti = 0; ti < ex->targets.size(); ++ti) {
+            TargetRT& t = ex->targets[ti];
+            RelState& tr = *st->find(t.id);
+            const u64 newt_n = ex->host_counts[target_count_base(ex, ti) + t.rules.size() + 1];
+            if (newt_n > 0) {
+                // TAIL <- TAIL u NEWT
+                const int tail = spk::kMaxLevels - 1;
+                const u64 tn = tr.level_n[tail] + newt_n;
+                SPK_CUDA(tr.spare.ensure(tn * 8, s), "cudaMallocAsync");
+                {
+                    const bool kernel = tr.level_n[tail] != 0;
+                    const int tm = ex->begin(SPARKALOG_K_MERGE, s);
+                    SPK_CUDA(launch_merge(tr.level[tail].as<u64>(), tr.level_n[tail], tr.newt.as<u64>(), newt_n,
+                                          tr.spare.as<u64>(), s),
+                             "merge_disjoint_kernel");
+                    ex->end(tm, s, 16.0 * static_cast<double>(tn), kernel ? 1 : 0);
+                    ex->stats.total_launches += kernel ? 1 : 0;
+                }
+                swap_arrays(tr.level[tail], tr.spare);
+                tr.level_n[tail] = tn;
+                // Cascade: a level merges down once it outgrows 1/kLevelRatio of the next.
+                for (int l = tail; l > 0; --l) {
+                    if (tr.level_n[l] == 0 || tr.level_n[l] * kLevelRatio <= tr.level_n[l - 1]) continue;
+                    if (tr.level_n[l - 1] == 0) {
+                        swap_arrays(tr.level[l - 1], tr.level[l]);
+                        tr.level_n[l - 1] = tr.level_n[l];
+                        tr.level_n[l] = 0;
+                        continue;
+                    }
+                    const u64 mn = tr.level_n[l - 1] + tr.level_n[l];
+                    SPK_CUDA(tr.spare.ensure(mn * 8, s), "cudaMallocAsync");
+                    const int tm = ex->begin(SPARKALOG_K_MERGE, s);
+                    SPK_CUDA(launch_merge(tr.level[l - 1].as<u64>(), tr.level_n[l - 1], tr.level[l].as<u64>(),
+                                          tr.level_n[l], tr.spare.as<u64>(), s),
+                             "merge_disjoint_kernel");
+                    ex->end(tm, s, 16.0 * static_cast<double>(mn), 1);
+                    ex->stats.total_launches += 1;
+                    swap_arrays(tr.level[l - 1], tr.spare);
+                    tr.level_n[l - 1] = mn;
+                    tr.level_n[l] = 0;
+                }
+            }
+            swap_arrays(tr.delta, tr.newt);
+            tr.delta_n = newt_n;
+            tr.version += 1;
+            total_new += newt_n;
+        }
+        iterations += 1;
+        ex->stats.rounds += 1;
+    }
+    SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    ex->collect();
+    if (summary) {
+        summary->iterations = iterations;
+        summary->total_new_rows = total_new;
+        if (summary->relation_ids && summary->relation_rows) {
+            const size_t n = std::min<size_t>(summary->relation_count, ex->relations.size());
+            for (size_t i = 0; i < n; ++i) {
+                summary->relation_ids[i] = ex->relations[i];
+                summary->relation_rows[i] = st->find(ex->relations[i])->full_rows();
+            }
+        }
+        summary->relation_count = ex->relations.size();
+    }
+    return 0;
+}
+
+}  // extern "C"

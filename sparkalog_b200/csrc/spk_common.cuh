@@ -1,0 +1,190 @@
+// Shared device primitives for the sparkalog B200 kernels.
+//
+// All kernels here are integer, HBM-bound work (sort, merge, join, compaction);
+// none of it is a dense contraction, so the tensor cores are not used.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+
+namespace spk {
+
+using u32 = std::uint32_t;
+using u64 = std::uint64_t;
+
+constexpr int kWarp = 32;
+
+// Error bits written to a device error word (never a trap or an assert).
+enum : u32 {
+    kErrLookbackTimeout = 1u << 0,   // a decoupled look-back spin hit its cap
+    kErrCapacity = 1u << 1,          // an output did not fit its buffer
+    kErrIndexRange = 1u << 2,        // a key outside the dense index range
+};
+
+__device__ __forceinline__ u32 lanemask_lt() {
+    u32 mask;
+    asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(mask));
+    return mask;
+}
+
+__device__ __forceinline__ u32 lane_id() { return threadIdx.x & (kWarp - 1); }
+__device__ __forceinline__ u32 warp_id() { return threadIdx.x / kWarp; }
+
+__device__ __forceinline__ u64 ld_volatile(const u64* p) {
+    u64 v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_volatile(u64* p, u64 v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// Decoupled look-back status words.
+//
+// One 64-bit word per (tile, channel): [63:40] epoch, [39:38] flag, [37:0]
+// value. A word whose epoch differs from the running launch's epoch reads as
+// "not yet published", so a status buffer never needs clearing between
+// launches as long as consecutive users of one buffer use distinct epochs.
+// ---------------------------------------------------------------------------
+constexpr u64 kFlagAggregate = 1;
+constexpr u64 kFlagInclusive = 2;
+constexpr int kValueBits = 38;
+constexpr u64 kValueMask = (1ull << kValueBits) - 1;
+constexpr u32 kEpochMask = (1u << 24) - 1;
+
+__device__ __forceinline__ u64 make_status(u32 epoch, u64 flag, u64 value) {
+    return (static_cast<u64>(epoch & kEpochMask) << 40) | (flag << kValueBits) | (value & kValueMask);
+}
+
+// Spin cap for one look-back wait. Predecessor tiles are always held by
+// resident CTAs (tile ids come from an atomic counter in acquisition order),
+// so a wait this long only happens if something is broken; the kernel then
+// records kErrLookbackTimeout and continues with what it has.
+constexpr u32 kSpinCap = 1u << 22;
+
+// Sequential look-back for one channel. Returns the exclusive prefix of tile
+// `tile` and publishes its inclusive prefix. `status` points at the word of
+// tile 0 for this channel; consecutive tiles are `stride` words apart.
+__device__ __forceinline__ u64 lookback_exclusive(u64* status, size_t stride, u64 tile, u64 aggregate,
+                                                  u32 epoch, u32* err) {
+    if (tile == 0) {
+        st_volatile(status, make_status(epoch, kFlagInclusive, aggregate));
+        return 0;
+    }
+    st_volatile(status + tile * stride, make_status(epoch, kFlagAggregate, aggregate));
+    u64 exclusive = 0;
+    long long t = static_cast<long long>(tile) - 1;
+    u32 spins = 0;
+    while (t >= 0) {
+        u64 w = ld_volatile(status + static_cast<u64>(t) * stride);
+        u32 e = static_cast<u32>(w >> 40) & kEpochMask;
+        u64 flag = (w >> kValueBits) & 3;
+        if (e != (epoch & kEpochMask) || flag == 0) {
+            if (++spins > kSpinCap) {
+                atomicOr(err, kErrLookbackTimeout);
+                break;
+            }
+            if (spins > 64) __nanosleep(64);
+            continue;
+        }
+        exclusive += w & kValueMask;
+        if (flag == kFlagInclusive) break;
+        --t;
+    }
+    st_volatile(status + tile * stride, make_status(epoch, kFlagInclusive, exclusive + aggregate));
+    return exclusive;
+}
+
+// Warp-cooperative look-back for a single channel (used by compaction
+// kernels): lane i inspects tile (tile - 1 - i) so 32 predecessors are read per
+// step. Must be called by all 32 lanes of one warp; every lane gets the result.
+__device__ __forceinline__ u64 warp_lookback_exclusive(u64* status, u64 tile, u64 aggregate, u32 epoch,
+                                                       u32* err) {
+    const u32 lane = lane_id();
+    if (tile == 0) {
+        if (lane == 0) st_volatile(status, make_status(epoch, kFlagInclusive, aggregate));
+        return 0;
+    }
+    if (lane == 0) st_volatile(status + tile, make_status(epoch, kFlagAggregate, aggregate));
+    u64 exclusive = 0;
+    long long base = static_cast<long long>(tile) - 1;
+    u32 spins = 0;
+    while (base >= 0) {
+        long long t = base - lane;
+        u64 w = 0;
+        bool ready = true;
+        u64 flag = 0;
+        if (t >= 0) {
+            w = ld_volatile(status + t);
+            u32 e = static_cast<u32>(w >> 40) & kEpochMask;
+            flag = (w >> kValueBits) & 3;
+            ready = (e == (epoch & kEpochMask)) && flag != 0;
+        } else {
+            flag = kFlagInclusive;  // before tile 0: acts as a zero inclusive prefix
+            w = 0;
+        }
+        // Find the first lane (closest predecessor) that is inclusive; every
+        // lane up to it must be ready.
+        u32 incl = __ballot_sync(0xffffffffu, ready && flag == kFlagInclusive);
+        u32 not_ready = __ballot_sync(0xffffffffu, !ready);
+        u32 first_incl = incl ? (__ffs(incl) - 1) : 32;
+        u32 first_wait = not_ready ? (__ffs(not_ready) - 1) : 32;
+        if (first_wait < first_incl || (first_incl == 32 && first_wait < 32)) {
+            if (++spins > kSpinCap) {
+                if (lane == 0) atomicOr(err, kErrLookbackTimeout);
+                break;
+            }
+            if (spins > 64) __nanosleep(64);
+            continue;
+        }
+        u64 v = (lane <= first_incl && t >= 0) ? (w & kValueMask) : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        exclusive += v;
+        if (first_incl < 32) break;
+        base -= 32;
+    }
+    if (lane == 0) st_volatile(status + tile, make_status(epoch, kFlagInclusive, exclusive + aggregate));
+    return exclusive;
+}
+
+// ---------------------------------------------------------------------------
+// Block-wide exclusive scan of one value per thread (THREADS % 32 == 0).
+// `scratch` holds THREADS/32 + 1 words. Returns the exclusive prefix and
+// writes the block total to *total. Contains __syncthreads().
+// ---------------------------------------------------------------------------
+template <int THREADS, typename T>
+__device__ __forceinline__ T block_exclusive_scan(T value, T* scratch, T* total) {
+    constexpr int kWarps = THREADS / kWarp;
+    const u32 lane = lane_id(), warp = warp_id();
+    T inclusive = value;
+#pragma unroll
+    for (int o = 1; o < kWarp; o <<= 1) {
+        T n = __shfl_up_sync(0xffffffffu, inclusive, o);
+        if (lane >= static_cast<u32>(o)) inclusive += n;
+    }
+    if (lane == kWarp - 1) scratch[warp] = inclusive;
+    __syncthreads();
+    if (warp == 0) {
+        T w = lane < static_cast<u32>(kWarps) ? scratch[lane] : T(0);
+        T wi = w;
+#pragma unroll
+        for (int o = 1; o < kWarp; o <<= 1) {
+            T n = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= static_cast<u32>(o)) wi += n;
+        }
+        if (lane < static_cast<u32>(kWarps)) scratch[lane] = wi - w;
+        if (lane == kWarps - 1) scratch[kWarps] = wi;
+    }
+    __syncthreads();
+    T result = scratch[warp] + inclusive - value;
+    *total = scratch[kWarps];
+    return result;
+}
+
+inline unsigned int ceil_div_u(size_t a, size_t b) { return static_cast<unsigned int>((a + b - 1) / b); }
+
+}  // namespace spk

@@ -1,0 +1,331 @@
+// Sorted-set kernels over lexicographic (first, second) u32 pairs:
+// unique compaction, anti-join (left - right), union (merge + dedup) and the
+// disjoint merge used by the device-resident fixpoint.
+//
+// Reference operators replaced:
+//   distinct's unique + unpack  column_ops.cu:474-481,149-165
+//   anti-join mark/select/gather column_ops.cu:167-227,551-641
+//   union merge/unique/unpack    column_ops.cu:643-775
+//
+// Every output-compacting kernel takes tiles in atomic-counter order, scans
+// its keep flags in the block, gets its global offset from a warp-parallel
+// decoupled look-back, stages the kept rows in shared memory and writes them
+// with coalesced stores. The last tile publishes the output count.
+#pragma once
+
+#include "spk_common.cuh"
+
+namespace spk {
+
+__device__ __forceinline__ u64 pack2(u32 a, u32 b) { return (static_cast<u64>(a) << 32) | b; }
+
+// Number of elements of `a` in the first `diag` merged elements of (a, b),
+// when ties put a's element first: the smallest i with a[i] > b[diag-1-i].
+template <class A, class B>
+__device__ __forceinline__ u64 merge_path(const A& a, u64 na, const B& b, u64 nb, u64 diag) {
+    u64 lo = diag > nb ? diag - nb : 0;
+    u64 hi = diag < na ? diag : na;
+    while (lo < hi) {
+        const u64 mid = (lo + hi) >> 1;
+        if (b(diag - 1 - mid) >= a(mid)) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+struct SoaKeys {
+    const u32* first;
+    const u32* second;
+    __device__ __forceinline__ u64 operator()(u64 i) const { return pack2(first[i], second[i]); }
+};
+struct PackedKeys {
+    const u64* keys;
+    __device__ __forceinline__ u64 operator()(u64 i) const { return keys[i]; }
+};
+struct SmemKeys {
+    const u64* keys;
+    __device__ __forceinline__ u64 operator()(u64 i) const { return keys[i]; }
+};
+
+// lower_bound over [lo, hi) of a sorted accessor.
+template <class A>
+__device__ __forceinline__ u64 lower_bound_keys(const A& a, u64 lo, u64 hi, u64 key) {
+    while (lo < hi) {
+        const u64 mid = (lo + hi) >> 1;
+        if (a(mid) < key) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Galloping lower_bound starting at `from` (known: a(from - 1) < key or from == lo).
+template <class A>
+__device__ __forceinline__ u64 gallop_lower_bound(const A& a, u64 from, u64 hi, u64 key) {
+    u64 step = 1, lo = from, probe = from;
+    while (probe < hi && a(probe) < key) {
+        lo = probe + 1;
+        probe = from + step;
+        step <<= 1;
+    }
+    return lower_bound_keys(a, lo, probe < hi ? probe : hi, key);
+}
+
+template <int THREADS>
+struct CompactShared {
+    u32 scan_scratch[THREADS / kWarp + 1];
+    u64 tile_offset;
+    u64 tile;
+};
+
+// Block scan of per-thread keep counts plus look-back. All threads return
+// the tile's global output offset; *thread_excl gets the thread's prefix and
+// *tile_total the tile's kept count.
+template <int THREADS>
+__device__ __forceinline__ u64 compact_offsets(u32 thread_count, u32* thread_excl, u32* tile_total, u64 tile,
+                                               u64* status, u32 epoch, u32* err, CompactShared<THREADS>& cs) {
+    u32 total;
+    const u32 excl = block_exclusive_scan<THREADS>(thread_count, cs.scan_scratch, &total);
+    if (warp_id() == 0) {
+        const u64 g = warp_lookback_exclusive(status, tile, total, epoch, err);
+        if (lane_id() == 0) cs.tile_offset = g;
+    }
+    __syncthreads();
+    *thread_excl = excl;
+    *tile_total = total;
+    return cs.tile_offset;
+}
+
+// ---------------------------------------------------------------------------
+// Unique + unpack of sorted packed keys (the end of distinct).
+// ---------------------------------------------------------------------------
+template <int THREADS, int ITEMS>
+__global__ void __launch_bounds__(THREADS) unique_unpack_kernel(const u64* buf_a, const u64* buf_b,
+                                                                const u32* final_sel, u64 n, u32* out_first,
+                                                                u32* out_second, u64* out_count, u64* status,
+                                                                u32* tile_counter, u32 epoch, u32* err) {
+    constexpr int kTile = THREADS * ITEMS;
+    __shared__ CompactShared<THREADS> cs;
+    __shared__ u64 stage[kTile];
+    const u64* keys = (final_sel && *final_sel) ? buf_b : buf_a;
+    const u64 num_tiles = (n + kTile - 1) / kTile;
+    for (;;) {
+        if (threadIdx.x == 0) cs.tile = atomicAdd(tile_counter, 1u);
+        __syncthreads();
+        const u64 tile = cs.tile;
+        if (tile >= num_tiles) break;
+        const u64 base = tile * kTile + static_cast<u64>(threadIdx.x) * ITEMS;
+        u64 v[ITEMS];
+        u32 keep = 0, count = 0;
+        u64 prev = (base > 0 && base - 1 < n) ? keys[base - 1] : 0;
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i) {
+            const u64 idx = base + i;
+            const bool valid = idx < n;
+            v[i] = valid ? keys[idx] : 0;
+            const bool k = valid && (idx == 0 || v[i] != prev);
+            prev = v[i];
+            keep |= (k ? 1u : 0u) << i;
+            count += k;
+        }
+        u32 excl, total;
+        const u64 off = compact_offsets<THREADS>(count, &excl, &total, tile, status, epoch, err, cs);
+        u32 w = excl;
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i)
+            if (keep & (1u << i)) stage[w++] = v[i];
+        __syncthreads();
+        for (u32 j = threadIdx.x; j < total; j += THREADS) {
+            const u64 k = stage[j];
+            out_first[off + j] = static_cast<u32>(k >> 32);
+            out_second[off + j] = static_cast<u32>(k);
+        }
+        if (tile == num_tiles - 1 && threadIdx.x == 0) *out_count = off + total;
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Anti-join over SoA columns: stable left - right (the reference's
+// SortedBinaryAntiJoin), with the reference's side outputs: flags[row] is 1
+// for kept rows, selected[] lists kept row ids, *selected_rows their count.
+// ---------------------------------------------------------------------------
+template <int THREADS, int ITEMS>
+__global__ void __launch_bounds__(THREADS) anti_join_soa_kernel(const u32* lf, const u32* ls, u64 ln, const u32* rf,
+                                                                const u32* rs, u64 rn, u32* flags, u32* selected,
+                                                                u32* selected_rows, u32* out_first, u32* out_second,
+                                                                u64* status, u32* tile_counter, u32 epoch, u32* err) {
+    constexpr int kTile = THREADS * ITEMS;
+    __shared__ CompactShared<THREADS> cs;
+    __shared__ u32 stage_row[kTile];
+    __shared__ u64 range[2];
+    const SoaKeys right{rf, rs};
+    const u64 num_tiles = (ln + kTile - 1) / kTile;
+    for (;;) {
+        if (threadIdx.x == 0) cs.tile = atomicAdd(tile_counter, 1u);
+        __syncthreads();
+        const u64 tile = cs.tile;
+        if (tile >= num_tiles) break;
+        const u64 tile_begin = tile * kTile;
+        const u64 tile_end = tile_begin + kTile < ln ? tile_begin + kTile : ln;
+        // Narrow the right range once per tile: [lb(first), lb(last)+1 bound).
+        if (threadIdx.x == 0) range[0] = lower_bound_keys(right, 0, rn, pack2(lf[tile_begin], ls[tile_begin]));
+        if (threadIdx.x == kWarp) {
+            const u64 last = pack2(lf[tile_end - 1], ls[tile_end - 1]);
+            u64 hi = lower_bound_keys(right, 0, rn, last);
+            range[1] = hi < rn ? hi + 1 : rn;
+        }
+        __syncthreads();
+        // lower_bound is monotone in the key, so any key between the tile's
+        // first and last keys has its lower bound inside [r_lo, r_hi); keys
+        // outside that span (an unsorted left input, which the reference's
+        // per-row binary search also accepts) search the whole right input.
+        const u64 r_lo = range[0], r_hi = range[1] > range[0] ? range[1] : range[0];
+        const u64 t_first = pack2(lf[tile_begin], ls[tile_begin]);
+        const u64 t_last = pack2(lf[tile_end - 1], ls[tile_end - 1]);
+        const u64 base = tile_begin + static_cast<u64>(threadIdx.x) * ITEMS;
+        u32 keep = 0, count = 0;
+        u64 cursor = r_lo, prev_key = 0;
+        bool have_cursor = false;
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i) {
+            const u64 idx = base + i;
+            if (idx < ln) {
+                const u64 key = pack2(lf[idx], ls[idx]);
+                u64 hi_bound = rn;
+                if (key >= t_first && key <= t_last) {
+                    hi_bound = r_hi;
+                    cursor = (have_cursor && key >= prev_key) ? gallop_lower_bound(right, cursor, r_hi, key)
+                                                              : lower_bound_keys(right, r_lo, r_hi, key);
+                    have_cursor = true;
+                } else {
+                    cursor = lower_bound_keys(right, 0, rn, key);
+                    have_cursor = false;
+                }
+                prev_key = key;
+                const bool matched = cursor < hi_bound && right(cursor) == key;
+                flags[idx] = matched ? 0u : 1u;
+                if (!matched) {
+                    keep |= 1u << i;
+                    ++count;
+                }
+            }
+        }
+        (void)cursor;
+        u32 excl, total;
+        const u64 off = compact_offsets<THREADS>(count, &excl, &total, tile, status, epoch, err, cs);
+        u32 w = excl;
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i)
+            if (keep & (1u << i)) stage_row[w++] = static_cast<u32>(base + i);
+        __syncthreads();
+        for (u32 j = threadIdx.x; j < total; j += THREADS) {
+            const u32 row = stage_row[j];
+            selected[off + j] = row;
+            out_first[off + j] = lf[row];
+            out_second[off + j] = ls[row];
+        }
+        if (tile == num_tiles - 1 && threadIdx.x == 0) *selected_rows = static_cast<u32>(off + total);
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Union over SoA columns: merge-path partitioned merge of two sorted inputs
+// with duplicate removal, unpacked into two output columns.
+// ---------------------------------------------------------------------------
+template <int THREADS, int ITEMS>
+__global__ void __launch_bounds__(THREADS) union_soa_kernel(const u32* lf, const u32* ls, u64 ln, const u32* rf,
+                                                            const u32* rs, u64 rn, u32* out_first, u32* out_second,
+                                                            u64* out_count, u64* status, u32* tile_counter, u32 epoch,
+                                                            u32* err) {
+    constexpr int kTile = THREADS * ITEMS;
+    __shared__ CompactShared<THREADS> cs;
+    __shared__ u64 sm[kTile + 2];
+    __shared__ u64 split[2];
+    __shared__ u64 tile_prev;
+    __shared__ int has_prev;
+    const SoaKeys a{lf, ls}, b{rf, rs};
+    const u64 total_in = ln + rn;
+    const u64 num_tiles = (total_in + kTile - 1) / kTile;
+    for (;;) {
+        if (threadIdx.x == 0) cs.tile = atomicAdd(tile_counter, 1u);
+        __syncthreads();
+        const u64 tile = cs.tile;
+        if (tile >= num_tiles) break;
+        const u64 d0 = tile * kTile;
+        const u64 d1 = d0 + kTile < total_in ? d0 + kTile : total_in;
+        if (threadIdx.x == 0) {
+            const u64 i0 = merge_path(a, ln, b, rn, d0);
+            split[0] = i0;
+            const u64 j0 = d0 - i0;
+            u64 p = 0;
+            int hp = 0;
+            if (i0 > 0) { p = a(i0 - 1); hp = 1; }
+            if (j0 > 0) { const u64 q = b(j0 - 1); p = hp ? (q > p ? q : p) : q; hp = 1; }
+            tile_prev = p;
+            has_prev = hp;
+        }
+        if (threadIdx.x == kWarp) split[1] = merge_path(a, ln, b, rn, d1);
+        __syncthreads();
+        const u64 i0 = split[0], i1 = split[1];
+        const u64 j0 = d0 - i0, j1 = d1 - i1;
+        const u32 na = static_cast<u32>(i1 - i0), nb = static_cast<u32>(j1 - j0);
+        for (u32 t = threadIdx.x; t < na; t += THREADS) sm[t] = a(i0 + t);
+        for (u32 t = threadIdx.x; t < nb; t += THREADS) sm[na + t] = b(j0 + t);
+        __syncthreads();
+        const SmemKeys sa{sm}, sb{sm + na};
+        const u32 diag = threadIdx.x * ITEMS;
+        const u32 len = d1 - d0 > diag ? static_cast<u32>(d1 - d0 - diag) : 0u;
+        u64 v[ITEMS];
+        u32 keep = 0, count = 0;
+        if (len > 0) {
+            u32 ia = static_cast<u32>(merge_path(sa, na, sb, nb, diag));
+            u32 ib = diag - ia;
+            u64 prev;
+            bool hp;
+            if (diag == 0) {
+                prev = tile_prev;
+                hp = has_prev != 0;
+            } else {
+                const u64 pa = ia > 0 ? sa(ia - 1) : 0, pb = ib > 0 ? sb(ib - 1) : 0;
+                prev = ia == 0 ? pb : (ib == 0 ? pa : (pa > pb ? pa : pb));
+                hp = true;
+            }
+#pragma unroll
+            for (int i = 0; i < ITEMS; ++i) {
+                if (static_cast<u32>(i) < len) {
+                    u64 x;
+                    if (ib >= nb || (ia < na && sa(ia) <= sb(ib))) x = sa(ia++);
+                    else x = sb(ib++);
+                    v[i] = x;
+                    const bool k = !hp || x != prev;
+                    prev = x;
+                    hp = true;
+                    if (k) {
+                        keep |= 1u << i;
+                        ++count;
+                    }
+                } else {
+                    v[i] = 0;
+                }
+            }
+        }
+        __syncthreads();  // sm is reused as the output stage
+        u32 excl, total;
+        const u64 off = compact_offsets<THREADS>(count, &excl, &total, tile, status, epoch, err, cs);
+        u32 w = excl;
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i)
+            if (keep & (1u << i)) sm[w++] = v[i];
+        __syncthreads();
+        for (u32 j = threadIdx.x; j < total; j += THREADS) {
+            const u64 k = sm[j];
+            out_first[off + j] = static_cast<u32>(k >> 32);
+            out_second[off + j] = static_cast<u32>(k);
+        }
+        if (tile == num_tiles - 1 && threadIdx.x == 0) *out_count = off + total;
+        __syncthreads();
+    }
+}
+
+}  // namespace spk

@@ -1,0 +1,235 @@
+"""Semi-naive fixpoint orchestration on the device (Tier B of the C ABI).
+
+Mirrors crates/sparkalog-recursion/src/generic.rs: ``RelationStore``
+(:16-121), ``RecursiveExecutor::{compile, run}`` (:407-525), ``SccSummary``
+(:536-542), the ``GenericExecutionError`` / ``RelationStoreError`` variants and
+``transitive_closure_scc`` (:629-661). The store keeps every relation resident
+on the GPU; only explicit reads copy rows back.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _native
+from .relational import (BinaryEqualityJoin, JoinInput, JoinProjection, RecursiveRulePlan, RecursiveSccPlan,
+                         RelationId, path_join)
+
+HOST, DEVICE = 0, 1
+FULL, DELTA = 0, 1
+
+
+class GenericExecutionError(RuntimeError):
+    """Errors of RecursiveExecutor and RelationStore; ``kind`` names the reference's variant."""
+
+    KINDS = {
+        -1: "Missing", -2: "Duplicate", -3: "NotRecursive", -4: "EmptyScc", -5: "DuplicateSccRelation",
+        -6: "DeltaOutsideScc", -7: "TargetOutsideScc", -8: "IncompatibleTargetPlans", -9: "MissingRuleTarget",
+        -10: "IterationLimit", -11: "TooManyRows", -12: "MissingPlanColumn", -20: "DeviceFault",
+        -21: "InvalidArgument", -22: "UnsortedFull",
+    }
+
+    def __init__(self, code: int, message: str):
+        self.code = code
+        self.kind = self.KINDS.get(code, "Cuda" if code > 0 else f"Error{code}")
+        super().__init__(f"{self.kind}: {message}")
+
+
+RelationStoreError = GenericExecutionError
+
+
+def _check(code: int) -> None:
+    if code != 0:
+        raise GenericExecutionError(code, _native.last_error())
+
+
+def _u32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.uint32))
+
+
+@dataclass
+class SccSummary:
+    """SccSummary (generic.rs:536-542); every operator runs on the GPU, so placements are omitted."""
+
+    iterations: int
+    total_new_rows: int
+    relation_rows: list[tuple[RelationId, int]]
+
+
+class RelationStore:
+    """Device-resident FULL/DELTA/NEWT buffers per relation (generic.rs:16-121)."""
+
+    def __init__(self, stream: torch.cuda.Stream | None = None):
+        L = _native.load()
+        self._stream = stream if stream is not None else torch.cuda.current_stream()
+        h = ctypes.c_void_p()
+        _check(L.sparkalog_store_create(self._stream.cuda_stream, ctypes.byref(h)))
+        self._h = h
+
+    def close(self) -> None:
+        h, self._h = getattr(self, "_h", None), None
+        if h:
+            _native.load().sparkalog_store_destroy(h)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    @staticmethod
+    def _columns(relation):
+        """Accepts (first, second) host arrays or device tensors; returns (p0, p1, rows, location, keep)."""
+        first, second = relation
+        if isinstance(first, torch.Tensor) and first.is_cuda:
+            if first.dtype not in (torch.int32, torch.uint32) or not first.is_contiguous():
+                raise ValueError("device columns must be contiguous 32-bit tensors")
+            return first.data_ptr(), second.data_ptr(), int(first.numel()), DEVICE, (first, second)
+        a, b = _u32(first), _u32(second)
+        if len(a) != len(b):
+            raise ValueError("column lengths differ")
+        return a.ctypes.data, b.ctypes.data, len(a), HOST, (a, b)
+
+    def insert_static(self, rid: RelationId | int, relation) -> None:
+        """RelationStore::insert_static (generic.rs:36-51)."""
+        p0, p1, n, loc, keep = self._columns(relation)
+        _check(_native.load().sparkalog_store_insert_static(self._h, int(getattr(rid, "value", rid)), p0, p1, n, loc))
+        del keep
+
+    def insert_recursive(self, rid: RelationId | int, full, delta) -> None:
+        """RelationStore::insert_recursive (generic.rs:53-79)."""
+        f0, f1, fn, loc, keep_f = self._columns(full)
+        d0, d1, dn, loc_d, keep_d = self._columns(delta)
+        if loc != loc_d:
+            raise ValueError("FULL and DELTA must both be host arrays or both device tensors")
+        _check(_native.load().sparkalog_store_insert_recursive(self._h, int(getattr(rid, "value", rid)), f0, f1, fn,
+                                                               d0, d1, dn, loc))
+        del keep_f, keep_d
+
+    def rows(self, rid: RelationId | int, version: int = FULL) -> int:
+        n = ctypes.c_size_t(0)
+        _check(_native.load().sparkalog_store_rows(self._h, int(getattr(rid, "value", rid)), version, ctypes.byref(n)))
+        return int(n.value)
+
+    def _read(self, rid, version: int) -> tuple[np.ndarray, np.ndarray]:
+        n = self.rows(rid, version)
+        a = np.empty(max(n, 1), dtype=np.uint32)
+        b = np.empty(max(n, 1), dtype=np.uint32)
+        _check(_native.load().sparkalog_store_read(self._h, int(getattr(rid, "value", rid)), version, a.ctypes.data,
+                                                   b.ctypes.data, HOST))
+        return a[:n], b[:n]
+
+    def full(self, rid: RelationId | int) -> tuple[np.ndarray, np.ndarray]:
+        """RelationStore::full (generic.rs:81-83), copied to the host as two columns."""
+        return self._read(rid, FULL)
+
+    def delta(self, rid: RelationId | int) -> tuple[np.ndarray, np.ndarray]:
+        """RelationStore::delta (generic.rs:85-91)."""
+        return self._read(rid, DELTA)
+
+    def read_into(self, rid: RelationId | int, version: int, first, second) -> int:
+        """Copies FULL/DELTA into caller buffers (numpy host arrays, possibly pinned, or device tensors)."""
+        n = self.rows(rid, version)
+        if isinstance(first, torch.Tensor) and first.is_cuda:
+            p0, p1, loc = first.data_ptr(), second.data_ptr(), DEVICE
+        elif isinstance(first, torch.Tensor):
+            p0, p1, loc = first.data_ptr(), second.data_ptr(), HOST
+        else:
+            p0, p1, loc = first.ctypes.data, second.ctypes.data, HOST
+        _check(_native.load().sparkalog_store_read(self._h, int(getattr(rid, "value", rid)), version, p0, p1, loc))
+        return n
+
+
+def _rule_c(rule: RecursiveRulePlan) -> _native.RulePlanC:
+    c = _native.RulePlanC()
+    c.target = rule.target.value
+    c.delta_input = rule.delta_input.value
+    c.right_input = rule.right_input.value
+    c.left_key = rule.join.left_key
+    c.right_key = rule.join.right_key
+    for j, p in enumerate(rule.join.output):
+        c.proj_side[j] = int(p.input)
+        c.proj_col[j] = p.column
+    c.distinct_cols[:] = list(rule.distinct.columns)
+    c.anti_left[:] = list(rule.anti_join.left)
+    c.anti_right[:] = list(rule.anti_join.right)
+    c.union_left[:] = list(rule.union.left)
+    c.union_right[:] = list(rule.union.right)
+    return c
+
+
+class RecursiveExecutor:
+    """RecursiveExecutor (generic.rs:400-525)."""
+
+    def __init__(self, handle: ctypes.c_void_p, plan: RecursiveSccPlan):
+        self._h = handle
+        self.plan = plan
+
+    @classmethod
+    def compile(cls, plan: RecursiveSccPlan, store: RelationStore) -> "RecursiveExecutor":
+        """RecursiveExecutor::compile (generic.rs:407-470)."""
+        rel = _u32([r.value for r in plan.relations])
+        rules = (_native.RulePlanC * max(len(plan.rules), 1))(*[_rule_c(r) for r in plan.rules])
+        h = ctypes.c_void_p()
+        _check(_native.load().sparkalog_executor_compile(store.handle, rel.ctypes.data_as(_native.c_u32p), len(rel),
+                                                         rules, len(plan.rules), ctypes.byref(h)))
+        return cls(h, plan)
+
+    def close(self) -> None:
+        h, self._h = getattr(self, "_h", None), None
+        if h:
+            _native.load().sparkalog_executor_destroy(h)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, store: RelationStore, max_iterations: int = 10_000) -> SccSummary:
+        """RecursiveExecutor::run (generic.rs:472-516): loops while any DELTA of the SCC is
+        non-empty and counts every executed round."""
+        n = len(self.plan.relations)
+        ids = (ctypes.c_uint32 * max(n, 1))()
+        rows = (ctypes.c_uint64 * max(n, 1))()
+        s = _native.SccSummaryC()
+        s.relation_count = n
+        s.relation_ids = ids
+        s.relation_rows = rows
+        _check(_native.load().sparkalog_executor_run(self._h, store.handle, max_iterations, ctypes.byref(s)))
+        return SccSummary(int(s.iterations), int(s.total_new_rows),
+                          [(RelationId(int(ids[i])), int(rows[i])) for i in range(n)])
+
+
+    def set_profiling(self, enable: bool) -> None:
+        """Times every kernel class with CUDA events on the store's stream."""
+        _check(_native.load().sparkalog_executor_set_profiling(self._h, 1 if enable else 0))
+
+    def stats(self, reset: bool = False) -> dict:
+        """Per-kernel-class launches, milliseconds and algorithmic bytes, plus total launches."""
+        s = _native.KernelStatsC()
+        _check(_native.load().sparkalog_executor_stats(self._h, ctypes.byref(s), 1 if reset else 0))
+        classes = {name: {"launches": int(s.launches[i]), "ms": float(s.milliseconds[i]),
+                          "bytes": float(s.bytes[i])} for i, name in enumerate(_native.KERNEL_CLASSES)}
+        return {"classes": classes, "total_launches": int(s.total_launches), "rounds": int(s.rounds)}
+
+
+def transitive_closure_scc(path: RelationId, edge: RelationId) -> RecursiveSccPlan:
+    """transitive_closure_scc (generic.rs:629-661)."""
+    return RecursiveSccPlan(relations=[path],
+                            rules=[RecursiveRulePlan(target=path, delta_input=path, right_input=edge,
+                                                     join=path_join())])
+
+
+__all__ = [
+    "GenericExecutionError", "RelationStoreError", "RelationStore", "RecursiveExecutor", "SccSummary",
+    "transitive_closure_scc", "BinaryEqualityJoin", "JoinInput", "JoinProjection", "FULL", "DELTA",
+]

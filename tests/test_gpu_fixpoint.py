@@ -1,0 +1,205 @@
+"""GPU parity of the device-resident fixpoint (Tier B) against the oracle.
+
+Mirrors crates/sparkalog-recursion/src/generic.rs:716-946 and
+crates/sparkalog-datalog/src/subset.rs:475-497: FULL of every SCC relation
+and the per-SCC iteration count must match bit for bit.
+"""
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import cols, pairs
+from sparkalog_b200 import generators
+
+pytestmark = pytest.mark.gpu
+
+
+def rec():
+    from sparkalog_b200 import recursion
+
+    return recursion
+
+
+def plan_for(case):
+    from sparkalog_b200.relational import RecursiveRulePlan, RecursiveSccPlan, RelationId, path_join
+
+    rules = [RecursiveRulePlan(RelationId(r["target"]), RelationId(r["delta_input"]), RelationId(r["right_input"]),
+                               path_join()) for r in case["rules"]]
+    return RecursiveSccPlan([RelationId(r) for r in case["scc"]], rules)
+
+
+def test_fixpoint_known_answers(cuda, known_answers):
+    R = rec()
+    for case in known_answers["fixpoint"]:
+        store = R.RelationStore()
+        for rid, rows in case["relations"].items():
+            store.insert_static(int(rid), cols(rows))
+        for rid, fd in case["recursive"].items():
+            store.insert_recursive(int(rid), cols(fd["full"]), cols(fd["delta"]))
+        ex = R.RecursiveExecutor.compile(plan_for(case), store)
+        summary = ex.run(store, 16)
+        if "iterations" in case:
+            assert summary.iterations == case["iterations"], case["source"]
+        if "total_new_rows" in case:
+            assert summary.total_new_rows == case["total_new_rows"], case["source"]
+        for rid, rows in case["full"].items():
+            assert pairs(store.full(int(rid))) == rows, case["source"]
+            assert store.rows(int(rid), R.DELTA) == 0
+        assert [(r.value, n) for r, n in summary.relation_rows] == [
+            (int(rid), len(case["full"][str(rid)])) for rid in case["scc"]]
+
+
+def test_incompatible_plans_rejected(cuda):
+    # generic.rs:917-946
+    R = rec()
+    from sparkalog_b200.relational import SortedBinaryUnion
+
+    store = R.RelationStore()
+    store.insert_static(0, cols([[1, 2]]))
+    store.insert_recursive(1, cols([[1, 2]]), cols([[1, 2]]))
+    plan = plan_for({"scc": [1], "rules": [{"target": 1, "delta_input": 1, "right_input": 0}] * 2})
+    plan.rules[1].union = SortedBinaryUnion(left=(0, 1), right=(1, 0))
+    with pytest.raises(R.GenericExecutionError) as err:
+        R.RecursiveExecutor.compile(plan, store)
+    assert err.value.kind == "IncompatibleTargetPlans"
+
+
+def test_iteration_limit_and_store_errors(cuda):
+    R = rec()
+    store = R.RelationStore()
+    e = cols([[i, i + 1] for i in range(10)])
+    store.insert_static(0, e)
+    store.insert_recursive(1, e, e)
+    with pytest.raises(R.GenericExecutionError) as err:
+        store.insert_static(0, e)
+    assert err.value.kind == "Duplicate"
+    with pytest.raises(R.GenericExecutionError) as err:
+        store.rows(7)
+    assert err.value.kind == "Missing"
+    ex = R.RecursiveExecutor.compile(R.transitive_closure_scc(*map(_rid, (1, 0))), store)
+    with pytest.raises(R.GenericExecutionError) as err:
+        ex.run(store, 3)
+    assert err.value.kind == "IterationLimit"
+
+
+def _rid(v):
+    from sparkalog_b200.relational import RelationId
+
+    return RelationId(v)
+
+
+@pytest.mark.parametrize("n", [2, 3, 17, 512])
+def test_chain_closure(cuda, n):
+    # tc-fixpoint.rs:118-154
+    R = rec()
+    src = np.arange(n - 1, dtype=np.uint32)
+    store = R.RelationStore()
+    store.insert_static(0, (src, src + 1))
+    store.insert_recursive(1, (src, src + 1), (src, src + 1))
+    summary = R.RecursiveExecutor.compile(R.transitive_closure_scc(_rid(1), _rid(0)), store).run(store, 1024)
+    assert store.rows(1) == n * (n - 1) // 2
+    assert store.rows(1, R.DELTA) == 0
+    assert summary.iterations == n - 1
+
+
+def run_tc_gpu(src, dst, max_iterations=10_000):
+    R = rec()
+    e0, e1 = oracle.btree_pairs(src, dst)
+    store = R.RelationStore()
+    store.insert_static(0, (e0, e1))
+    store.insert_recursive(1, (e0, e1), (e0, e1))
+    summary = R.RecursiveExecutor.compile(R.transitive_closure_scc(_rid(1), _rid(0)), store).run(store,
+                                                                                                 max_iterations)
+    return store.full(1), summary
+
+
+@pytest.mark.parametrize("n,e,seed", [(40, 60, 9), (2000, 8000, 1), (5000, 4500, 2), (300_000, 262_500, 6),
+                                      (1_000, 1_000, 7)])
+def test_tc_matches_oracle(cuda, n, e, seed):
+    src, dst = generators.er_edges(n, e, seed)
+    (p0, p1), summary = run_tc_gpu(src, dst)
+    (w0, w1), it, new = oracle.transitive_closure(src, dst, threads=8)
+    assert summary.iterations == it
+    assert summary.total_new_rows == new
+    assert np.array_equal(p0, w0) and np.array_equal(p1, w1)
+
+
+def test_tc_seed_with_duplicates_and_unsorted_delta(cuda):
+    # FULL may hold duplicates (the first union removes them) and DELTA's
+    # order does not matter: distinct sorts the join output.
+    R = rec()
+    e0, e1 = cols([[1, 2], [2, 3], [3, 4], [4, 5], [5, 6]])
+    full = cols([[1, 2], [1, 2], [2, 3], [3, 4], [4, 5], [5, 6]])
+    delta = cols([[5, 6], [1, 2], [3, 4], [2, 3], [4, 5]])
+    store = R.RelationStore()
+    store.insert_static(0, (e0, e1))
+    store.insert_recursive(1, full, delta)
+    summary = R.RecursiveExecutor.compile(R.transitive_closure_scc(_rid(1), _rid(0)), store).run(store)
+    st = oracle.Store()
+    st.insert_static(0, (e0, e1))
+    st.insert_recursive(1, full, delta)
+    it, new = st.run_scc([1], [oracle.tc_rule(1, 0)])
+    assert summary.iterations == it and summary.total_new_rows == new
+    assert pairs(store.full(1)) == pairs(st.full(1))
+
+
+def test_join_on_second_column_and_right_projection(cuda):
+    # A rule keyed on the right relation's second column, projecting (R.0, L.1):
+    # p(z, y) :- p(x, y), e(z, x). Exercises the sorted (key, row) index path.
+    from sparkalog_b200.relational import (BinaryEqualityJoin, JoinInput, JoinProjection, RecursiveRulePlan,
+                                           RecursiveSccPlan)
+
+    R = rec()
+    src, dst = generators.er_edges(3000, 3300, 21)
+    e0, e1 = oracle.btree_pairs(src, dst)
+    join = BinaryEqualityJoin(0, 1, (JoinProjection(JoinInput.RIGHT, 0), JoinProjection(JoinInput.LEFT, 1)))
+    plan = RecursiveSccPlan([_rid(1)], [RecursiveRulePlan(_rid(1), _rid(1), _rid(0), join)])
+    store = R.RelationStore()
+    store.insert_static(0, (e0, e1))
+    store.insert_recursive(1, (e0, e1), (e0, e1))
+    summary = R.RecursiveExecutor.compile(plan, store).run(store)
+    st = oracle.Store()
+    st.insert_static(0, (e0, e1))
+    st.insert_recursive(1, (e0, e1), (e0, e1))
+    it, new = st.run_scc([1], [oracle.rule_plan(1, 1, 0, left_key=0, right_key=1, projection=((1, 0), (0, 1)))])
+    assert summary.iterations == it and summary.total_new_rows == new
+    assert pairs(store.full(1)) == pairs(st.full(1))
+
+
+def test_execute_binary_source_program(cuda, known_answers):
+    # subset.rs:475-497 (value ids interned by first appearance).
+    from sparkalog_b200.datalog import BinaryProgramPlan, BinarySccPlan, BinarySeedPlan, execute_binary
+    from sparkalog_b200.recursion import transitive_closure_scc
+
+    case = known_answers["source_program"]
+    vid = {int(k): v for k, v in case["value_ids"].items()}
+    edge, path = _rid(0), _rid(1)
+    plan = BinaryProgramPlan(
+        predicate_count=2,
+        facts=[(edge, (vid[a], vid[b])) for a, b in [(1, 2), (2, 3), (3, 4)]],
+        recursive_sccs=[BinarySccPlan(transitive_closure_scc(path, edge), [BinarySeedPlan(path, edge, (0, 1))])],
+        outputs=[path],
+    )
+    result = execute_binary(plan, 16)
+    assert result.summaries[0].iterations == case["iterations"]
+    assert pairs(result.store.full(1)) == case["path_value_ids"]
+
+
+def test_device_inputs_and_reads(cuda):
+    R = rec()
+    torch = cuda
+    src, dst = generators.er_edges(20_000, 17_500, 3)
+    d0 = torch.from_numpy(src.view(np.int32)).cuda()
+    d1 = torch.from_numpy(dst.view(np.int32)).cuda()
+    store = R.RelationStore()
+    store.insert_static(0, (d0, d1))
+    store.insert_recursive(1, (d0, d1), (d0, d1))
+    R.RecursiveExecutor.compile(R.transitive_closure_scc(_rid(1), _rid(0)), store).run(store)
+    n = store.rows(1)
+    o0 = torch.empty(n, dtype=torch.int32, device="cuda")
+    o1 = torch.empty(n, dtype=torch.int32, device="cuda")
+    store.read_into(1, R.FULL, o0, o1)
+    (w0, w1), _, _ = oracle.transitive_closure(src, dst, threads=8)
+    assert np.array_equal(o0.cpu().numpy().view(np.uint32), w0)
+    assert np.array_equal(o1.cpu().numpy().view(np.uint32), w1)
