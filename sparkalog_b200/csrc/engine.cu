@@ -101,6 +101,16 @@ struct DevArray {
         return cudaSuccess;
     }
 
+    // Like ensure(), but a fresh allocation is zero-filled. Decoupled
+    // look-back status buffers must start zeroed: pool memory recycled from
+    // relation rows can otherwise decode as a published status word.
+    cudaError_t ensure_zeroed(size_t need, cudaStream_t s) {
+        if (need <= bytes && ptr) return cudaSuccess;
+        cudaError_t st = ensure(need, s);
+        if (st != cudaSuccess) return st;
+        return cudaMemsetAsync(ptr, 0, bytes, s);
+    }
+
     void release(cudaStream_t s) {
         if (ptr) cudaFreeAsync(ptr, s);
         ptr = nullptr;
@@ -320,7 +330,7 @@ namespace {
 int radix_sort(u64* a, u64* b, const u64* n_dev, u64 n_host_bound, SortScratch& sc, sparkalog_executor* ex,
                u32* err, cudaStream_t s, int* hist_timing, int* pass_timing) {
     SPK_CUDA(sc.plan.ensure(sizeof(spk::RadixPlan), s), "cudaMallocAsync");
-    SPK_CUDA(sc.status.ensure(spk::radix_status_words(n_host_bound) * 8, s), "cudaMallocAsync");
+    SPK_CUDA(sc.status.ensure_zeroed(spk::radix_status_words(n_host_bound) * 8, s), "cudaMallocAsync");
     spk::RadixPlan* plan = sc.plan.as<spk::RadixPlan>();
     const int th = ex->begin(SPARKALOG_K_SORT_HIST, s);
     SPK_CUDA(cudaMemsetAsync(plan, 0, spk::kRadixPlanClearBytes, s), "cudaMemsetAsync");
@@ -747,7 +757,7 @@ int sparkalog_executor_run(sparkalog_executor* ex, sparkalog_store* st, size_t m
             if (r.has_dups && r.level_n[0] > 0) {
                 const u64 n = r.level_n[0];
                 SPK_CUDA(r.spare.ensure(n * 8, s), "cudaMallocAsync");
-                SPK_CUDA(ex->status.ensure(((n + kSetTile - 1) / kSetTile + 1) * 8, s), "cudaMallocAsync");
+                SPK_CUDA(ex->status.ensure_zeroed(((n + kSetTile - 1) / kSetTile + 1) * 8, s), "cudaMallocAsync");
                 SPK_CUDA(cudaMemsetAsync(counters, 0, kCounterWords * 4, s), "cudaMemsetAsync");
                 SPK_CUDA(cudaMemsetAsync(counts, 0, 8, s), "cudaMemsetAsync");
                 // unique over the packed run: anti-join against no levels.
@@ -842,7 +852,7 @@ int sparkalog_executor_run(sparkalog_executor* ex, sparkalog_store* st, size_t m
                 SPK_CUDA(st->find(t.id)->newt.ensure(t.j_cap * 8, s), "cudaMallocAsync");
                 max_status_words = std::max<size_t>(max_status_words, (t.j_cap + kSetTile - 1) / kSetTile + 1);
             }
-            SPK_CUDA(ex->status.ensure(max_status_words * 8, s), "cudaMallocAsync");
+            SPK_CUDA(ex->status.ensure_zeroed(max_status_words * 8, s), "cudaMallocAsync");
             SPK_CUDA(cudaMemsetAsync(counters, 0, (kCounterWords + 1) * 4, s), "cudaMemsetAsync");
             SPK_CUDA(cudaMemsetAsync(counts, 0, ex->counts_words * 8, s), "cudaMemsetAsync");
             size_t counter_slot = 0;
