@@ -101,6 +101,23 @@ SPARKALOG_API int sparkalog_union_u32(const uint32_t* left_first, const uint32_t
                                       uint64_t* unique_rows, uint32_t* output_first, uint32_t* output_second,
                                       void* temporary, size_t temporary_bytes, void* stream);
 
+/* sparkalog_anti_join_u32 without the `temporary` buffer, for callers that
+ * cannot allocate device memory (a runtime whose HBM budget is fully handed to
+ * relation buffers, a binding with no device allocator, a pipeline that must
+ * not take cudaMalloc's implicit synchronisation). No counterpart in the
+ * reference. The kernel's scratch is a fixed static array in the library
+ * (about 513 KiB per device, kept until exit), shared by every call on a
+ * device: calls that overlap on the GPU race, so order them on one stream.
+ * left_rows above SPARKALOG_ANTI_JOIN_NO_ALLOC_MAX_LEFT_ROWS is rejected with
+ * cudaErrorInvalidValue. The first call on a device looks up the array's
+ * address; make it before any stream capture. Allocates nothing. */
+#define SPARKALOG_ANTI_JOIN_NO_ALLOC_MAX_LEFT_ROWS (1ull << 27)
+SPARKALOG_API int sparkalog_anti_join_u32_no_alloc(const uint32_t* left_first, const uint32_t* left_second,
+                                                   size_t left_rows, const uint32_t* right_first,
+                                                   const uint32_t* right_second, size_t right_rows, uint32_t* flags,
+                                                   uint32_t* selected, uint32_t* selected_rows,
+                                                   uint32_t* output_first, uint32_t* output_second, void* stream);
+
 /* Asynchronous error bits of this device's Tier A kernels (a decoupled
  * look-back that hit its spin cap). No counterpart in the reference, whose
  * CUB kernels have no such wait. reset != 0 clears the bits. */

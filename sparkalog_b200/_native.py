@@ -29,6 +29,7 @@ TIER_A = [
     "sparkalog_anti_join_u32",
     "sparkalog_union_u32_temporary_bytes",
     "sparkalog_union_u32",
+    "sparkalog_anti_join_u32_no_alloc",
     "sparkalog_b200_device_error",
 ]
 TIER_B = [
@@ -123,6 +124,8 @@ def load() -> ctypes.CDLL:
                                                       vp]
     L.sparkalog_union_u32.argtypes = [vp, vp, ctypes.c_size_t, vp, vp, ctypes.c_size_t, vp, vp, vp, vp, vp, vp, vp,
                                       vp, ctypes.c_size_t, vp]
+    L.sparkalog_anti_join_u32_no_alloc.argtypes = [vp, vp, ctypes.c_size_t, vp, vp, ctypes.c_size_t, vp, vp, vp,
+                                                   vp, vp, vp]
     L.sparkalog_b200_device_error.argtypes = [c_u32p, i]
     for name in TIER_A:
         getattr(L, name).restype = i

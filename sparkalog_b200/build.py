@@ -21,6 +21,7 @@ INCLUDE_DIR = PACKAGE_DIR.parent / "include"
 
 SOURCES = [
     "abi_operators.cu",
+    "abi_no_alloc.cu",
     "engine.cu",
 ]
 
