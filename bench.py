@@ -62,6 +62,10 @@ def parse_args():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--workload", choices=sorted(WORKLOADS), default="er_16m_14_68m")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--fixpoint-only", action="store_true",
+                   help="run warmup + steps fixpoints and print a summary (for profilers; no JSON contract line)")
+    p.add_argument("--nodes", type=int, default=None, help="override the workload's node count (profiling)")
+    p.add_argument("--edges", type=int, default=None, help="override the workload's edge count (profiling)")
     return p.parse_args()
 
 
@@ -199,6 +203,8 @@ def run_ours(args):
     from sparkalog_b200.relational import RelationId
 
     nodes, edges, seed = WORKLOADS[args.workload]
+    nodes = args.nodes or nodes
+    edges = args.edges or edges
     src, dst = generators.er_edges(nodes, edges, seed)
     ps, pd = partition(src, dst, nodes, rank, world)
     stream = torch.cuda.current_stream()
@@ -227,6 +233,14 @@ def run_ours(args):
 
     for _ in range(args.warmup):
         summary, _ = step()
+
+    if args.fixpoint_only:
+        for _ in range(args.steps):
+            summary, stats = step(profile=True)
+        torch.cuda.synchronize()
+        print(json.dumps({"nodes": nodes, "edges": edges, "iterations": summary.iterations,
+                          "derived_tuples": summary.total_new_rows, "stats": stats}), flush=True)
+        return
 
     timer_start = torch.cuda.Event(enable_timing=True)
     timer_end = torch.cuda.Event(enable_timing=True)

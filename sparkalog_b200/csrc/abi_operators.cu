@@ -88,8 +88,7 @@ __global__ void __launch_bounds__(THREADS) pack_histogram_kernel(const u32* firs
         }
         for (int p = 0; p < passes; ++p) {
             const u32 d = valid ? static_cast<u32>((k >> (p * spk::kRadixBits)) & (spk::kRadix - 1)) : spk::kRadix;
-            const u32 peers = __match_any_sync(0xffffffffu, d);
-            if (valid && (peers & spk::lanemask_lt()) == 0) atomicAdd(&sh[p][d], __popc(peers));
+            spk::warp_histogram_add(sh[p], d);
         }
     }
     __syncthreads();

@@ -64,6 +64,7 @@ constexpr int kSetItems = 8;
 constexpr int kSetTile = kThreads * kSetItems;
 constexpr int kJoinItems = 8;
 constexpr int kJoinTile = kThreads * kJoinItems;
+constexpr int kLevelStage = 4096;  // level rows staged in shared memory per anti-join tile
 constexpr int kMergeItems = 8;
 constexpr int kMergeTile = kThreads * kMergeItems;
 constexpr int kSortThreads = spk::RadixSortConfig::kThreads;
@@ -130,6 +131,12 @@ struct RelState {
     bool has_dups = false;  // level[0] as inserted has adjacent duplicates
     DevArray level[spk::kMaxLevels];
     u64 level_n[spk::kMaxLevels] = {0, 0, 0};
+    // Bucket directories of the levels (see spk::Levels), rebuilt lazily
+    // after a level changes.
+    DevArray dir[spk::kMaxLevels];
+    bool dir_valid[spk::kMaxLevels] = {false, false, false};
+    u32 dir_shift[spk::kMaxLevels] = {0, 0, 0};
+    u64 dir_buckets[spk::kMaxLevels] = {0, 0, 0};
     DevArray spare;         // merge destination, swapped with a level after a merge
     DevArray delta, newt;
     u64 delta_n = 0;
@@ -148,6 +155,8 @@ struct sparkalog_store {
     std::map<u32, RelState> relations;
     DevArray scratch_u32[2];   // staging columns for host inserts / reads
     DevArray flags;            // device flag words
+    DevArray merge_splits;     // diagonal splits of the merge pre-pass
+    u32 max_value = 0;         // largest value stored in any column
     u32* pinned = nullptr;     // small pinned host buffer
 
     RelState* find(u32 id) {
@@ -168,30 +177,42 @@ unsigned simple_grid(size_t n) {
     return static_cast<unsigned>(std::max<size_t>(1, std::min(blocks, cap)));
 }
 
-// Merge of two disjoint sorted runs into `out` (capacity checked by caller).
-cudaError_t launch_merge(const u64* a, u64 na, const u64* b, u64 nb, u64* out, cudaStream_t s) {
+// Merge of two disjoint sorted runs into `out` (capacity checked by caller):
+// a parallel diagonal-split pre-pass, then the merge. Returns the number of
+// kernels launched through *launches.
+cudaError_t launch_merge(const u64* a, u64 na, const u64* b, u64 nb, u64* out, DevArray& splits, cudaStream_t s,
+                         u64* launches = nullptr) {
     const u64 total = na + nb;
+    if (launches) *launches = 0;
     if (total == 0) return cudaSuccess;
     if (nb == 0) return cudaMemcpyAsync(out, a, na * 8, cudaMemcpyDeviceToDevice, s);
     if (na == 0) return cudaMemcpyAsync(out, b, nb * 8, cudaMemcpyDeviceToDevice, s);
-    auto kernel = spk::merge_disjoint_kernel<kThreads, kMergeItems>;
     const size_t tiles = (total + kMergeTile - 1) / kMergeTile;
-    kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, tiles), kThreads, 0, s>>>(a, na, b, nb, out);
+    cudaError_t st = splits.ensure((tiles + 1) * 8, s);
+    if (st != cudaSuccess) return st;
+    spk::merge_partition_kernel<<<simple_grid(tiles + 1), 256, 0, s>>>(a, na, b, nb, kMergeTile, splits.as<u64>());
+    st = cudaGetLastError();
+    if (st != cudaSuccess) return st;
+    auto kernel = spk::merge_disjoint_kernel<kThreads, kMergeItems>;
+    kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, tiles), kThreads, 0, s>>>(
+        a, na, b, nb, splits.as<u64>(), out);
+    if (launches) *launches = 2;
     return cudaGetLastError();
 }
 
 // Collapses all levels of a relation into level[0] (a single sorted run).
-int materialize(RelState& r, cudaStream_t s) {
+int materialize(RelState& r, DevArray& splits, cudaStream_t s) {
     for (int l = 1; l < spk::kMaxLevels; ++l) {
         if (r.level_n[l] == 0) continue;
         const u64 total = r.level_n[0] + r.level_n[l];
         SPK_CUDA(r.spare.ensure(total * 8, s), "cudaMallocAsync");
         SPK_CUDA(launch_merge(r.level[0].as<u64>(), r.level_n[0], r.level[l].as<u64>(), r.level_n[l],
-                              r.spare.as<u64>(), s),
+                              r.spare.as<u64>(), splits, s),
                  "merge_disjoint_kernel");
         swap_arrays(r.level[0], r.spare);
         r.level_n[0] = total;
         r.level_n[l] = 0;
+        r.dir_valid[0] = r.dir_valid[l] = false;
     }
     return 0;
 }
@@ -216,13 +237,38 @@ int pack_columns(sparkalog_store* st, const u32* c0, const u32* c1, size_t rows,
         d1 = st->scratch_u32[1].as<u32>();
     }
     u32* flags = st->flags.as<u32>();
-    SPK_CUDA(cudaMemsetAsync(flags, 0, 4, s), "cudaMemsetAsync");
+    SPK_CUDA(cudaMemsetAsync(flags, 0, 8, s), "cudaMemsetAsync");
     spk::pack_rows_kernel<<<simple_grid(rows), 256, 0, s>>>(d0, d1, rows, dst.as<u64>(), flags);
     SPK_CUDA(cudaGetLastError(), "pack_rows_kernel");
-    SPK_CUDA(cudaMemcpyAsync(st->pinned, flags, 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+    SPK_CUDA(cudaMemcpyAsync(st->pinned, flags, 8, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
     SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
     *sorted = (st->pinned[0] & 1u) == 0;
     *has_dups = (st->pinned[0] & 2u) != 0;
+    st->max_value = std::max(st->max_value, st->pinned[1]);
+    return 0;
+}
+
+// Rebuilds the bucket directory of every non-empty level whose rows changed.
+// The bucket width comes from the store's largest value, which bounds every
+// key: ~64 rows per bucket.
+int refresh_directories(sparkalog_store* st, RelState& r, cudaStream_t s, u64* launches) {
+    const u64 key_max = (static_cast<u64>(st->max_value) << 32) | st->max_value;
+    int key_bits = 64 - __builtin_clzll(key_max | 1);
+    for (int l = 0; l < spk::kMaxLevels; ++l) {
+        if (r.level_n[l] == 0 || r.dir_valid[l]) continue;
+        const u64 target = std::max<u64>(r.level_n[l] / 64, 1);
+        const int target_bits = 64 - __builtin_clzll(target);
+        const u32 shift = static_cast<u32>(std::max(0, key_bits - target_bits));
+        const u64 buckets = (key_max >> shift) + 1;
+        SPK_CUDA(r.dir[l].ensure((buckets + 1) * 4, s), "cudaMallocAsync");
+        spk::level_directory_kernel<<<simple_grid(buckets + 1), 256, 0, s>>>(r.level[l].as<u64>(), r.level_n[l], shift,
+                                                                            buckets, r.dir[l].as<u32>());
+        SPK_CUDA(cudaGetLastError(), "level_directory_kernel");
+        r.dir_shift[l] = shift;
+        r.dir_buckets[l] = buckets;
+        r.dir_valid[l] = true;
+        if (launches) *launches += 1;
+    }
     return 0;
 }
 
@@ -387,7 +433,7 @@ int build_index_impl(sparkalog_executor* ex, sparkalog_store* st, IndexCache& ic
     RelState* r = st->find(relation);
     if (!r) return fail(SPARKALOG_E_MISSING, "relation " + std::to_string(relation) + " is not registered");
     if (r->recursive) {
-        int rc = materialize(*r, s);
+        int rc = materialize(*r, st->merge_splits, s);
         if (rc) return rc;
     }
     const u64 n = r->level_n[0];
@@ -487,6 +533,7 @@ void sparkalog_store_destroy(sparkalog_store* st) {
     cudaStream_t s = st->stream;
     for (auto& kv : st->relations) {
         for (auto& l : kv.second.level) l.release(s);
+        for (auto& d : kv.second.dir) d.release(s);
         kv.second.spare.release(s);
         kv.second.delta.release(s);
         kv.second.newt.release(s);
@@ -494,6 +541,7 @@ void sparkalog_store_destroy(sparkalog_store* st) {
     st->scratch_u32[0].release(s);
     st->scratch_u32[1].release(s);
     st->flags.release(s);
+    st->merge_splits.release(s);
     cudaStreamSynchronize(s);
     if (st->pinned) cudaFreeHost(st->pinned);
     delete st;
@@ -565,7 +613,7 @@ int sparkalog_store_read(sparkalog_store* st, u32 id, int version, u32* first, u
     u64 n;
     if (version == SPARKALOG_FULL) {
         if (r->recursive) {
-            int rc = materialize(*r, s);
+            int rc = materialize(*r, st->merge_splits, s);
             if (rc) return rc;
         }
         src = r->level[0].as<u64>();
@@ -749,7 +797,7 @@ int sparkalog_executor_run(sparkalog_executor* ex, sparkalog_store* st, size_t m
     if (any_delta) {
         for (u32 id : ex->relations) {
             RelState& r = *st->find(id);
-            int rc = materialize(r, s);
+            int rc = materialize(r, st->merge_splits, s);
             if (rc) return rc;
             if (!r.sorted)
                 return fail(SPARKALOG_E_UNSORTED_FULL,
@@ -765,7 +813,7 @@ int sparkalog_executor_run(sparkalog_executor* ex, sparkalog_store* st, size_t m
                 none.n = 0;
                 u64* nptr = counts + 1;
                 SPK_CUDA(cudaMemcpyAsync(nptr, &r.level_n[0], 8, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
-                auto kernel = spk::anti_join_levels_kernel<kThreads, kSetItems>;
+                auto kernel = spk::anti_join_levels_kernel<kThreads, kSetItems, kLevelStage>;
                 const size_t tiles = (n + kSetTile - 1) / kSetTile;
                 kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, tiles), kThreads, 0, s>>>(
                     r.level[0].as<u64>(), r.level[0].as<u64>(), nullptr, nptr, none, r.spare.as<u64>(), counts,
@@ -777,6 +825,7 @@ int sparkalog_executor_run(sparkalog_executor* ex, sparkalog_store* st, size_t m
                 swap_arrays(r.level[0], r.spare);
                 r.level_n[0] = ex->host_counts[0];
                 r.has_dups = false;
+                r.dir_valid[0] = false;
             }
         }
     }
@@ -909,25 +958,33 @@ int sparkalog_executor_run(sparkalog_executor* ex, sparkalog_store* st, size_t m
                                     &pass_t[ti]);
                 if (rc) return rc;
                 RelState& tr = *st->find(t.id);
+                u64 dir_launches = 0;
+                {
+                    int rc = refresh_directories(st, tr, s, &dir_launches);
+                    if (rc) return rc;
+                }
                 spk::Levels lv{};
                 lv.n = 0;
                 for (int l = 0; l < spk::kMaxLevels; ++l) {
                     if (tr.level_n[l] == 0) continue;
                     lv.keys[lv.n] = tr.level[l].as<u64>();
                     lv.count[lv.n] = tr.level_n[l];
+                    lv.dir[lv.n] = tr.dir[l].as<u32>();
+                    lv.shift[lv.n] = tr.dir_shift[l];
+                    lv.buckets[lv.n] = tr.dir_buckets[l];
                     ++lv.n;
                 }
-                auto kernel = spk::anti_join_levels_kernel<kThreads, kSetItems>;
+                auto kernel = spk::anti_join_levels_kernel<kThreads, kSetItems, kLevelStage>;
                 const size_t tiles = (t.j_cap + kSetTile - 1) / kSetTile;
+                const u32* sel = &t.sort.plan.as<spk::RadixPlan>()->final_sel;
                 anti_t[ti] = ex->begin(SPARKALOG_K_ANTI_JOIN, s);
                 kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, std::max<size_t>(tiles, 1)),
-                         kThreads, 0, s>>>(t.j_a.as<u64>(), t.j_b.as<u64>(),
-                                           &t.sort.plan.as<spk::RadixPlan>()->final_sel, jn, lv, tr.newt.as<u64>(),
+                         kThreads, 0, s>>>(t.j_a.as<u64>(), t.j_b.as<u64>(), sel, jn, lv, tr.newt.as<u64>(),
                                            tc + t.rules.size() + 1, ex->status.as<u64>(), counters + counter_slot++,
                                            ex->epoch++, err);
                 SPK_CUDA(cudaGetLastError(), "anti_join_levels_kernel");
                 ex->end(anti_t[ti], s, 0.0, 1);
-                ex->stats.total_launches += 1;
+                ex->stats.total_launches += 1 + dir_launches;
                 SPK_CUDA(cudaMemcpyAsync(ex->host_active + ti * spk::kMaxPasses, t.sort.plan.as<spk::RadixPlan>()->active,
                                          spk::kMaxPasses * 4, cudaMemcpyDeviceToHost, s),
                          "cudaMemcpyAsync");
@@ -988,36 +1045,43 @@ int sparkalog_executor_run(sparkalog_executor* ex, sparkalog_store* st, size_t m
                 const u64 tn = tr.level_n[tail] + newt_n;
                 SPK_CUDA(tr.spare.ensure(tn * 8, s), "cudaMallocAsync");
                 {
-                    const bool kernel = tr.level_n[tail] != 0;
+                    u64 launched = 0;
                     const int tm = ex->begin(SPARKALOG_K_MERGE, s);
                     SPK_CUDA(launch_merge(tr.level[tail].as<u64>(), tr.level_n[tail], tr.newt.as<u64>(), newt_n,
-                                          tr.spare.as<u64>(), s),
+                                          tr.spare.as<u64>(), st->merge_splits, s, &launched),
                              "merge_disjoint_kernel");
-                    ex->end(tm, s, 16.0 * static_cast<double>(tn), kernel ? 1 : 0);
-                    ex->stats.total_launches += kernel ? 1 : 0;
+                    ex->end(tm, s, 16.0 * static_cast<double>(tn), launched);
+                    ex->stats.total_launches += launched;
                 }
                 swap_arrays(tr.level[tail], tr.spare);
                 tr.level_n[tail] = tn;
+                tr.dir_valid[tail] = false;
                 // Cascade: a level merges down once it outgrows 1/kLevelRatio of the next.
                 for (int l = tail; l > 0; --l) {
                     if (tr.level_n[l] == 0 || tr.level_n[l] * kLevelRatio <= tr.level_n[l - 1]) continue;
                     if (tr.level_n[l - 1] == 0) {
                         swap_arrays(tr.level[l - 1], tr.level[l]);
+                        swap_arrays(tr.dir[l - 1], tr.dir[l]);
+                        std::swap(tr.dir_valid[l - 1], tr.dir_valid[l]);
+                        std::swap(tr.dir_shift[l - 1], tr.dir_shift[l]);
+                        std::swap(tr.dir_buckets[l - 1], tr.dir_buckets[l]);
                         tr.level_n[l - 1] = tr.level_n[l];
                         tr.level_n[l] = 0;
                         continue;
                     }
                     const u64 mn = tr.level_n[l - 1] + tr.level_n[l];
                     SPK_CUDA(tr.spare.ensure(mn * 8, s), "cudaMallocAsync");
+                    u64 launched = 0;
                     const int tm = ex->begin(SPARKALOG_K_MERGE, s);
                     SPK_CUDA(launch_merge(tr.level[l - 1].as<u64>(), tr.level_n[l - 1], tr.level[l].as<u64>(),
-                                          tr.level_n[l], tr.spare.as<u64>(), s),
+                                          tr.level_n[l], tr.spare.as<u64>(), st->merge_splits, s, &launched),
                              "merge_disjoint_kernel");
-                    ex->end(tm, s, 16.0 * static_cast<double>(mn), 1);
-                    ex->stats.total_launches += 1;
+                    ex->end(tm, s, 16.0 * static_cast<double>(mn), launched);
+                    ex->stats.total_launches += launched;
                     swap_arrays(tr.level[l - 1], tr.spare);
                     tr.level_n[l - 1] = mn;
                     tr.level_n[l] = 0;
+                    tr.dir_valid[l - 1] = tr.dir_valid[l] = false;
                 }
             }
             swap_arrays(tr.delta, tr.newt);

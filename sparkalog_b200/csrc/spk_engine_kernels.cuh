@@ -16,24 +16,67 @@ namespace spk {
 
 constexpr int kMaxLevels = 3;
 
+// A level's bucket directory: dir[b] = first row whose key >> shift >= b, for
+// b in [0, buckets]; about 64 rows per bucket. It turns a search over a level
+// of n rows into two loads of a small (L2-resident) array plus a search over
+// one bucket, instead of a log2(n)-long chain of dependent DRAM loads.
 struct Levels {
     const u64* keys[kMaxLevels];
     u64 count[kMaxLevels];
+    const u32* dir[kMaxLevels];
+    u32 shift[kMaxLevels];
+    u64 buckets[kMaxLevels];
     int n;
 };
+
+// lower_bound of `key` in level l through its directory.
+__device__ __forceinline__ void dir_range(const Levels& lv, int l, u64 key, u64* lo, u64* hi) {
+    const u64 b = key >> lv.shift[l];
+    if (b >= lv.buckets[l]) {
+        *lo = *hi = lv.count[l];
+        return;
+    }
+    *lo = lv.dir[l][b];
+    *hi = lv.dir[l][b + 1];
+}
+
+__device__ __forceinline__ u64 dir_lower_bound(const Levels& lv, int l, u64 key) {
+    u64 lo, hi;
+    dir_range(lv, l, key, &lo, &hi);
+    return lower_bound_keys(PackedKeys{lv.keys[l]}, lo, hi, key);
+}
+
+// Builds a level's bucket directory: one independent binary search per
+// bucket boundary (all in parallel, so no thread walks a long gap of empty
+// buckets). `buckets` must exceed the largest key >> shift.
+static __global__ void level_directory_kernel(const u64* keys, u64 n, u32 shift, u64 buckets, u32* dir) {
+    const PackedKeys k{keys};
+    const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+    for (u64 b = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; b <= buckets; b += stride)
+        dir[b] = static_cast<u32>(b == buckets ? n : lower_bound_keys(k, 0, n, b << shift));
+}
 
 // NEWT = unique(sorted candidates) - FULL, where FULL is the union of the
 // levels. Candidates come from the radix sort's final buffer. This fuses the
 // reference's BinaryDistinct unique step with SortedBinaryAntiJoin.
-template <int THREADS, int ITEMS>
+//
+// Per tile of candidates and per level, one warp finds the level's slice
+// that covers the tile's key span (warp_lower_bound, ~log32 dependent loads).
+// A slice that fits in shared memory is staged there with coalesced loads and
+// every thread merges its sorted candidates against it; a larger slice (a
+// sparse tile against a big level) is searched per candidate with galloping
+// searches in global memory. Kept rows are compacted with a decoupled
+// look-back, so NEWT stays sorted.
+template <int THREADS, int ITEMS, int STAGE>
 __global__ void __launch_bounds__(THREADS) anti_join_levels_kernel(const u64* buf_a, const u64* buf_b,
                                                                    const u32* final_sel, const u64* n_ptr,
                                                                    Levels levels, u64* out, u64* out_count,
                                                                    u64* status, u32* tile_counter, u32 epoch,
                                                                    u32* err) {
     constexpr int kTile = THREADS * ITEMS;
+    static_assert(STAGE >= kTile, "the output stage reuses the level stage");
     __shared__ CompactShared<THREADS> cs;
-    __shared__ u64 stage[kTile];
+    __shared__ u64 stage[STAGE];
     __shared__ u64 range_lo[kMaxLevels], range_hi[kMaxLevels];
     const u64* keys = (final_sel && *final_sel) ? buf_b : buf_a;
     const u64 n = *n_ptr;
@@ -48,23 +91,19 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_kernel(const u64* bu
         const u64 tile = cs.tile;
         if (tile >= num_tiles) break;
         const u64 tile_begin = tile * kTile;
-        const u64 tile_end = tile_begin + kTile < n ? tile_begin + kTile : n;
-        // Narrow every level to the tile's key span (one warp per level).
-        const int w = static_cast<int>(warp_id());
-        if (w < levels.n && lane_id() == 0) {
-            const PackedKeys lv{levels.keys[w]};
-            const u64 c = levels.count[w];
-            range_lo[w] = lower_bound_keys(lv, 0, c, keys[tile_begin]);
-            const u64 hi = lower_bound_keys(lv, 0, c, keys[tile_end - 1]);
-            range_hi[w] = hi < c ? hi + 1 : c;
+        if (threadIdx.x < static_cast<u32>(levels.n)) {
+            // The tile's slice of level l: from the lower bound of its first
+            // key to just past the lower bound of its last key.
+            const int l = static_cast<int>(threadIdx.x);
+            const u64 c = levels.count[l];
+            const u64 last = keys[(tile_begin + kTile < n ? tile_begin + kTile : n) - 1];
+            range_lo[l] = dir_lower_bound(levels, l, keys[tile_begin]);
+            const u64 hi = dir_lower_bound(levels, l, last) + 1;
+            range_hi[l] = hi < c ? hi : c;
         }
-        __syncthreads();
         const u64 base = tile_begin + static_cast<u64>(threadIdx.x) * ITEMS;
         u64 v[ITEMS];
-        u32 keep = 0, count = 0;
-        u64 cursor[kMaxLevels];
-#pragma unroll
-        for (int l = 0; l < kMaxLevels; ++l) cursor[l] = l < levels.n ? range_lo[l] : 0;
+        u32 keep = 0;
         u64 prev = (base > 0 && base - 1 < n) ? keys[base - 1] : 0;
 #pragma unroll
         for (int i = 0; i < ITEMS; ++i) {
@@ -73,26 +112,72 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_kernel(const u64* bu
             if (idx < n) {
                 const u64 k = keys[idx];
                 v[i] = k;
-                bool kept = (idx == 0 || k != prev);
+                if (idx == 0 || k != prev) keep |= 1u << i;
                 prev = k;
-                if (kept) {
+            }
+        }
+        __syncthreads();
+        for (int l = 0; l < levels.n; ++l) {
+            const u64 lo = range_lo[l];
+            const u64 len = range_hi[l] - lo;
+            const PackedKeys lv{levels.keys[l]};
+            if (len <= static_cast<u64>(STAGE)) {
+                for (u32 t = threadIdx.x; t < len; t += THREADS) stage[t] = lv(lo + t);
+                __syncthreads();
+                if (keep) {
+                    const SmemKeys sk{stage};
+                    u64 cur = 0;
+                    bool have = false;
 #pragma unroll
-                    for (int l = 0; l < kMaxLevels; ++l) {
-                        if (l < levels.n) {
-                            const PackedKeys lv{levels.keys[l]};
-                            cursor[l] = gallop_lower_bound(lv, cursor[l], range_hi[l], k);
-                            if (cursor[l] < range_hi[l] && lv(cursor[l]) == k) kept = false;
+                    for (int i = 0; i < ITEMS; ++i) {
+                        if (keep & (1u << i)) {
+                            cur = have ? gallop_lower_bound(sk, cur, len, v[i]) : lower_bound_keys(sk, 0, len, v[i]);
+                            have = true;
+                            if (cur < len && stage[cur] == v[i]) keep &= ~(1u << i);
                         }
                     }
                 }
-                if (kept) {
-                    keep |= 1u << i;
-                    ++count;
+                __syncthreads();
+            } else if (keep) {
+                // Sparse tile against a large slice: each candidate's search
+                // starts from its directory bucket (two loads of a small
+                // array), then the bucket searches of all ITEMS candidates
+                // run branch-free in lock step, so every step issues ITEMS
+                // independent loads instead of one dependent chain.
+                u64 pos[ITEMS], span[ITEMS], end[ITEMS];
+                u64 max_span = 0;
+#pragma unroll
+                for (int i = 0; i < ITEMS; ++i) {
+                    span[i] = 0;
+                    pos[i] = end[i] = 0;
+                    if (keep & (1u << i)) {
+                        dir_range(levels, l, v[i], &pos[i], &end[i]);
+                        span[i] = end[i] - pos[i];
+                        max_span = span[i] > max_span ? span[i] : max_span;
+                    }
+                }
+                while (max_span > 1) {
+#pragma unroll
+                    for (int i = 0; i < ITEMS; ++i) {
+                        if (span[i] > 1) {
+                            const u64 half = span[i] >> 1;
+                            pos[i] = lv(pos[i] + half - 1) < v[i] ? pos[i] + half : pos[i];
+                            span[i] -= half;
+                        }
+                    }
+                    max_span -= max_span >> 1;
+                }
+#pragma unroll
+                for (int i = 0; i < ITEMS; ++i) {
+                    if ((keep & (1u << i)) && end[i] > pos[i]) {
+                        const u64 p = pos[i] + (lv(pos[i]) < v[i] ? 1 : 0);
+                        if (p < end[i] && lv(p) == v[i]) keep &= ~(1u << i);
+                    }
                 }
             }
         }
         u32 excl, total;
-        const u64 off = compact_offsets<THREADS>(count, &excl, &total, tile, status, epoch, err, cs);
+        const u64 off = compact_offsets<THREADS>(__popc(keep), &excl, &total, tile, status, epoch, err, cs);
         u32 wpos = excl;
 #pragma unroll
         for (int i = 0; i < ITEMS; ++i)
@@ -104,25 +189,34 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_kernel(const u64* bu
     }
 }
 
+// Diagonal splits for merge_disjoint_kernel: splits[t] = number of `a` rows
+// among the first t * tile merged rows, for t in [0, tiles]; one thread per
+// diagonal.
+static __global__ void merge_partition_kernel(const u64* a, u64 na, const u64* b, u64 nb, u32 tile, u64* splits) {
+    const u64 total = na + nb;
+    const u64 tiles = (total + tile - 1) / tile;
+    const PackedKeys ka{a}, kb{b};
+    const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+    for (u64 t = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; t <= tiles; t += stride) {
+        const u64 d = t * tile < total ? t * tile : total;
+        splits[t] = merge_path(ka, na, kb, nb, d);
+    }
+}
+
 // Merge of two sorted, mutually disjoint runs (levels are disjoint by
 // construction: NEWT excludes FULL). Output position = merge diagonal, so no
 // compaction or look-back is needed: pure streaming at HBM rate.
 template <int THREADS, int ITEMS>
 __global__ void __launch_bounds__(THREADS) merge_disjoint_kernel(const u64* a, u64 na, const u64* b, u64 nb,
-                                                                 u64* out) {
+                                                                 const u64* splits, u64* out) {
     constexpr int kTile = THREADS * ITEMS;
     __shared__ u64 sm[kTile];
-    __shared__ u64 split[2];
-    const PackedKeys ka{a}, kb{b};
     const u64 total = na + nb;
     const u64 num_tiles = (total + kTile - 1) / kTile;
     for (u64 tile = blockIdx.x; tile < num_tiles; tile += gridDim.x) {
         const u64 d0 = tile * kTile;
         const u64 d1 = d0 + kTile < total ? d0 + kTile : total;
-        if (threadIdx.x == 0) split[0] = merge_path(ka, na, kb, nb, d0);
-        if (threadIdx.x == kWarp) split[1] = merge_path(ka, na, kb, nb, d1);
-        __syncthreads();
-        const u64 i0 = split[0], i1 = split[1];
+        const u64 i0 = splits[tile], i1 = splits[tile + 1];
         const u64 j0 = d0 - i0, j1 = d1 - i1;
         const u32 sa_n = static_cast<u32>(i1 - i0), sb_n = static_cast<u32>(j1 - j0);
         for (u32 t = threadIdx.x; t < sa_n; t += THREADS) sm[t] = a[i0 + t];
@@ -158,9 +252,11 @@ __global__ void __launch_bounds__(THREADS) merge_disjoint_kernel(const u64* a, u
 static __global__ void pack_rows_kernel(const u32* c0, const u32* c1, u64 n, u64* out, u32* flags) {
     const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
     bool unsorted = false, dup = false;
+    u32 max_value = 0;
     for (u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
         const u64 k = pack2(c0[i], c1[i]);
         out[i] = k;
+        max_value = max(max_value, max(c0[i], c1[i]));
         if (i > 0) {
             const u64 p = pack2(c0[i - 1], c1[i - 1]);
             unsorted |= p > k;
@@ -169,6 +265,10 @@ static __global__ void pack_rows_kernel(const u32* c0, const u32* c1, u64 n, u64
     }
     if (__any_sync(0xffffffffu, unsorted) && lane_id() == 0) atomicOr(flags, 1u);
     if (__any_sync(0xffffffffu, dup) && lane_id() == 0) atomicOr(flags, 2u);
+    // flags[1]: the largest value in either column (bounds every key the
+    // pipeline can derive, since derived rows only project stored values).
+    max_value = __reduce_max_sync(0xffffffffu, max_value);
+    if (lane_id() == 0) atomicMax(flags + 1, max_value);
 }
 
 static __global__ void unpack_rows_kernel(const u64* in, u64 n, u32* c0, u32* c1) {

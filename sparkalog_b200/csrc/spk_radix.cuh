@@ -41,6 +41,20 @@ struct RadixPlan {
 // Bytes of RadixPlan that must be zero before radix_histogram runs.
 constexpr size_t kRadixPlanClearBytes = sizeof(u32) * (kMaxPasses * kRadix + kMaxPasses);
 
+// Warp-aggregated histogram update: d == kRadix marks an inactive lane.
+// A digit shared by the whole warp (constant high bits, or the sorted high
+// bits of a join output) costs one shared atomic; otherwise lanes with equal
+// digits are grouped with match.any and each group's leader adds its size.
+__device__ __forceinline__ void warp_histogram_add(u32* hist, u32 d) {
+    const u32 d0 = __shfl_sync(0xffffffffu, d, 0);
+    if (__all_sync(0xffffffffu, d == d0)) {
+        if (lane_id() == 0 && d0 < static_cast<u32>(kRadix)) atomicAdd(&hist[d0], static_cast<u32>(kWarp));
+        return;
+    }
+    const u32 peers = __match_any_sync(0xffffffffu, d);
+    if (d < static_cast<u32>(kRadix) && (peers & lanemask_lt()) == 0) atomicAdd(&hist[d], __popc(peers));
+}
+
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS) radix_histogram(const u64* __restrict__ keys, const u64* n_ptr,
                                                            u64 n_host, RadixPlan* plan, int begin_bit,
@@ -59,8 +73,7 @@ __global__ void __launch_bounds__(THREADS) radix_histogram(const u64* __restrict
         const u64 k = valid ? keys[i] : 0;
         for (int p = 0; p < passes; ++p) {
             const u32 d = valid ? static_cast<u32>((k >> (begin_bit + p * kRadixBits)) & (kRadix - 1)) : kRadix;
-            const u32 peers = __match_any_sync(0xffffffffu, d);
-            if (valid && (peers & lanemask_lt()) == 0) atomicAdd(&sh[p][d], __popc(peers));
+            warp_histogram_add(sh[p], d);
         }
     }
     __syncthreads();

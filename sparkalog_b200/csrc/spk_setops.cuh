@@ -70,6 +70,29 @@ __device__ __forceinline__ u64 gallop_lower_bound(const A& a, u64 from, u64 hi, 
     return lower_bound_keys(a, lo, probe < hi ? probe : hi, key);
 }
 
+// Warp-cooperative lower_bound over [lo, hi): each step the 32 lanes probe 32
+// evenly spaced positions and the ballot of "probe < key" (a prefix, since
+// the input is sorted) cuts the range 32-fold, so a search over n keys costs
+// about log32(n) dependent loads instead of log2(n). All 32 lanes must call
+// it with the same arguments; all get the result.
+template <class A>
+__device__ __forceinline__ u64 warp_lower_bound(const A& a, u64 lo, u64 hi, u64 key) {
+    const u32 lane = lane_id();
+    while (hi - lo > kWarp) {
+        const u64 step = (hi - lo + kWarp - 1) / kWarp;
+        const u64 pos = lo + (static_cast<u64>(lane) + 1) * step - 1;
+        const bool less = pos < hi && a(pos) < key;
+        const u32 c = __popc(__ballot_sync(0xffffffffu, less));
+        const u64 nlo = lo + c * step;
+        const u64 nhi = lo + (static_cast<u64>(c) + 1) * step;
+        lo = nlo < hi ? nlo : hi;
+        hi = nhi < hi ? nhi : hi;
+    }
+    const u64 pos = lo + lane;
+    const bool less = pos < hi && a(pos) < key;
+    return lo + __popc(__ballot_sync(0xffffffffu, less));
+}
+
 template <int THREADS>
 struct CompactShared {
     u32 scan_scratch[THREADS / kWarp + 1];
@@ -168,11 +191,12 @@ __global__ void __launch_bounds__(THREADS) anti_join_soa_kernel(const u32* lf, c
         const u64 tile_begin = tile * kTile;
         const u64 tile_end = tile_begin + kTile < ln ? tile_begin + kTile : ln;
         // Narrow the right range once per tile: [lb(first), lb(last)+1 bound).
-        if (threadIdx.x == 0) range[0] = lower_bound_keys(right, 0, rn, pack2(lf[tile_begin], ls[tile_begin]));
-        if (threadIdx.x == kWarp) {
-            const u64 last = pack2(lf[tile_end - 1], ls[tile_end - 1]);
-            u64 hi = lower_bound_keys(right, 0, rn, last);
-            range[1] = hi < rn ? hi + 1 : rn;
+        if (warp_id() == 0) {
+            const u64 lo = warp_lower_bound(right, 0, rn, pack2(lf[tile_begin], ls[tile_begin]));
+            if (lane_id() == 0) range[0] = lo;
+        } else if (warp_id() == 1) {
+            const u64 hi = warp_lower_bound(right, 0, rn, pack2(lf[tile_end - 1], ls[tile_end - 1]));
+            if (lane_id() == 0) range[1] = hi < rn ? hi + 1 : rn;
         }
         __syncthreads();
         // lower_bound is monotone in the key, so any key between the tile's
