@@ -202,6 +202,17 @@ SPARKALOG_API int sparkalog_store_rows(sparkalog_store* store, uint32_t id, int 
 SPARKALOG_API int sparkalog_store_read(sparkalog_store* store, uint32_t id, int version, uint32_t* first,
                                        uint32_t* second, int location);
 
+/* Stratified negation over completed relations: stores
+ *   out(x, y) :- left(x, y), !right(x, y).
+ * as a new static relation `out_id` holding the sorted, deduplicated rows of
+ * FULL(left) that are absent from FULL(right). This is the GeneralCpu
+ * evaluation of such a clause (general.rs:478-551: positive atom scan, then a
+ * negated atom checked against the completed FULL of an earlier stratum),
+ * which outputs a BTreeSet (sorted, unique); the reference's binary lowering
+ * rejects the clause (subset.rs:56-63), so this extends the device path. */
+SPARKALOG_API int sparkalog_store_anti_join(sparkalog_store* store, uint32_t left_id, uint32_t right_id,
+                                            uint32_t out_id);
+
 /* RecursiveExecutor::compile, generic.rs:407-470. */
 SPARKALOG_API int sparkalog_executor_compile(sparkalog_store* store, const uint32_t* relations,
                                              size_t relation_count, const sparkalog_rule_plan* rules,
@@ -234,6 +245,17 @@ typedef struct sparkalog_kernel_stats {
     uint64_t total_launches;
     uint64_t rounds;
 } sparkalog_kernel_stats;
+
+/* Per-segment activity for batched runs, where independent instances share
+ * one SCC and a row's segment (instance) is its first column >> shift. After
+ * each round the executor records, for every segment that gained NEWT rows,
+ * round_index + 1 and the number of rows. An instance whose seed DELTA was
+ * non-empty then ran last_active_round[s] + 1 rounds of its own fixpoint (the
+ * count RecursiveExecutor::run would report for it alone). No counterpart in
+ * the reference, which runs one instance at a time. */
+SPARKALOG_API int sparkalog_executor_track_segments(sparkalog_executor* executor, uint32_t shift, uint32_t count);
+SPARKALOG_API int sparkalog_executor_segment_stats(sparkalog_executor* executor, uint32_t* last_active_round,
+                                                   uint64_t* new_rows);
 
 SPARKALOG_API int sparkalog_executor_set_profiling(sparkalog_executor* executor, int enable);
 SPARKALOG_API int sparkalog_executor_stats(sparkalog_executor* executor, sparkalog_kernel_stats* out, int reset);

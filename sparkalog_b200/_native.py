@@ -39,9 +39,12 @@ TIER_B = [
     "sparkalog_store_insert_recursive",
     "sparkalog_store_rows",
     "sparkalog_store_read",
+    "sparkalog_store_anti_join",
     "sparkalog_executor_compile",
     "sparkalog_executor_destroy",
     "sparkalog_executor_run",
+    "sparkalog_executor_track_segments",
+    "sparkalog_executor_segment_stats",
     "sparkalog_executor_set_profiling",
     "sparkalog_executor_stats",
     "sparkalog_last_error",
@@ -142,6 +145,8 @@ def load() -> ctypes.CDLL:
     L.sparkalog_store_rows.restype = i
     L.sparkalog_store_read.argtypes = [vp, ctypes.c_uint32, i, vp, vp, i]
     L.sparkalog_store_read.restype = i
+    L.sparkalog_store_anti_join.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]
+    L.sparkalog_store_anti_join.restype = i
     L.sparkalog_executor_compile.argtypes = [vp, c_u32p, ctypes.c_size_t, ctypes.POINTER(RulePlanC), ctypes.c_size_t,
                                              ctypes.POINTER(vp)]
     L.sparkalog_executor_compile.restype = i
@@ -149,6 +154,10 @@ def load() -> ctypes.CDLL:
     L.sparkalog_executor_destroy.restype = None
     L.sparkalog_executor_run.argtypes = [vp, vp, ctypes.c_size_t, ctypes.POINTER(SccSummaryC)]
     L.sparkalog_executor_run.restype = i
+    L.sparkalog_executor_track_segments.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32]
+    L.sparkalog_executor_track_segments.restype = i
+    L.sparkalog_executor_segment_stats.argtypes = [vp, c_u32p, c_u64p]
+    L.sparkalog_executor_segment_stats.restype = i
     L.sparkalog_executor_set_profiling.argtypes = [vp, i]
     L.sparkalog_executor_set_profiling.restype = i
     L.sparkalog_executor_stats.argtypes = [vp, ctypes.POINTER(KernelStatsC), i]

@@ -315,6 +315,11 @@ struct sparkalog_executor {
     SortScratch index_sort;
     DevArray index_pairs[2];
     u32* host_active = nullptr;  // pinned: radix pass activity per target (8 words each)
+    // Batched runs: per-segment (instance) activity, see sparkalog_executor_track_segments.
+    u32 seg_shift = 0;
+    u32 seg_count = 0;
+    DevArray seg_seen;           // u32[seg_count]
+    DevArray seg_new;            // u64[seg_count]
 
     // Profiling: CUDA events around each kernel class on the executor's stream.
     struct Timing {
@@ -643,6 +648,81 @@ int sparkalog_store_read(sparkalog_store* st, u32 id, int version, u32* first, u
     return 0;
 }
 
+int sparkalog_store_anti_join(sparkalog_store* st, u32 left_id, u32 right_id, u32 out_id) {
+    if (!st) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null store");
+    RelState* left = st->find(left_id);
+    RelState* right = st->find(right_id);
+    if (!left) return fail(SPARKALOG_E_MISSING, "relation " + std::to_string(left_id) + " is not registered");
+    if (!right) return fail(SPARKALOG_E_MISSING, "relation " + std::to_string(right_id) + " is not registered");
+    if (st->find(out_id))
+        return fail(SPARKALOG_E_DUPLICATE, "relation " + std::to_string(out_id) + " is already registered");
+    cudaStream_t s = st->stream;
+    int rc = materialize(*left, st->merge_splits, s);
+    if (rc) return rc;
+    rc = materialize(*right, st->merge_splits, s);
+    if (rc) return rc;
+    if (!right->sorted && right->level_n[0] > 1)
+        return fail(SPARKALOG_E_UNSORTED_FULL, "FULL of relation " + std::to_string(right_id) + " is not sorted");
+    sparkalog_executor scratch;  // sort scratch, look-back buffers and epochs for this one operation
+    const u64 n = left->level_n[0];
+    RelState out;
+    SPK_CUDA(out.level[0].ensure(std::max<u64>(n, 1) * 8, s), "cudaMallocAsync");
+    u64 out_n = 0;
+    if (n > 0) {
+        DevArray a, b, counts;
+        SPK_CUDA(a.ensure(n * 8, s), "cudaMallocAsync");
+        SPK_CUDA(b.ensure(n * 8, s), "cudaMallocAsync");
+        SPK_CUDA(counts.ensure(64, s), "cudaMallocAsync");
+        SPK_CUDA(scratch.counters.ensure((kCounterWords + 64) * 4, s), "cudaMallocAsync");
+        SPK_CUDA(cudaMemsetAsync(scratch.counters.ptr, 0, (kCounterWords + 64) * 4, s), "cudaMemsetAsync");
+        SPK_CUDA(cudaMemcpyAsync(a.ptr, left->level[0].ptr, n * 8, cudaMemcpyDeviceToDevice, s), "cudaMemcpyAsync");
+        u32* err = scratch.counters.as<u32>() + kErrWord;
+        rc = radix_sort(a.as<u64>(), b.as<u64>(), nullptr, n, scratch.index_sort, &scratch, err, s, nullptr, nullptr);
+        if (rc) return rc;
+        rc = refresh_directories(st, *right, s, nullptr);
+        if (rc) return rc;
+        spk::Levels lv{};
+        lv.n = 0;
+        if (right->level_n[0] > 0) {
+            lv.keys[0] = right->level[0].as<u64>();
+            lv.count[0] = right->level_n[0];
+            lv.dir[0] = right->dir[0].as<u32>();
+            lv.shift[0] = right->dir_shift[0];
+            lv.buckets[0] = right->dir_buckets[0];
+            lv.n = 1;
+        }
+        SPK_CUDA(scratch.status.ensure_zeroed(((n + kSetTile - 1) / kSetTile + 1) * 8, s), "cudaMallocAsync");
+        u64* nptr = counts.as<u64>() + 1;
+        SPK_CUDA(cudaMemcpyAsync(nptr, &left->level_n[0], 8, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
+        auto kernel = spk::anti_join_levels_kernel<kThreads, kSetItems, kLevelStage>;
+        const size_t tiles = (n + kSetTile - 1) / kSetTile;
+        kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, tiles), kThreads, 0, s>>>(
+            a.as<u64>(), b.as<u64>(), &scratch.index_sort.plan.as<spk::RadixPlan>()->final_sel, nptr, lv,
+            out.level[0].as<u64>(), counts.as<u64>(), scratch.status.as<u64>(), scratch.counters.as<u32>(),
+            scratch.epoch++, err);
+        SPK_CUDA(cudaGetLastError(), "anti_join_levels_kernel");
+        u64 host[2] = {0, 0};
+        SPK_CUDA(cudaMemcpyAsync(st->pinned, counts.ptr, 8, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+        SPK_CUDA(cudaMemcpyAsync(st->pinned + 2, err, 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+        SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+        std::memcpy(host, st->pinned, 8);
+        if (st->pinned[2]) return fail(SPARKALOG_E_DEVICE_FAULT, "device error bits " + std::to_string(st->pinned[2]));
+        out_n = host[0];
+        a.release(s);
+        b.release(s);
+        counts.release(s);
+        scratch.counters.release(s);
+        scratch.status.release(s);
+        scratch.index_sort.plan.release(s);
+        scratch.index_sort.status.release(s);
+    }
+    out.level_n[0] = out_n;
+    out.sorted = true;
+    out.has_dups = false;
+    st->relations[out_id] = std::move(out);
+    return 0;
+}
+
 int sparkalog_executor_compile(sparkalog_store* st, const u32* relations, size_t relation_count,
                                const sparkalog_rule_plan* rules, size_t rule_count, sparkalog_executor** out) {
     if (!st || !out || (relation_count && !relations) || (rule_count && !rules))
@@ -736,6 +816,8 @@ void sparkalog_executor_destroy(sparkalog_executor* ex) {
         ic.rows.release(s);
     }
     ex->counts.release(s);
+    ex->seg_seen.release(s);
+    ex->seg_new.release(s);
     ex->rule_delta.release(s);
     ex->counters.release(s);
     ex->status.release(s);
@@ -753,6 +835,33 @@ void sparkalog_executor_destroy(sparkalog_executor* ex) {
     }
     for (cudaEvent_t e : ex->free_events) cudaEventDestroy(e);
     delete ex;
+}
+
+int sparkalog_executor_track_segments(sparkalog_executor* ex, u32 shift, u32 count) {
+    if (!ex || shift > 31) return fail(SPARKALOG_E_INVALID_ARGUMENT, "invalid segment tracking arguments");
+    cudaStream_t s = nullptr;
+    ex->seg_shift = shift;
+    ex->seg_count = count;
+    if (count) {
+        SPK_CUDA(ex->seg_seen.ensure(static_cast<size_t>(count) * 4, s), "cudaMallocAsync");
+        SPK_CUDA(ex->seg_new.ensure(static_cast<size_t>(count) * 8, s), "cudaMallocAsync");
+        SPK_CUDA(cudaMemsetAsync(ex->seg_seen.ptr, 0, static_cast<size_t>(count) * 4, s), "cudaMemsetAsync");
+        SPK_CUDA(cudaMemsetAsync(ex->seg_new.ptr, 0, static_cast<size_t>(count) * 8, s), "cudaMemsetAsync");
+        SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    }
+    return 0;
+}
+
+int sparkalog_executor_segment_stats(sparkalog_executor* ex, u32* last_active_round, u64* new_rows) {
+    if (!ex || !last_active_round || !new_rows) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null argument");
+    if (ex->seg_count == 0) return 0;
+    SPK_CUDA(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+    SPK_CUDA(cudaMemcpy(last_active_round, ex->seg_seen.ptr, static_cast<size_t>(ex->seg_count) * 4,
+                        cudaMemcpyDeviceToHost),
+             "cudaMemcpy");
+    SPK_CUDA(cudaMemcpy(new_rows, ex->seg_new.ptr, static_cast<size_t>(ex->seg_count) * 8, cudaMemcpyDeviceToHost),
+             "cudaMemcpy");
+    return 0;
 }
 
 int sparkalog_executor_set_profiling(sparkalog_executor* ex, int enable) {
@@ -1083,6 +1192,13 @@ int sparkalog_executor_run(sparkalog_executor* ex, sparkalog_store* st, size_t m
                     tr.level_n[l] = 0;
                     tr.dir_valid[l - 1] = tr.dir_valid[l] = false;
                 }
+            }
+            if (ex->seg_count && newt_n > 0) {
+                spk::segment_activity_kernel<<<simple_grid(newt_n), 256, 0, s>>>(
+                    tr.newt.as<u64>(), newt_n, ex->seg_shift, ex->seg_count, static_cast<u32>(iterations + 1),
+                    ex->seg_seen.as<u32>(), ex->seg_new.as<unsigned long long>());
+                SPK_CUDA(cudaGetLastError(), "segment_activity_kernel");
+                ex->stats.total_launches += 1;
             }
             swap_arrays(tr.delta, tr.newt);
             tr.delta_n = newt_n;

@@ -189,6 +189,29 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_kernel(const u64* bu
     }
 }
 
+// Per-segment activity of one round's NEWT rows (sorted, so a segment's rows
+// are contiguous): seen[seg] = max(seen[seg], round1), new_rows[seg] += rows.
+// Lanes holding the same segment are grouped with match.any and one lane per
+// group updates the counters.
+static __global__ void segment_activity_kernel(const u64* rows, u64 n, u32 shift, u32 count, u32 round1,
+                                               u32* seen, unsigned long long* new_rows) {
+    const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+    const u64 rounds = (n + stride - 1) / stride;
+    for (u64 r = 0; r < rounds; ++r) {
+        const u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x + r * stride;
+        u32 seg = 0xffffffffu;
+        if (i < n) {
+            const u32 s = static_cast<u32>(rows[i] >> 32) >> shift;
+            seg = s < count ? s : 0xffffffffu;
+        }
+        const u32 peers = __match_any_sync(0xffffffffu, seg);
+        if (seg != 0xffffffffu && (peers & lanemask_lt()) == 0) {
+            atomicMax(&seen[seg], round1);
+            atomicAdd(&new_rows[seg], static_cast<unsigned long long>(__popc(peers)));
+        }
+    }
+}
+
 // Diagonal splits for merge_disjoint_kernel: splits[t] = number of `a` rows
 // among the first t * tile merged rows, for t in [0, tiles]; one thread per
 // diagonal.

@@ -135,6 +135,13 @@ class RelationStore:
         """RelationStore::delta (generic.rs:85-91)."""
         return self._read(rid, DELTA)
 
+    def anti_join(self, left: RelationId | int, right: RelationId | int, out: RelationId | int) -> int:
+        """Stores ``out(x, y) :- left(x, y), !right(x, y).`` as a new static relation
+        (GeneralCpu's clause evaluation, general.rs:478-551); returns its row count."""
+        ids = [int(getattr(r, "value", r)) for r in (left, right, out)]
+        _check(_native.load().sparkalog_store_anti_join(self._h, *ids))
+        return self.rows(ids[2])
+
     def read_into(self, rid: RelationId | int, version: int, first, second) -> int:
         """Copies FULL/DELTA into caller buffers (numpy host arrays, possibly pinned, or device tensors)."""
         n = self.rows(rid, version)
@@ -208,6 +215,21 @@ class RecursiveExecutor:
         return SccSummary(int(s.iterations), int(s.total_new_rows),
                           [(RelationId(int(ids[i])), int(rows[i])) for i in range(n)])
 
+
+    def track_segments(self, shift: int, count: int) -> None:
+        """Records per-segment (first column >> shift) activity each round; see segment_stats."""
+        _check(_native.load().sparkalog_executor_track_segments(self._h, shift, count))
+        self._segments = count
+
+    def segment_stats(self) -> tuple[np.ndarray, np.ndarray]:
+        """(last_active_round, new_rows) per segment: a segment that gained rows in
+        round r (0-based) has last_active_round >= r + 1."""
+        n = getattr(self, "_segments", 0)
+        seen = np.zeros(max(n, 1), dtype=np.uint32)
+        new = np.zeros(max(n, 1), dtype=np.uint64)
+        _check(_native.load().sparkalog_executor_segment_stats(self._h, seen.ctypes.data_as(_native.c_u32p),
+                                                               new.ctypes.data_as(_native.c_u64p)))
+        return seen[:n], new[:n]
 
     def set_profiling(self, enable: bool) -> None:
         """Times every kernel class with CUDA events on the store's stream."""

@@ -1,0 +1,73 @@
+"""CPU tests of host-side logic that needs no GPU: batching tags and splits,
+workload generators, x-range partitioning."""
+
+import numpy as np
+import pytest
+
+from sparkalog_b200 import generators
+
+
+def test_batched_tagging_and_split():
+    from sparkalog_b200.batched import BatchedTransitiveClosure
+
+    inst = [(np.array([2, 0, 2], np.uint32), np.array([3, 1, 3], np.uint32)),
+            (np.zeros(0, np.uint32), np.zeros(0, np.uint32)),
+            (np.array([5], np.uint32), np.array([6], np.uint32))]
+    b = BatchedTransitiveClosure(inst, id_bits=4)
+    f, s = b.tagged_edges()
+    assert f.tolist() == [0, 2, 32 + 5] and s.tolist() == [1, 3, 32 + 6]
+    assert np.all(np.diff((f.astype(np.uint64) << np.uint64(32)) | s) > 0)
+    seen = np.array([0, 0, 1], np.uint32)
+    new = np.array([0, 0, 0], np.uint64)
+    res = b.split(f, s, seen, new)
+    assert [r.path[0].tolist() for r in res] == [[0, 2], [], [5]]
+    assert [r.iterations for r in res] == [1, 0, 2]
+
+
+def test_batched_rejects_out_of_range_ids():
+    from sparkalog_b200.batched import BatchedTransitiveClosure
+
+    with pytest.raises(ValueError):
+        BatchedTransitiveClosure([(np.array([16], np.uint32), np.array([1], np.uint32))], id_bits=4)
+    with pytest.raises(ValueError):
+        BatchedTransitiveClosure([(np.zeros(0, np.uint32), np.zeros(0, np.uint32))] * 17, id_bits=28)
+
+
+def test_batched_instance_parameters():
+    params = generators.batched_instances(4096, 3)
+    n = np.array([p.nodes for p in params])
+    d = np.array([p.degree for p in params])
+    assert n.min() >= 64 and n.max() <= 16384
+    assert d.min() >= 0.5 and d.max() <= 1.2
+    # log-uniform node counts: about half the instances below the geometric mean.
+    assert 0.45 < np.mean(n < 1024) < 0.55
+    assert generators.batched_instances(10, 3)[4] == params[4]
+
+
+def test_served_requests_stream():
+    reqs = generators.served_requests(2000, 500.0, 9)
+    arrivals = np.array([r.arrival_s for r in reqs])
+    assert np.all(np.diff(arrivals) > 0)
+    assert abs(len(reqs) / arrivals[-1] - 500.0) < 50.0
+    e = np.array([r.edges for r in reqs])
+    assert e.min() >= 1000 and e.max() <= 4_000_000
+    assert all(0.6 <= r.degree <= 0.95 for r in reqs)
+
+
+def test_uniform_pairs_dedup_and_sorted():
+    c0, c1 = generators.uniform_pairs(50, 5000, 1)
+    packed = (c0.astype(np.uint64) << np.uint64(32)) | c1
+    assert np.all(np.diff(packed) > 0)
+    assert c0.max() < 50 and c1.max() < 50
+
+
+def test_bench_partition_covers_every_row():
+    import bench
+
+    src, dst = generators.er_edges(1000, 3000, 4)
+    parts = [bench.partition(src, dst, 1000, r, 3) for r in range(3)]
+    assert sum(len(p[0]) for p in parts) == len(src)
+    assert np.array_equal(np.concatenate([p[0] for p in parts]), src)
+    for r, (s, _) in enumerate(parts):
+        if len(s):
+            assert s.min() >= 1000 * r // 3 and s.max() < 1000 * (r + 1) // 3
