@@ -223,6 +223,33 @@ SPARKALOG_API void sparkalog_executor_destroy(sparkalog_executor* executor);
 SPARKALOG_API int sparkalog_executor_run(sparkalog_executor* executor, sparkalog_store* store,
                                          size_t max_iterations, sparkalog_scc_summary* summary);
 
+/* ---- Serving: relations stay resident while requests join and leave ----
+ * No counterparts in the reference, whose Database re-runs every fixpoint
+ * from scratch after an insert (database.rs:82-112). Requests are kept apart
+ * by a tag in the high bits of both columns (a "segment": first >> shift). */
+
+/* Runs at most `rounds` rounds of the loop (no error at the limit);
+ * *converged = 1 when every DELTA of the SCC is empty afterwards. */
+SPARKALOG_API int sparkalog_executor_step(sparkalog_executor* executor, sparkalog_store* store, size_t rounds,
+                                          sparkalog_scc_summary* summary, int* converged);
+
+/* FULL(id) u= rows, and for a recursive relation also DELTA(id) u= (rows not
+ * already in FULL), so the next round derives from them: new facts join a
+ * resident fixpoint. Rows may be unsorted and may repeat. */
+SPARKALOG_API int sparkalog_store_append(sparkalog_store* store, uint32_t id, const uint32_t* first,
+                                         const uint32_t* second, size_t rows, int location);
+
+/* Copies the rows of FULL(id) whose first >> shift == segment, sorted, into
+ * (first, second); with first == NULL only *rows is set. */
+SPARKALOG_API int sparkalog_store_extract_segment(sparkalog_store* store, uint32_t id, uint32_t shift,
+                                                  uint32_t segment, uint32_t* first, uint32_t* second,
+                                                  int location, size_t* rows);
+
+/* Removes every row whose first >> shift is one of `segments` from FULL and
+ * DELTA of relation id (a completed request's rows, freeing its tag). */
+SPARKALOG_API int sparkalog_store_remove_segments(sparkalog_store* store, uint32_t id, uint32_t shift,
+                                                  const uint32_t* segments, size_t count);
+
 /* Per-kernel-class statistics of an executor, measured with CUDA events on
  * the executor's stream while profiling is enabled. No counterpart in the
  * reference (which has no tracing); used to report achieved HBM bandwidth.
@@ -259,6 +286,11 @@ SPARKALOG_API int sparkalog_executor_segment_stats(sparkalog_executor* executor,
 
 SPARKALOG_API int sparkalog_executor_set_profiling(sparkalog_executor* executor, int enable);
 SPARKALOG_API int sparkalog_executor_stats(sparkalog_executor* executor, sparkalog_kernel_stats* out, int reset);
+
+/* Grows the current device's stream-ordered memory pool to at least `bytes`
+ * and keeps it (relations are allocated from it), so a long-running process
+ * does not pay for pool growth inside its first large requests. */
+SPARKALOG_API int sparkalog_reserve_device_memory(size_t bytes, void* stream);
 
 /* Thread-local description of the last failure. */
 SPARKALOG_API const char* sparkalog_last_error(void);

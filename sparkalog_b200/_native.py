@@ -41,12 +41,17 @@ TIER_B = [
     "sparkalog_store_read",
     "sparkalog_store_anti_join",
     "sparkalog_executor_compile",
+    "sparkalog_executor_step",
+    "sparkalog_store_append",
+    "sparkalog_store_extract_segment",
+    "sparkalog_store_remove_segments",
     "sparkalog_executor_destroy",
     "sparkalog_executor_run",
     "sparkalog_executor_track_segments",
     "sparkalog_executor_segment_stats",
     "sparkalog_executor_set_profiling",
     "sparkalog_executor_stats",
+    "sparkalog_reserve_device_memory",
     "sparkalog_last_error",
 ]
 EXPORTED = TIER_A + TIER_B
@@ -147,6 +152,16 @@ def load() -> ctypes.CDLL:
     L.sparkalog_store_read.restype = i
     L.sparkalog_store_anti_join.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]
     L.sparkalog_store_anti_join.restype = i
+    L.sparkalog_executor_step.argtypes = [vp, vp, ctypes.c_size_t, ctypes.POINTER(SccSummaryC),
+                                          ctypes.POINTER(ctypes.c_int)]
+    L.sparkalog_executor_step.restype = i
+    L.sparkalog_store_append.argtypes = [vp, ctypes.c_uint32, vp, vp, ctypes.c_size_t, i]
+    L.sparkalog_store_append.restype = i
+    L.sparkalog_store_extract_segment.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, vp, vp, i,
+                                                  c_sizep]
+    L.sparkalog_store_extract_segment.restype = i
+    L.sparkalog_store_remove_segments.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, c_u32p, ctypes.c_size_t]
+    L.sparkalog_store_remove_segments.restype = i
     L.sparkalog_executor_compile.argtypes = [vp, c_u32p, ctypes.c_size_t, ctypes.POINTER(RulePlanC), ctypes.c_size_t,
                                              ctypes.POINTER(vp)]
     L.sparkalog_executor_compile.restype = i
@@ -162,6 +177,8 @@ def load() -> ctypes.CDLL:
     L.sparkalog_executor_set_profiling.restype = i
     L.sparkalog_executor_stats.argtypes = [vp, ctypes.POINTER(KernelStatsC), i]
     L.sparkalog_executor_stats.restype = i
+    L.sparkalog_reserve_device_memory.argtypes = [ctypes.c_size_t, vp]
+    L.sparkalog_reserve_device_memory.restype = i
     L.sparkalog_last_error.argtypes = []
     L.sparkalog_last_error.restype = ctypes.c_char_p
     _lib = L

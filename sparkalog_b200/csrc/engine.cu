@@ -140,6 +140,7 @@ struct RelState {
     DevArray spare;         // merge destination, swapped with a level after a merge
     DevArray delta, newt;
     u64 delta_n = 0;
+    bool delta_sorted = true;  // DELTA is sorted and unique (always after a round)
 
     u64 full_rows() const {
         u64 n = 0;
@@ -150,6 +151,8 @@ struct RelState {
 
 }  // namespace
 
+struct StoreOps;
+
 struct sparkalog_store {
     cudaStream_t stream = nullptr;
     std::map<u32, RelState> relations;
@@ -157,6 +160,7 @@ struct sparkalog_store {
     DevArray flags;            // device flag words
     DevArray merge_splits;     // diagonal splits of the merge pre-pass
     u32 max_value = 0;         // largest value stored in any column
+    StoreOps* ops = nullptr;   // scratch of store-level operations (anti-join, append, segments)
     u32* pinned = nullptr;     // small pinned host buffer
 
     RelState* find(u32 id) {
@@ -282,11 +286,19 @@ struct IndexCache {
     u32 relation = 0;
     u64 version = 0;
     u32 column = 0;
-    DevArray offsets;   // u32[num_keys + 1]
+    DevArray offsets;   // u32[num_keys + 1] (dense index)
     DevArray rows;      // u32[n] (empty when identity)
     bool identity = true;
     u64 num_keys = 0;
     u32 max_degree = 0;
+    // Bucketed index, used when the key domain is much larger than the row
+    // count (tagged serving keys): sorted first-column keys plus a bucket
+    // directory over them, instead of max_key + 1 dense offsets.
+    bool bucketed = false;
+    DevArray keys32;    // u32[n]
+    DevArray bucket_dir;
+    u32 bucket_shift = 0;
+    u64 buckets = 0;
 };
 
 struct TargetRT {
@@ -318,6 +330,7 @@ struct sparkalog_executor {
     // Batched runs: per-segment (instance) activity, see sparkalog_executor_track_segments.
     u32 seg_shift = 0;
     u32 seg_count = 0;
+    u64 rounds_total = 0;        // rounds executed over the executor's lifetime (all run/step calls)
     DevArray seg_seen;           // u32[seg_count]
     DevArray seg_new;            // u64[seg_count]
 
@@ -421,6 +434,121 @@ size_t target_count_base(const sparkalog_executor* ex, size_t t) {
     return base;
 }
 
+}  // namespace
+
+// Scratch of store-level operations: a rule-less executor supplies the sort
+// scratch, look-back epochs and launch counting; the rest are buffers.
+struct StoreOps {
+    sparkalog_executor ex;
+    DevArray a, b;       // sort ping-pong of operation inputs
+    DevArray counts;     // u64 words
+    DevArray counters;   // u32 tile counters; error bits at word 32
+    DevArray status;     // look-back words
+    DevArray bitmap;     // dead-segment bitmap
+    u64* host = nullptr; // pinned 256 bytes
+};
+
+namespace {
+
+StoreOps& store_ops(sparkalog_store* st) {
+    if (!st->ops) {
+        auto* ops = new StoreOps();
+        cudaStream_t s = st->stream;
+        ops->counts.ensure(256, s);
+        ops->counters.ensure(256, s);
+        cudaMemsetAsync(ops->counters.ptr, 0, 256, s);
+        cudaMallocHost(&ops->host, 256);
+        st->ops = ops;
+    }
+    StoreOps& ops = *st->ops;
+    if (ops.ex.epoch > spk::kEpochMask - 4096) {
+        cudaStream_t s = st->stream;
+        if (ops.status.ptr) cudaMemsetAsync(ops.status.ptr, 0, ops.status.bytes, s);
+        if (ops.ex.index_sort.status.ptr) cudaMemsetAsync(ops.ex.index_sort.status.ptr, 0, ops.ex.index_sort.status.bytes, s);
+        ops.ex.epoch = 1;
+    }
+    return ops;
+}
+
+void release_store_ops(sparkalog_store* st) {
+    if (!st->ops) return;
+    cudaStream_t s = st->stream;
+    StoreOps& o = *st->ops;
+    for (DevArray* d : {&o.a, &o.b, &o.counts, &o.counters, &o.status, &o.bitmap, &o.ex.index_sort.plan,
+                        &o.ex.index_sort.status})
+        d->release(s);
+    cudaStreamSynchronize(s);
+    if (o.host) cudaFreeHost(o.host);
+    delete st->ops;
+    st->ops = nullptr;
+}
+
+int refresh_directories(sparkalog_store* st, RelState& r, cudaStream_t s, u64* launches);
+
+// out = sort + unique of the n packed rows in ops.a, minus every FULL level of
+// `right` (the anti-join of GeneralCpu negation, and the novelty check of an
+// append). ops.b is the sort's second buffer.
+int sorted_difference(sparkalog_store* st, u64 n, RelState& right, DevArray& out, u64* out_n) {
+    cudaStream_t s = st->stream;
+    StoreOps& ops = store_ops(st);
+    u32* err = ops.counters.as<u32>() + 32;
+    SPK_CUDA(ops.b.ensure(n * 8, s), "cudaMallocAsync");
+    SPK_CUDA(out.ensure(std::max<u64>(n, 1) * 8, s), "cudaMallocAsync");
+    int rc = radix_sort(ops.a.as<u64>(), ops.b.as<u64>(), nullptr, n, ops.ex.index_sort, &ops.ex, err, s, nullptr,
+                        nullptr);
+    if (rc) return rc;
+    rc = refresh_directories(st, right, s, nullptr);
+    if (rc) return rc;
+    spk::Levels lv{};
+    lv.n = 0;
+    for (int l = 0; l < spk::kMaxLevels; ++l) {
+        if (right.level_n[l] == 0) continue;
+        lv.keys[lv.n] = right.level[l].as<u64>();
+        lv.count[lv.n] = right.level_n[l];
+        lv.dir[lv.n] = right.dir[l].as<u32>();
+        lv.shift[lv.n] = right.dir_shift[l];
+        lv.buckets[lv.n] = right.dir_buckets[l];
+        ++lv.n;
+    }
+    SPK_CUDA(ops.status.ensure_zeroed(((n + kSetTile - 1) / kSetTile + 1) * 8, s), "cudaMallocAsync");
+    SPK_CUDA(cudaMemsetAsync(ops.counters.ptr, 0, 32 * 4, s), "cudaMemsetAsync");
+    ops.host[0] = n;
+    u64* nptr = ops.counts.as<u64>() + 1;
+    SPK_CUDA(cudaMemcpyAsync(nptr, ops.host, 8, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
+    auto kernel = spk::anti_join_levels_kernel<kThreads, kSetItems, kLevelStage>;
+    const size_t tiles = (n + kSetTile - 1) / kSetTile;
+    kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, tiles), kThreads, 0, s>>>(
+        ops.a.as<u64>(), ops.b.as<u64>(), &ops.ex.index_sort.plan.as<spk::RadixPlan>()->final_sel, nptr, lv,
+        out.as<u64>(), ops.counts.as<u64>(), ops.status.as<u64>(), ops.counters.as<u32>(), ops.ex.epoch++, err);
+    SPK_CUDA(cudaGetLastError(), "anti_join_levels_kernel");
+    SPK_CUDA(cudaMemcpyAsync(ops.host, ops.counts.ptr, 8, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+    SPK_CUDA(cudaMemcpyAsync(ops.host + 1, err, 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+    SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    const u32 bits = static_cast<u32>(ops.host[1] & 0xffffffffu);
+    if (bits) return fail(SPARKALOG_E_DEVICE_FAULT, "device error bits " + std::to_string(bits));
+    *out_n = ops.host[0];
+    return 0;
+}
+
+// Sorts and deduplicates DELTA of r in place (it may have been inserted unsorted).
+int sort_unique_delta(sparkalog_store* st, RelState& r) {
+    cudaStream_t s = st->stream;
+    StoreOps& ops = store_ops(st);
+    if (r.delta_n) {
+        SPK_CUDA(ops.a.ensure(r.delta_n * 8, s), "cudaMallocAsync");
+        SPK_CUDA(cudaMemcpyAsync(ops.a.ptr, r.delta.ptr, r.delta_n * 8, cudaMemcpyDeviceToDevice, s),
+                 "cudaMemcpyAsync");
+        RelState none;
+        u64 n = 0;
+        int rc = sorted_difference(st, r.delta_n, none, r.newt, &n);
+        if (rc) return rc;
+        swap_arrays(r.delta, r.newt);
+        r.delta_n = n;
+    }
+    r.delta_sorted = true;
+    return 0;
+}
+
 int build_index_impl(sparkalog_executor* ex, sparkalog_store* st, IndexCache& ic, u32 relation, u32 column);
 
 // Builds a rule's right index; its kernels are counted as launches but kept
@@ -478,10 +606,31 @@ int build_index_impl(sparkalog_executor* ex, sparkalog_store* st, IndexCache& ic
         SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
     }
     ic.num_keys = n ? (last >> 32) + 1 : 0;
-    SPK_CUDA(ic.offsets.ensure((ic.num_keys + 1) * 4, s), "cudaMallocAsync");
     u32* maxdeg = ex->counters.as<u32>() + kErrWord + 1;
     SPK_CUDA(cudaMemsetAsync(maxdeg, 0, 4, s), "cudaMemsetAsync");
-    if (n) {
+    ic.bucketed = n && ic.num_keys > std::max<u64>(4 * n, u64(1) << 22);
+    if (ic.bucketed) {
+        // ~8 keys per bucket.
+        const u64 max_key = last >> 32;
+        const int key_bits = 64 - __builtin_clzll(max_key | 1);
+        const int target_bits = 64 - __builtin_clzll(std::max<u64>(n / 8, 1));
+        ic.bucket_shift = static_cast<u32>(std::max(0, key_bits - target_bits));
+        ic.buckets = (max_key >> ic.bucket_shift) + 1;
+        SPK_CUDA(ic.keys32.ensure(n * 4, s), "cudaMallocAsync");
+        SPK_CUDA(ic.bucket_dir.ensure((ic.buckets + 1) * 4, s), "cudaMallocAsync");
+        spk::high_words_kernel<<<simple_grid(n), 256, 0, s>>>(sorted_keys, n, ic.keys32.as<u32>());
+        SPK_CUDA(cudaGetLastError(), "high_words_kernel");
+        spk::key_directory_kernel<<<simple_grid(ic.buckets + 1), 256, 0, s>>>(ic.keys32.as<u32>(), n, ic.bucket_shift,
+                                                                             ic.buckets, ic.bucket_dir.as<u32>());
+        SPK_CUDA(cudaGetLastError(), "key_directory_kernel");
+        spk::max_run_kernel<<<simple_grid(n), 256, 0, s>>>(sorted_keys, n, maxdeg);
+        SPK_CUDA(cudaGetLastError(), "max_run_kernel");
+        ex->stats.total_launches += ic.identity ? 3 : 5;
+    } else {
+        SPK_CUDA(ic.offsets.ensure((ic.num_keys + 1) * 4, s), "cudaMallocAsync");
+    }
+    if (ic.bucketed) {
+    } else if (n) {
         spk::dense_offsets_kernel<<<simple_grid(n), 256, 0, s>>>(sorted_keys, n, ic.num_keys, ic.offsets.as<u32>(),
                                                                  maxdeg);
         SPK_CUDA(cudaGetLastError(), "dense_offsets_kernel");
@@ -507,6 +656,22 @@ bool valid_cols(const u32 c[2]) { return c[0] <= 1 && c[1] <= 1; }
 extern "C" {
 
 const char* sparkalog_last_error(void) { return g_last_error.c_str(); }
+
+int sparkalog_reserve_device_memory(size_t bytes, void* stream) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int dev = 0;
+    cudaMemPool_t pool;
+    SPK_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+    SPK_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev), "cudaDeviceGetDefaultMemPool");
+    uint64_t threshold = ~0ull;
+    SPK_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold), "cudaMemPoolSetAttribute");
+    if (bytes == 0) return 0;
+    void* p = nullptr;
+    SPK_CUDA(cudaMallocAsync(&p, bytes, s), "cudaMallocAsync");
+    SPK_CUDA(cudaFreeAsync(p, s), "cudaFreeAsync");
+    SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    return 0;
+}
 
 int sparkalog_store_create(void* stream, sparkalog_store** out) {
     if (!out) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null output pointer");
@@ -547,6 +712,7 @@ void sparkalog_store_destroy(sparkalog_store* st) {
     st->scratch_u32[1].release(s);
     st->flags.release(s);
     st->merge_splits.release(s);
+    release_store_ops(st);
     cudaStreamSynchronize(s);
     if (st->pinned) cudaFreeHost(st->pinned);
     delete st;
@@ -585,10 +751,12 @@ int sparkalog_store_insert_recursive(sparkalog_store* st, u32 id, const u32* ful
             SPK_CUDA(cudaMemcpyAsync(r.delta.ptr, r.level[0].ptr, full_rows * 8, cudaMemcpyDeviceToDevice,
                                      st->stream),
                      "cudaMemcpyAsync");
+        r.delta_sorted = r.sorted && !r.has_dups;
     } else {
         bool dsorted, ddups;
         rc = pack_columns(st, delta_first, delta_second, delta_rows, location, r.delta, &dsorted, &ddups);
         if (rc) return rc;
+        r.delta_sorted = dsorted && !ddups;
     }
     r.delta_n = delta_rows;
     SPK_CUDA(r.newt.ensure(4096, st->stream), "cudaMallocAsync");
@@ -659,67 +827,189 @@ int sparkalog_store_anti_join(sparkalog_store* st, u32 left_id, u32 right_id, u3
     cudaStream_t s = st->stream;
     int rc = materialize(*left, st->merge_splits, s);
     if (rc) return rc;
-    rc = materialize(*right, st->merge_splits, s);
-    if (rc) return rc;
     if (!right->sorted && right->level_n[0] > 1)
         return fail(SPARKALOG_E_UNSORTED_FULL, "FULL of relation " + std::to_string(right_id) + " is not sorted");
-    sparkalog_executor scratch;  // sort scratch, look-back buffers and epochs for this one operation
     const u64 n = left->level_n[0];
     RelState out;
-    SPK_CUDA(out.level[0].ensure(std::max<u64>(n, 1) * 8, s), "cudaMallocAsync");
     u64 out_n = 0;
     if (n > 0) {
-        DevArray a, b, counts;
-        SPK_CUDA(a.ensure(n * 8, s), "cudaMallocAsync");
-        SPK_CUDA(b.ensure(n * 8, s), "cudaMallocAsync");
-        SPK_CUDA(counts.ensure(64, s), "cudaMallocAsync");
-        SPK_CUDA(scratch.counters.ensure((kCounterWords + 64) * 4, s), "cudaMallocAsync");
-        SPK_CUDA(cudaMemsetAsync(scratch.counters.ptr, 0, (kCounterWords + 64) * 4, s), "cudaMemsetAsync");
-        SPK_CUDA(cudaMemcpyAsync(a.ptr, left->level[0].ptr, n * 8, cudaMemcpyDeviceToDevice, s), "cudaMemcpyAsync");
-        u32* err = scratch.counters.as<u32>() + kErrWord;
-        rc = radix_sort(a.as<u64>(), b.as<u64>(), nullptr, n, scratch.index_sort, &scratch, err, s, nullptr, nullptr);
+        StoreOps& ops = store_ops(st);
+        SPK_CUDA(ops.a.ensure(n * 8, s), "cudaMallocAsync");
+        SPK_CUDA(cudaMemcpyAsync(ops.a.ptr, left->level[0].ptr, n * 8, cudaMemcpyDeviceToDevice, s), "cudaMemcpyAsync");
+        rc = sorted_difference(st, n, *right, out.level[0], &out_n);
         if (rc) return rc;
-        rc = refresh_directories(st, *right, s, nullptr);
-        if (rc) return rc;
-        spk::Levels lv{};
-        lv.n = 0;
-        if (right->level_n[0] > 0) {
-            lv.keys[0] = right->level[0].as<u64>();
-            lv.count[0] = right->level_n[0];
-            lv.dir[0] = right->dir[0].as<u32>();
-            lv.shift[0] = right->dir_shift[0];
-            lv.buckets[0] = right->dir_buckets[0];
-            lv.n = 1;
-        }
-        SPK_CUDA(scratch.status.ensure_zeroed(((n + kSetTile - 1) / kSetTile + 1) * 8, s), "cudaMallocAsync");
-        u64* nptr = counts.as<u64>() + 1;
-        SPK_CUDA(cudaMemcpyAsync(nptr, &left->level_n[0], 8, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
-        auto kernel = spk::anti_join_levels_kernel<kThreads, kSetItems, kLevelStage>;
-        const size_t tiles = (n + kSetTile - 1) / kSetTile;
-        kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, tiles), kThreads, 0, s>>>(
-            a.as<u64>(), b.as<u64>(), &scratch.index_sort.plan.as<spk::RadixPlan>()->final_sel, nptr, lv,
-            out.level[0].as<u64>(), counts.as<u64>(), scratch.status.as<u64>(), scratch.counters.as<u32>(),
-            scratch.epoch++, err);
-        SPK_CUDA(cudaGetLastError(), "anti_join_levels_kernel");
-        u64 host[2] = {0, 0};
-        SPK_CUDA(cudaMemcpyAsync(st->pinned, counts.ptr, 8, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
-        SPK_CUDA(cudaMemcpyAsync(st->pinned + 2, err, 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
-        SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
-        std::memcpy(host, st->pinned, 8);
-        if (st->pinned[2]) return fail(SPARKALOG_E_DEVICE_FAULT, "device error bits " + std::to_string(st->pinned[2]));
-        out_n = host[0];
-        a.release(s);
-        b.release(s);
-        counts.release(s);
-        scratch.counters.release(s);
-        scratch.status.release(s);
-        scratch.index_sort.plan.release(s);
-        scratch.index_sort.status.release(s);
+    } else {
+        SPK_CUDA(out.level[0].ensure(8, s), "cudaMallocAsync");
     }
     out.level_n[0] = out_n;
     out.sorted = true;
     out.has_dups = false;
     st->relations[out_id] = std::move(out);
+    return 0;
+}
+
+int sparkalog_store_append(sparkalog_store* st, u32 id, const u32* first, const u32* second, size_t rows,
+                           int location) {
+    if (!st) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null store");
+    RelState* r = st->find(id);
+    if (!r) return fail(SPARKALOG_E_MISSING, "relation " + std::to_string(id) + " is not registered");
+    if (rows > 0xffffffffull) return fail(SPARKALOG_E_TOO_MANY_ROWS, "too many rows for u32 row ids");
+    if (rows == 0) return 0;
+    cudaStream_t s = st->stream;
+    if (!r->sorted || r->has_dups) {
+        int rc = materialize(*r, st->merge_splits, s);
+        if (rc) return rc;
+        if (!r->sorted) return fail(SPARKALOG_E_UNSORTED_FULL, "FULL of relation " + std::to_string(id) + " is not sorted");
+    }
+    StoreOps& ops = store_ops(st);
+    bool sorted_in, dups_in;
+    int rc = pack_columns(st, first, second, rows, location, ops.a, &sorted_in, &dups_in);
+    if (rc) return rc;
+    DevArray fresh;
+    u64 fresh_n = 0;
+    rc = sorted_difference(st, rows, *r, fresh, &fresh_n);
+    if (rc) return rc;
+    if (fresh_n > 0) {
+        // FULL: new rows are disjoint from every level, so they merge into TAIL
+        // (level 0 for a static relation, which keeps a single run).
+        const int l = r->recursive ? spk::kMaxLevels - 1 : 0;
+        const u64 tn = r->level_n[l] + fresh_n;
+        SPK_CUDA(r->spare.ensure(tn * 8, s), "cudaMallocAsync");
+        SPK_CUDA(launch_merge(r->level[l].as<u64>(), r->level_n[l], fresh.as<u64>(), fresh_n, r->spare.as<u64>(),
+                              st->merge_splits, s),
+                 "merge_disjoint_kernel");
+        swap_arrays(r->level[l], r->spare);
+        r->level_n[l] = tn;
+        r->dir_valid[l] = false;
+        if (r->recursive) {
+            // DELTA u= fresh rows (DELTA is part of FULL, so they are disjoint).
+            if (!r->delta_sorted) {
+                rc = sort_unique_delta(st, *r);
+                if (rc) return rc;
+            }
+            const u64 dn = r->delta_n + fresh_n;
+            SPK_CUDA(r->newt.ensure(std::max<u64>(dn, 1) * 8, s), "cudaMallocAsync");
+            SPK_CUDA(launch_merge(r->delta.as<u64>(), r->delta_n, fresh.as<u64>(), fresh_n, r->newt.as<u64>(),
+                                  st->merge_splits, s),
+                     "merge_disjoint_kernel");
+            swap_arrays(r->delta, r->newt);
+            r->delta_n = dn;
+        }
+        r->version += 1;
+    }
+    SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    fresh.release(s);
+    return 0;
+}
+
+int sparkalog_store_extract_segment(sparkalog_store* st, u32 id, u32 shift, u32 segment, u32* first, u32* second,
+                                    int location, size_t* rows) {
+    if (!st || !rows || shift > 31) return fail(SPARKALOG_E_INVALID_ARGUMENT, "invalid argument");
+    RelState* r = st->find(id);
+    if (!r) return fail(SPARKALOG_E_MISSING, "relation " + std::to_string(id) + " is not registered");
+    cudaStream_t s = st->stream;
+    if (!r->sorted) return fail(SPARKALOG_E_UNSORTED_FULL, "FULL of relation " + std::to_string(id) + " is not sorted");
+    const u64 lo_key = static_cast<u64>(segment) << (shift + 32);
+    const u64 next = static_cast<u64>(segment) + 1;
+    const u64 hi_key = (next << shift) > 0xffffffffull ? ~0ull : next << (shift + 32);
+    spk::Levels lv{};
+    int map[spk::kMaxLevels];
+    for (int l = 0; l < spk::kMaxLevels; ++l) {
+        if (r->level_n[l] == 0) continue;
+        map[lv.n] = l;
+        lv.keys[lv.n] = r->level[l].as<u64>();
+        lv.count[lv.n] = r->level_n[l];
+        ++lv.n;
+    }
+    StoreOps& ops = store_ops(st);
+    u64 bounds[2 * spk::kMaxLevels] = {0};
+    if (lv.n) {
+        spk::level_bounds_kernel<<<1, 32, 0, s>>>(lv, lo_key, hi_key, ops.counts.as<u64>());
+        SPK_CUDA(cudaGetLastError(), "level_bounds_kernel");
+        SPK_CUDA(cudaMemcpyAsync(ops.host, ops.counts.ptr, sizeof(bounds), cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+        SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+        std::memcpy(bounds, ops.host, sizeof(bounds));
+    }
+    u64 total = 0;
+    for (int k = 0; k < lv.n; ++k) total += bounds[2 * k + 1] - bounds[2 * k];
+    *rows = total;
+    if (!first) return 0;
+    if (!second) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null output column");
+    if (total == 0) return 0;
+    // Merge the (disjoint, sorted) slices of the levels into one sorted run.
+    SPK_CUDA(ops.a.ensure(total * 8, s), "cudaMallocAsync");
+    SPK_CUDA(ops.b.ensure(total * 8, s), "cudaMallocAsync");
+    u64 have = 0;
+    for (int k = 0; k < lv.n; ++k) {
+        const u64 len = bounds[2 * k + 1] - bounds[2 * k];
+        if (len == 0) continue;
+        const u64* slice = r->level[map[k]].as<u64>() + bounds[2 * k];
+        SPK_CUDA(launch_merge(ops.a.as<u64>(), have, slice, len, ops.b.as<u64>(), st->merge_splits, s),
+                 "merge_disjoint_kernel");
+        swap_arrays(ops.a, ops.b);
+        have += len;
+    }
+    u32* d0 = first;
+    u32* d1 = second;
+    if (location == SPARKALOG_HOST) {
+        SPK_CUDA(st->scratch_u32[0].ensure(total * 4, s), "cudaMallocAsync");
+        SPK_CUDA(st->scratch_u32[1].ensure(total * 4, s), "cudaMallocAsync");
+        d0 = st->scratch_u32[0].as<u32>();
+        d1 = st->scratch_u32[1].as<u32>();
+    }
+    spk::unpack_rows_kernel<<<simple_grid(total), 256, 0, s>>>(ops.a.as<u64>(), total, d0, d1);
+    SPK_CUDA(cudaGetLastError(), "unpack_rows_kernel");
+    if (location == SPARKALOG_HOST) {
+        SPK_CUDA(cudaMemcpyAsync(first, d0, total * 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+        SPK_CUDA(cudaMemcpyAsync(second, d1, total * 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+    }
+    SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    return 0;
+}
+
+int sparkalog_store_remove_segments(sparkalog_store* st, u32 id, u32 shift, const u32* segments, size_t count) {
+    if (!st || shift > 31 || (count && !segments)) return fail(SPARKALOG_E_INVALID_ARGUMENT, "invalid argument");
+    RelState* r = st->find(id);
+    if (!r) return fail(SPARKALOG_E_MISSING, "relation " + std::to_string(id) + " is not registered");
+    if (count == 0) return 0;
+    cudaStream_t s = st->stream;
+    const u64 segs = 1ull << (32 - shift);
+    const u64 words = (segs + 31) / 32;
+    std::vector<u32> bitmap(words, 0);
+    for (size_t k = 0; k < count; ++k) {
+        if (segments[k] >= segs) return fail(SPARKALOG_E_INVALID_ARGUMENT, "segment out of range");
+        bitmap[segments[k] >> 5] |= 1u << (segments[k] & 31);
+    }
+    StoreOps& ops = store_ops(st);
+    SPK_CUDA(ops.bitmap.ensure(words * 4, s), "cudaMallocAsync");
+    SPK_CUDA(cudaMemcpyAsync(ops.bitmap.ptr, bitmap.data(), words * 4, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
+    auto filter = [&](DevArray& buf, u64& n, DevArray& spare) -> int {
+        if (n == 0) return 0;
+        SPK_CUDA(spare.ensure(n * 8, s), "cudaMallocAsync");
+        SPK_CUDA(ops.status.ensure_zeroed(((n + kSetTile - 1) / kSetTile + 1) * 8, s), "cudaMallocAsync");
+        SPK_CUDA(cudaMemsetAsync(ops.counters.ptr, 0, 64, s), "cudaMemsetAsync");
+        auto kernel = spk::filter_segments_kernel<kThreads, kSetItems>;
+        const size_t tiles = (n + kSetTile - 1) / kSetTile;
+        kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, tiles), kThreads, 0, s>>>(
+            buf.as<u64>(), n, shift, ops.bitmap.as<u32>(), spare.as<u64>(), ops.counts.as<u64>(),
+            ops.status.as<u64>(), ops.counters.as<u32>(), ops.ex.epoch++, ops.counters.as<u32>() + 32);
+        SPK_CUDA(cudaGetLastError(), "filter_segments_kernel");
+        SPK_CUDA(cudaMemcpyAsync(ops.host, ops.counts.ptr, 8, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+        SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+        swap_arrays(buf, spare);
+        std::memcpy(&n, ops.host, 8);
+        return 0;
+    };
+    for (int l = 0; l < spk::kMaxLevels; ++l) {
+        int rc = filter(r->level[l], r->level_n[l], r->spare);
+        if (rc) return rc;
+        r->dir_valid[l] = false;
+    }
+    if (r->recursive) {
+        int rc = filter(r->delta, r->delta_n, r->newt);
+        if (rc) return rc;
+    }
+    r->version += 1;
     return 0;
 }
 
@@ -814,6 +1104,8 @@ void sparkalog_executor_destroy(sparkalog_executor* ex) {
     for (auto& ic : ex->index) {
         ic.offsets.release(s);
         ic.rows.release(s);
+        ic.keys32.release(s);
+        ic.bucket_dir.release(s);
     }
     ex->counts.release(s);
     ex->seg_seen.release(s);
@@ -877,8 +1169,12 @@ int sparkalog_executor_stats(sparkalog_executor* ex, sparkalog_kernel_stats* out
     return 0;
 }
 
-int sparkalog_executor_run(sparkalog_executor* ex, sparkalog_store* st, size_t max_iterations,
-                           sparkalog_scc_summary* summary) {
+// Runs rounds while any DELTA of the SCC is non-empty, at most max_iterations
+// of them. With limit_is_error the limit is RecursiveExecutor::run's
+// IterationLimit error; otherwise the call just stops (a step of a serving
+// loop). *converged reports whether every DELTA is empty afterwards.
+static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_iterations, bool limit_is_error,
+                      sparkalog_scc_summary* summary, int* converged) {
     if (!ex || !st) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null argument");
     cudaStream_t s = st->stream;
     for (const auto& p : ex->rules) {
@@ -906,6 +1202,7 @@ int sparkalog_executor_run(sparkalog_executor* ex, sparkalog_store* st, size_t m
     if (any_delta) {
         for (u32 id : ex->relations) {
             RelState& r = *st->find(id);
+            if (r.sorted && !r.has_dups) continue;  // levels are already sorted, disjoint runs
             int rc = materialize(r, st->merge_splits, s);
             if (rc) return rc;
             if (!r.sorted)
@@ -949,6 +1246,7 @@ int sparkalog_executor_run(sparkalog_executor* ex, sparkalog_store* st, size_t m
         }
         if (!has_delta) break;
         if (iterations >= max_iterations) {
+            if (!limit_is_error) break;
             if (summary) {
                 summary->iterations = iterations;
                 summary->total_new_rows = total_new;
@@ -1029,8 +1327,16 @@ int sparkalog_executor_run(sparkalog_executor* ex, sparkalog_store* st, size_t m
                     a.delta = d.delta.as<u64>();
                     a.delta_count = ex->rule_delta.as<u64>() + k;
                     a.left_key = p.left_key;
-                    a.dense_offsets = ic.offsets.as<u32>();
-                    a.dense_keys = ic.num_keys;
+                    if (ic.bucketed) {
+                        a.dense_offsets = nullptr;
+                        a.bucket_dir = ic.bucket_dir.as<u32>();
+                        a.bucket_shift = ic.bucket_shift;
+                        a.buckets = ic.buckets;
+                        a.keys = ic.keys32.as<u32>();
+                    } else {
+                        a.dense_offsets = ic.offsets.as<u32>();
+                        a.dense_keys = ic.num_keys;
+                    }
                     a.rows = ic.identity ? nullptr : ic.rows.as<u32>();
                     a.right = right.level[0].as<u64>();
                     a.side[0] = p.proj_side[0];
@@ -1195,18 +1501,20 @@ int sparkalog_executor_run(sparkalog_executor* ex, sparkalog_store* st, size_t m
             }
             if (ex->seg_count && newt_n > 0) {
                 spk::segment_activity_kernel<<<simple_grid(newt_n), 256, 0, s>>>(
-                    tr.newt.as<u64>(), newt_n, ex->seg_shift, ex->seg_count, static_cast<u32>(iterations + 1),
+                    tr.newt.as<u64>(), newt_n, ex->seg_shift, ex->seg_count, static_cast<u32>(ex->rounds_total + 1),
                     ex->seg_seen.as<u32>(), ex->seg_new.as<unsigned long long>());
                 SPK_CUDA(cudaGetLastError(), "segment_activity_kernel");
                 ex->stats.total_launches += 1;
             }
             swap_arrays(tr.delta, tr.newt);
             tr.delta_n = newt_n;
+            tr.delta_sorted = true;
             tr.version += 1;
             total_new += newt_n;
         }
         iterations += 1;
         ex->stats.rounds += 1;
+        ex->rounds_total += 1;
     }
     SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
     ex->collect();
@@ -1222,7 +1530,22 @@ int sparkalog_executor_run(sparkalog_executor* ex, sparkalog_store* st, size_t m
         }
         summary->relation_count = ex->relations.size();
     }
+    if (converged) {
+        bool any = false;
+        for (u32 id : ex->relations) any |= st->find(id)->delta_n != 0;
+        *converged = any ? 0 : 1;
+    }
     return 0;
+}
+
+int sparkalog_executor_run(sparkalog_executor* ex, sparkalog_store* st, size_t max_iterations,
+                           sparkalog_scc_summary* summary) {
+    return run_rounds(ex, st, max_iterations, true, summary, nullptr);
+}
+
+int sparkalog_executor_step(sparkalog_executor* ex, sparkalog_store* st, size_t rounds,
+                            sparkalog_scc_summary* summary, int* converged) {
+    return run_rounds(ex, st, rounds, false, summary, converged);
 }
 
 }  // extern "C"

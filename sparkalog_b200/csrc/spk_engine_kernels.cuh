@@ -212,6 +212,104 @@ static __global__ void segment_activity_kernel(const u64* rows, u64 n, u32 shift
     }
 }
 
+// Row range of one key interval [lo_key, hi_key) in every level: out[2l] and
+// out[2l + 1] are the lower bounds of lo_key and hi_key in level l.
+static __global__ void level_bounds_kernel(Levels levels, u64 lo_key, u64 hi_key, u64* out) {
+    const int l = static_cast<int>(threadIdx.x);
+    if (l >= levels.n) return;
+    const PackedKeys k{levels.keys[l]};
+    out[2 * l] = lower_bound_keys(k, 0, levels.count[l], lo_key);
+    out[2 * l + 1] = lower_bound_keys(k, 0, levels.count[l], hi_key);
+}
+
+// Compaction that drops every row whose segment (first column >> shift) is
+// set in the `dead` bitmap; order is kept (decoupled look-back offsets).
+template <int THREADS, int ITEMS>
+__global__ void __launch_bounds__(THREADS) filter_segments_kernel(const u64* in, u64 n, u32 shift, const u32* dead,
+                                                                  u64* out, u64* out_count, u64* status,
+                                                                  u32* tile_counter, u32 epoch, u32* err) {
+    constexpr int kTile = THREADS * ITEMS;
+    __shared__ CompactShared<THREADS> cs;
+    __shared__ u64 stage[kTile];
+    const u64 num_tiles = (n + kTile - 1) / kTile;
+    if (num_tiles == 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) *out_count = 0;
+        return;
+    }
+    for (;;) {
+        if (threadIdx.x == 0) cs.tile = atomicAdd(tile_counter, 1u);
+        __syncthreads();
+        const u64 tile = cs.tile;
+        if (tile >= num_tiles) break;
+        const u64 base = tile * kTile + static_cast<u64>(threadIdx.x) * ITEMS;
+        u64 v[ITEMS];
+        u32 keep = 0;
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i) {
+            const u64 idx = base + i;
+            v[i] = 0;
+            if (idx < n) {
+                v[i] = in[idx];
+                const u32 seg = static_cast<u32>(v[i] >> 32) >> shift;
+                if (!((dead[seg >> 5] >> (seg & 31)) & 1u)) keep |= 1u << i;
+            }
+        }
+        u32 excl, total;
+        const u64 off = compact_offsets<THREADS>(__popc(keep), &excl, &total, tile, status, epoch, err, cs);
+        u32 w = excl;
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i)
+            if (keep & (1u << i)) stage[w++] = v[i];
+        __syncthreads();
+        for (u32 j = threadIdx.x; j < total; j += THREADS) out[off + j] = stage[j];
+        if (tile == num_tiles - 1 && threadIdx.x == 0) *out_count = off + total;
+        __syncthreads();
+    }
+}
+
+// Longest run of equal first-column keys in sorted rows (the index's largest
+// match count, which bounds a join's output).
+static __global__ void max_run_kernel(const u64* sorted, u64 n, u32* max_degree) {
+    const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+    u32 local_max = 0;
+    for (u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const u32 key = static_cast<u32>(sorted[i] >> 32);
+        if (i == 0 || static_cast<u32>(sorted[i - 1] >> 32) != key) {
+            u64 j = i + 1;
+            while (j < n && static_cast<u32>(sorted[j] >> 32) == key) ++j;
+            const u32 len = static_cast<u32>(j - i);
+            local_max = len > local_max ? len : local_max;
+        }
+    }
+    atomicMax(max_degree, local_max);
+}
+
+// First-column keys of an index (high words of packed rows or pairs).
+static __global__ void high_words_kernel(const u64* in, u64 n, u32* out) {
+    const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+    for (u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+        out[i] = static_cast<u32>(in[i] >> 32);
+}
+
+// Bucket directory over sorted u32 keys: dir[b] = lower bound of b << shift.
+static __global__ void key_directory_kernel(const u32* keys, u64 n, u32 shift, u64 buckets, u32* dir) {
+    const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+    for (u64 b = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; b <= buckets; b += stride) {
+        if (b == buckets) {
+            dir[b] = static_cast<u32>(n);
+            continue;
+        }
+        const u64 key = b << shift;
+        u64 lo = 0, hi = n;
+        while (lo < hi) {
+            const u64 mid = (lo + hi) >> 1;
+            if (static_cast<u64>(keys[mid]) < key) lo = mid + 1;
+            else hi = mid;
+        }
+        dir[b] = static_cast<u32>(lo);
+    }
+}
+
 // Diagonal splits for merge_disjoint_kernel: splits[t] = number of `a` rows
 // among the first t * tile merged rows, for t in [0, tiles]; one thread per
 // diagonal.

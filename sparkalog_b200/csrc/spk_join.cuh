@@ -174,9 +174,12 @@ struct FusedJoinArgs {
     u32 left_key;             // 0: first column of DELTA, 1: second
     const u32* dense_offsets; // dense CSR over key values [0, dense_keys], or null
     u64 dense_keys;
-    const u32* keys;          // sparse U32RangeIndex fallback (keys/starts)
+    const u32* keys;          // sparse U32RangeIndex (keys/starts), or the bucketed index's sorted keys
     const u32* starts;
     u64 unique_keys;
+    const u32* bucket_dir;    // bucketed index: dir[b] = first position whose key >> bucket_shift >= b
+    u32 bucket_shift;
+    u64 buckets;
     const u32* rows;          // index rows; null means identity (index built on a sorted column)
     const u64* right;         // packed right relation rows
     u32 side[2];              // 0: left, 1: right
@@ -232,6 +235,26 @@ __global__ void __launch_bounds__(THREADS) join_fused_kernel(FusedJoinArgs a) {
                     if (key < a.dense_keys) {
                         begin = a.dense_offsets[key];
                         cnt[i] = a.dense_offsets[key + 1] - begin;
+                    }
+                } else if (a.bucket_dir) {
+                    // Sparse key domain: the key's bucket bounds a short search
+                    // for the first and one-past-last position of the key.
+                    const u64 b = static_cast<u64>(key) >> a.bucket_shift;
+                    if (b < a.buckets) {
+                        u64 lo = a.bucket_dir[b], hi = a.bucket_dir[b + 1];
+                        while (lo < hi) {
+                            const u64 mid = (lo + hi) >> 1;
+                            if (a.keys[mid] < key) lo = mid + 1;
+                            else hi = mid;
+                        }
+                        u64 up = lo, top = a.bucket_dir[b + 1];
+                        while (up < top) {
+                            const u64 mid = (up + top) >> 1;
+                            if (a.keys[mid] <= key) up = mid + 1;
+                            else top = mid;
+                        }
+                        begin = static_cast<u32>(lo);
+                        cnt[i] = static_cast<u32>(up - lo);
                     }
                 } else {
                     const long long idx = find_index_key(a.keys, a.unique_keys, key);

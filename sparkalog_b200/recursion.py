@@ -142,6 +142,31 @@ class RelationStore:
         _check(_native.load().sparkalog_store_anti_join(self._h, *ids))
         return self.rows(ids[2])
 
+    def append(self, rid: RelationId | int, relation) -> None:
+        """FULL u= rows (and DELTA u= the genuinely new rows of a recursive relation),
+        so a resident fixpoint continues from them."""
+        p0, p1, n, loc, keep = self._columns(relation)
+        _check(_native.load().sparkalog_store_append(self._h, int(getattr(rid, "value", rid)), p0, p1, n, loc))
+        del keep
+
+    def extract_segment(self, rid: RelationId | int, shift: int, segment: int) -> tuple[np.ndarray, np.ndarray]:
+        """Sorted rows of FULL whose first column >> shift == segment."""
+        L = _native.load()
+        rid = int(getattr(rid, "value", rid))
+        n = ctypes.c_size_t(0)
+        _check(L.sparkalog_store_extract_segment(self._h, rid, shift, segment, None, None, HOST, ctypes.byref(n)))
+        a = np.empty(max(n.value, 1), dtype=np.uint32)
+        b = np.empty(max(n.value, 1), dtype=np.uint32)
+        _check(L.sparkalog_store_extract_segment(self._h, rid, shift, segment, a.ctypes.data, b.ctypes.data, HOST,
+                                                 ctypes.byref(n)))
+        return a[: n.value], b[: n.value]
+
+    def remove_segments(self, rid: RelationId | int, shift: int, segments) -> None:
+        """Drops every row whose first column >> shift is in ``segments`` from FULL and DELTA."""
+        segs = _u32(list(segments))
+        _check(_native.load().sparkalog_store_remove_segments(self._h, int(getattr(rid, "value", rid)), shift,
+                                                              segs.ctypes.data_as(_native.c_u32p), len(segs)))
+
     def read_into(self, rid: RelationId | int, version: int, first, second) -> int:
         """Copies FULL/DELTA into caller buffers (numpy host arrays, possibly pinned, or device tensors)."""
         n = self.rows(rid, version)
@@ -216,6 +241,22 @@ class RecursiveExecutor:
                           [(RelationId(int(ids[i])), int(rows[i])) for i in range(n)])
 
 
+    def step(self, store: RelationStore, rounds: int = 1) -> tuple[SccSummary, bool]:
+        """Runs at most ``rounds`` rounds (no error at the limit); returns the
+        summary of those rounds and whether every DELTA is now empty."""
+        n = len(self.plan.relations)
+        ids = (ctypes.c_uint32 * max(n, 1))()
+        rows = (ctypes.c_uint64 * max(n, 1))()
+        s = _native.SccSummaryC()
+        s.relation_count = n
+        s.relation_ids = ids
+        s.relation_rows = rows
+        conv = ctypes.c_int(0)
+        _check(_native.load().sparkalog_executor_step(self._h, store.handle, rounds, ctypes.byref(s),
+                                                      ctypes.byref(conv)))
+        return (SccSummary(int(s.iterations), int(s.total_new_rows),
+                           [(RelationId(int(ids[i])), int(rows[i])) for i in range(n)]), bool(conv.value))
+
     def track_segments(self, shift: int, count: int) -> None:
         """Records per-segment (first column >> shift) activity each round; see segment_stats."""
         _check(_native.load().sparkalog_executor_track_segments(self._h, shift, count))
@@ -242,6 +283,12 @@ class RecursiveExecutor:
         classes = {name: {"launches": int(s.launches[i]), "ms": float(s.milliseconds[i]),
                           "bytes": float(s.bytes[i])} for i, name in enumerate(_native.KERNEL_CLASSES)}
         return {"classes": classes, "total_launches": int(s.total_launches), "rounds": int(s.rounds)}
+
+
+def reserve_device_memory(nbytes: int, stream: torch.cuda.Stream | None = None) -> None:
+    """Grows and keeps the device memory pool that relations are allocated from."""
+    s = stream if stream is not None else torch.cuda.current_stream()
+    _check(_native.load().sparkalog_reserve_device_memory(int(nbytes), s.cuda_stream))
 
 
 def transitive_closure_scc(path: RelationId, edge: RelationId) -> RecursiveSccPlan:

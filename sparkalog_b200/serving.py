@@ -1,0 +1,266 @@
+"""Serving: continuous batching of transitive-closure requests on one GPU.
+
+Each request is the TC program over its own edge set. The server keeps one
+device-resident store: relation 0 is the union of every admitted request's
+EDB, relation 1 the union of their path relations, each request's rows tagged
+with a slot number in the high bits of both columns (node ids keep the low
+``id_bits``). One shared RecursiveExecutor advances every active request by a
+round at a time, so the iterations of concurrent requests run in the same
+kernel launches. Between rounds the server
+
+* admits requests that have arrived, while a slot is free and the HBM budget
+  (estimated from each request's edge count times the FULL/EDB growth seen in
+  earlier requests) allows: their tagged edges are appended to the EDB and,
+  as seed, to FULL and DELTA of the path relation, which starts their
+  fixpoints (crates/sparkalog-datalog/src/subset.rs:381-408 seeds path with
+  the edges the same way);
+* completes every request that derived no new rows in the last round: its
+  DELTA is empty, so its fixpoint is done. Its FULL slice is copied out and
+  its slot is retired; retired slots' rows are purged from the store in one
+  pass when free slots run out or the budget needs the room.
+
+Per request, the result (rows and iteration count) equals the request run
+alone: tags keep requests disjoint, and the executor's per-segment activity
+gives each one the number of rounds its own RecursiveExecutor::run would take.
+"""
+
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .recursion import RecursiveExecutor, RelationStore, transitive_closure_scc
+from .relational import RelationId
+
+EDB, PATH = 0, 1
+
+
+@dataclass
+class ServeRequest:
+    request_id: int
+    arrival_s: float
+    src: np.ndarray
+    dst: np.ndarray
+
+
+@dataclass
+class Completion:
+    request_id: int
+    path: tuple[np.ndarray, np.ndarray]
+    iterations: int
+    new_rows: int
+    arrival_s: float
+    admitted_s: float
+    finished_s: float
+
+    @property
+    def latency_s(self) -> float:
+        return self.finished_s - self.arrival_s
+
+
+@dataclass
+class _Active:
+    request: ServeRequest
+    slot: int
+    admit_round: int
+    admitted_s: float
+    base_new_rows: int
+    est_bytes: float
+
+
+class FixpointServer:
+    """Continuous-batching TC server over one device-resident store."""
+
+    def __init__(self, id_bits: int = 23, budget_bytes: float = 120e9, growth_prior: float = 16.0, stream=None,
+                 clock=time.perf_counter):
+        self.shift = id_bits
+        self.slots = 1 << (32 - id_bits)
+        self.budget = budget_bytes
+        self.growth = growth_prior
+        self.clock = clock
+        self.store = RelationStore(stream)
+        empty = (np.zeros(0, dtype=np.uint32), np.zeros(0, dtype=np.uint32))
+        self.store.insert_static(EDB, empty)
+        self.store.insert_recursive(PATH, empty, empty)
+        self.executor = RecursiveExecutor.compile(transitive_closure_scc(RelationId(PATH), RelationId(EDB)),
+                                                  self.store)
+        self.executor.track_segments(self.shift, self.slots)
+        self.free = list(range(self.slots - 1, -1, -1))
+        self.retired: list[int] = []
+        self.retired_bytes = 0.0
+        self.active: dict[int, _Active] = {}
+        self.rounds = 0
+        self.completions: list[Completion] = []
+
+    # ------------------------------------------------------------ admission
+
+    def estimate_bytes(self, edges: int) -> float:
+        """HBM estimate of one request: EDB + FULL rows (8 B packed) with the
+        growth factor observed so far, doubled for merge and sort buffers."""
+        return 16.0 * edges * (1.0 + self.growth)
+
+    def resident_bytes(self) -> float:
+        return sum(a.est_bytes for a in self.active.values()) + self.retired_bytes
+
+    def can_admit(self, request: ServeRequest, batch: list[ServeRequest] = ()) -> bool:
+        """Whether `request` fits next to the active requests and the `batch`
+        already chosen for admission (a free slot each, and the HBM budget)."""
+        if len(self.free) <= len(batch) and self.retired:
+            self.purge()
+        if len(self.free) <= len(batch):
+            return False
+        reserved = sum(self.estimate_bytes(len(r.src)) for r in batch)
+        need = self.estimate_bytes(len(request.src))
+        if self.resident_bytes() + reserved + need > self.budget and self.retired:
+            self.purge()
+        return self.resident_bytes() + reserved + need <= self.budget or (not self.active and not batch)
+
+    def admit(self, requests: list[ServeRequest]) -> None:
+        """Appends the requests' tagged edges to the EDB and, as seed, to FULL/DELTA of path."""
+        if not requests:
+            return
+        now = self.clock()
+        _, new_rows = self.executor.segment_stats()
+        firsts, seconds = [], []
+        for req in requests:
+            slot = self.free.pop()
+            # Raw edge lists: the device append sorts and deduplicates them.
+            s = np.asarray(req.src, dtype=np.uint32)
+            d = np.asarray(req.dst, dtype=np.uint32)
+            if len(s) and max(int(s.max()), int(d.max())) >= (1 << self.shift):
+                raise ValueError(f"request {req.request_id} has node ids >= 2^{self.shift}")
+            tag = np.uint32(slot << self.shift)
+            firsts.append(s | tag)
+            seconds.append(d | tag)
+            if len(s) == 0:
+                # No seed: the fixpoint runs zero rounds.
+                self.completions.append(Completion(req.request_id, (s, d), 0, 0, req.arrival_s, now, now))
+                self.free.append(slot)
+                continue
+            self.active[slot] = _Active(req, slot, self.rounds, now, int(new_rows[slot]),
+                                        self.estimate_bytes(len(s)))
+        first, second = np.concatenate(firsts), np.concatenate(seconds)
+        if len(first):
+            self.store.append(EDB, (first, second))
+            self.store.append(PATH, (first, second))
+
+    # ------------------------------------------------------------ rounds
+
+    def step(self) -> list[Completion]:
+        """One round for every active request, then completes the finished ones."""
+        if not self.active:
+            return []
+        summary, _ = self.executor.step(self.store, 1)
+        self.rounds += summary.iterations
+        seen, new_rows = self.executor.segment_stats()
+        done = [slot for slot in self.active if int(seen[slot]) != self.rounds]
+        finished = []
+        now = None
+        for slot in done:
+            a = self.active.pop(slot)
+            f0, f1 = self.store.extract_segment(PATH, self.shift, slot)
+            mask = np.uint32((1 << self.shift) - 1)
+            iterations = int(seen[slot]) - a.admit_round + 1 if int(seen[slot]) > a.admit_round else 1
+            now = self.clock()
+            c = Completion(a.request.request_id, (f0 & mask, f1 & mask), iterations,
+                           int(new_rows[slot]) - a.base_new_rows, a.request.arrival_s, a.admitted_s, now)
+            finished.append(c)
+            edges = max(len(a.request.src), 1)
+            self.growth = 0.8 * self.growth + 0.2 * (len(f0) / edges)
+            self.retired.append(slot)
+            self.retired_bytes += 16.0 * (len(f0) + edges)
+        self.completions.extend(finished)
+        return finished
+
+    def purge(self) -> None:
+        """Removes every retired request's rows from the store and frees its slot."""
+        if not self.retired:
+            return
+        self.store.remove_segments(EDB, self.shift, self.retired)
+        self.store.remove_segments(PATH, self.shift, self.retired)
+        self.free.extend(self.retired)
+        self.retired = []
+        self.retired_bytes = 0.0
+
+    def close(self) -> None:
+        self.executor.close()
+        self.store.close()
+
+
+@dataclass
+class ServeReport:
+    completions: list[Completion] = field(default_factory=list)
+    wall_s: float = 0.0
+    rounds: int = 0
+
+    def latencies(self) -> np.ndarray:
+        return np.array([c.latency_s for c in self.completions])
+
+    def summary(self) -> dict:
+        lat = self.latencies()
+        tuples = sum(c.new_rows for c in self.completions)
+        return {"requests": len(self.completions), "wall_s": self.wall_s,
+                "p50_ms": float(np.percentile(lat, 50) * 1e3) if len(lat) else None,
+                "p99_ms": float(np.percentile(lat, 99) * 1e3) if len(lat) else None,
+                "requests_per_s": len(self.completions) / self.wall_s if self.wall_s else None,
+                "derived_tuples_per_s": tuples / self.wall_s if self.wall_s else None,
+                "rounds": self.rounds}
+
+
+def serve(requests: list[ServeRequest], server: FixpointServer, realtime: bool = True) -> ServeReport:
+    """Replays an arrival stream against the continuous-batching server."""
+    pending = sorted(requests, key=lambda r: r.arrival_s)
+    start = server.clock()
+    server.clock = (lambda base=server.clock: base() - start)
+    i = 0
+    while i < len(pending) or server.active:
+        now = server.clock()
+        batch = []
+        while i < len(pending) and (pending[i].arrival_s <= now or not realtime):
+            if not server.can_admit(pending[i], batch):
+                break
+            batch.append(pending[i])
+            i += 1
+        server.admit(batch)
+        if server.active:
+            server.step()
+        elif i < len(pending):
+            wait = pending[i].arrival_s - server.clock()
+            if wait > 0:
+                time.sleep(wait)
+    report = ServeReport(list(server.completions), server.clock(), server.rounds)
+    return report
+
+
+def serve_one_at_a_time(requests: list[ServeRequest], stream=None, realtime: bool = True,
+                        clock=time.perf_counter) -> ServeReport:
+    """The baseline: a FIFO loop that runs each request alone through the same engine."""
+    pending = sorted(requests, key=lambda r: r.arrival_s)
+    start = clock()
+    now = lambda: clock() - start
+    report = ServeReport()
+    for req in pending:
+        if realtime and req.arrival_s > now():
+            time.sleep(req.arrival_s - now())
+        admitted = now()
+        s = np.asarray(req.src, dtype=np.uint32)
+        d = np.asarray(req.dst, dtype=np.uint32)
+        empty = (np.zeros(0, dtype=np.uint32), np.zeros(0, dtype=np.uint32))
+        store = RelationStore(stream)
+        store.insert_static(EDB, empty)
+        store.insert_recursive(PATH, empty, empty)
+        # Same device-side sort/deduplication of the raw edges as the server.
+        store.append(EDB, (s, d))
+        store.append(PATH, (s, d))
+        ex = RecursiveExecutor.compile(transitive_closure_scc(RelationId(PATH), RelationId(EDB)), store)
+        summary = ex.run(store)
+        path = store.full(PATH)
+        ex.close()
+        store.close()
+        report.rounds += summary.iterations
+        report.completions.append(Completion(req.request_id, path, summary.iterations, summary.total_new_rows,
+                                             req.arrival_s, admitted, now()))
+    report.wall_s = now()
+    return report
