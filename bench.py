@@ -82,11 +82,9 @@ def measured_peaks():
 
 def partition(src, dst, nodes, rank, world):
     """Seed rows whose x lies in this rank's contiguous node range."""
-    lo = nodes * rank // world
-    hi = nodes * (rank + 1) // world
-    a = np.searchsorted(src, lo, side="left")
-    b = np.searchsorted(src, hi, side="left")
-    return src[a:b], dst[a:b]
+    from sparkalog_b200.sharding import partition_seed
+
+    return partition_seed(src, dst, nodes, rank, world)
 
 
 class ClockSampler:
