@@ -263,6 +263,7 @@ enum {
     SPARKALOG_K_ANTI_JOIN = 3,   /* unique + anti-join against the FULL levels */
     SPARKALOG_K_MERGE = 4,       /* merge of NEWT / levels */
     SPARKALOG_K_INDEX = 5,       /* right-relation index build */
+    SPARKALOG_K_FUSED = 6,       /* fused join + distinct (then the anti-join) */
     SPARKALOG_K_CLASSES = 8
 };
 typedef struct sparkalog_kernel_stats {
@@ -285,6 +286,12 @@ SPARKALOG_API int sparkalog_executor_segment_stats(sparkalog_executor* executor,
                                                    uint64_t* new_rows);
 
 SPARKALOG_API int sparkalog_executor_set_profiling(sparkalog_executor* executor, int enable);
+
+/* Enables (default) or disables the fused join + distinct kernel for rules
+ * whose join output starts with DELTA's first column. Disabled, every round
+ * runs the general join, radix sort and anti-join; results are identical. No
+ * counterpart in the reference. */
+SPARKALOG_API int sparkalog_executor_set_fused(sparkalog_executor* executor, int enable);
 SPARKALOG_API int sparkalog_executor_stats(sparkalog_executor* executor, sparkalog_kernel_stats* out, int reset);
 
 /* Grows the current device's stream-ordered memory pool to at least `bytes`

@@ -50,6 +50,7 @@ TIER_B = [
     "sparkalog_executor_track_segments",
     "sparkalog_executor_segment_stats",
     "sparkalog_executor_set_profiling",
+    "sparkalog_executor_set_fused",
     "sparkalog_executor_stats",
     "sparkalog_reserve_device_memory",
     "sparkalog_last_error",
@@ -88,7 +89,7 @@ class SccSummaryC(ctypes.Structure):
     ]
 
 
-KERNEL_CLASSES = ["join", "sort_histogram", "sort_pass", "anti_join", "merge", "index"]
+KERNEL_CLASSES = ["join", "sort_histogram", "sort_pass", "anti_join", "merge", "index", "join_distinct"]
 
 
 class KernelStatsC(ctypes.Structure):
@@ -175,6 +176,8 @@ def load() -> ctypes.CDLL:
     L.sparkalog_executor_segment_stats.restype = i
     L.sparkalog_executor_set_profiling.argtypes = [vp, i]
     L.sparkalog_executor_set_profiling.restype = i
+    L.sparkalog_executor_set_fused.argtypes = [vp, i]
+    L.sparkalog_executor_set_fused.restype = i
     L.sparkalog_executor_stats.argtypes = [vp, ctypes.POINTER(KernelStatsC), i]
     L.sparkalog_executor_stats.restype = i
     L.sparkalog_reserve_device_memory.argtypes = [ctypes.c_size_t, vp]

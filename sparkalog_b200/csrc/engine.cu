@@ -26,9 +26,11 @@
 #include "spk_host.h"
 #include "spk_join.cuh"
 #include "spk_radix.cuh"
+#include "spk_fused.cuh"
 #include "spk_setops.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -307,6 +309,8 @@ struct TargetRT {
     DevArray j_a, j_b;     // candidate buffers (sort ping-pong)
     u64 j_cap = 0;         // elements
     SortScratch sort;
+    u32 fused_rows = 1024; // nominal DELTA rows per fused tile (halved when tiles overflow)
+    bool force_generic = false;  // redo the current round with the general kernels
 };
 
 }  // namespace
@@ -342,6 +346,7 @@ struct sparkalog_executor {
         u64 launches;
     };
     bool profiling = false;
+    bool fused_enabled = true;
     std::vector<cudaEvent_t> free_events;
     std::vector<Timing> timings;
     sparkalog_kernel_stats stats{};
@@ -432,6 +437,44 @@ size_t target_count_base(const sparkalog_executor* ex, size_t t) {
     size_t base = 0;
     for (size_t i = 0; i < t; ++i) base += ex->targets[i].rules.size() + 2;
     return base;
+}
+
+constexpr int kFusedThreads = 256;
+constexpr int kFusedCap = 3840;     // join output rows per fused tile (shared memory)
+constexpr int kFusedRowCap = 2048;  // DELTA rows per fused tile
+constexpr size_t kFusedFlagBase = 8;      // fallback flags live at err + 8 + target
+constexpr size_t kFusedMaxTargets = 48;
+
+// The fused round applies to a target with one rule whose join output starts
+// with DELTA's first column (then the join output is sorted by it) while
+// DELTA is sorted.
+bool fused_eligible(const sparkalog_executor* ex, sparkalog_store* st, size_t ti) {
+    const TargetRT& t = ex->targets[ti];
+    if (!ex->fused_enabled || t.force_generic || t.rules.size() != 1 || ti >= kFusedMaxTargets) return false;
+    const sparkalog_rule_plan& p = ex->rules[t.rules[0]];
+    if (p.proj_side[0] != 0 || p.proj_col[0] != 0) return false;
+    const RelState* d = st->find(p.delta_input);
+    return d && d->delta_sorted;
+}
+
+int launch_fused(const spk::FusedRoundArgs& a, size_t tiles, cudaStream_t s) {
+    auto kernel = spk::fused_join_distinct_kernel<kFusedThreads, kFusedCap, kFusedRowCap>;
+    constexpr size_t smem = spk::FusedLayout<kFusedThreads, kFusedCap, kFusedRowCap>::kBytes;
+    // The shared-memory opt-in is per device.
+    static std::atomic<u64> configured{0};
+    int device = 0;
+    SPK_CUDA(cudaGetDevice(&device), "cudaGetDevice");
+    const u64 bit = 1ull << (device & 63);
+    if (!(configured.load() & bit)) {
+        SPK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+                 "cudaFuncSetAttribute");
+        configured.fetch_or(bit);
+    }
+    const unsigned grid = spk::persistent_grid(reinterpret_cast<const void*>(kernel), kFusedThreads, smem,
+                                               std::max<size_t>(tiles, 1));
+    kernel<<<grid, kFusedThreads, smem, s>>>(a);
+    SPK_CUDA(cudaGetLastError(), "fused_join_distinct_kernel");
+    return 0;
 }
 
 }  // namespace
@@ -1080,7 +1123,7 @@ int sparkalog_executor_compile(sparkalog_store* st, const u32* relations, size_t
     cudaError_t e = ex->counts.ensure(ex->counts_words * 8, s);
     if (e == cudaSuccess) e = ex->counters.ensure((kCounterWords + 64) * 4, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(ex->counters.ptr, 0, (kCounterWords + 64) * 4, s);
-    if (e == cudaSuccess) e = cudaMallocHost(&ex->host_counts, ex->counts_words * 8 + 64);
+    if (e == cudaSuccess) e = cudaMallocHost(&ex->host_counts, ex->counts_words * 8 + 512);
     if (e == cudaSuccess) e = ex->rule_delta.ensure(std::max<size_t>(rule_count, 1) * 8, s);
     if (e == cudaSuccess) e = cudaMallocHost(&ex->host_rule_delta, std::max<size_t>(rule_count, 1) * 8);
     if (e == cudaSuccess) e = cudaMallocHost(&ex->host_active, relation_count * spk::kMaxPasses * 4 + 64);
@@ -1159,6 +1202,12 @@ int sparkalog_executor_segment_stats(sparkalog_executor* ex, u32* last_active_ro
 int sparkalog_executor_set_profiling(sparkalog_executor* ex, int enable) {
     if (!ex) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null executor");
     ex->profiling = enable != 0;
+    return 0;
+}
+
+int sparkalog_executor_set_fused(sparkalog_executor* ex, int enable) {
+    if (!ex) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null executor");
+    ex->fused_enabled = enable != 0;
     return 0;
 }
 
@@ -1307,15 +1356,27 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
             for (auto& t : ex->targets) {
                 SPK_CUDA(st->find(t.id)->newt.ensure(t.j_cap * 8, s), "cudaMallocAsync");
                 max_status_words = std::max<size_t>(max_status_words, (t.j_cap + kSetTile - 1) / kSetTile + 1);
+                // Fused tiles are DELTA-row tiles: one status word each.
+                u64 delta_rows = 0;
+                for (size_t k : t.rules) delta_rows += ex->host_rule_delta[k];
+                max_status_words = std::max<size_t>(max_status_words, (delta_rows + t.fused_rows - 1) / t.fused_rows + 1);
             }
             SPK_CUDA(ex->status.ensure_zeroed(max_status_words * 8, s), "cudaMallocAsync");
-            SPK_CUDA(cudaMemsetAsync(counters, 0, (kCounterWords + 1) * 4, s), "cudaMemsetAsync");
+            SPK_CUDA(cudaMemsetAsync(counters, 0, (kCounterWords + kFusedFlagBase + kFusedMaxTargets) * 4, s),
+                     "cudaMemsetAsync");
             SPK_CUDA(cudaMemsetAsync(counts, 0, ex->counts_words * 8, s), "cudaMemsetAsync");
             size_t counter_slot = 0;
+            // Targets whose single rule projects DELTA's first column (the
+            // transitive-closure shape) run the fused round kernel; the rest
+            // join, radix sort and anti-join with the general kernels.
+            std::vector<char> fused(ex->targets.size(), 0);
+            for (size_t ti = 0; ti < ex->targets.size(); ++ti) fused[ti] = fused_eligible(ex, st, ti) ? 1 : 0;
             const int join_timing = ex->begin(SPARKALOG_K_JOIN, s);
+            u64 join_launches = 0;
             // Joins: every rule appends into its target's candidate buffer.
             for (size_t ti = 0; ti < ex->targets.size(); ++ti) {
                 TargetRT& t = ex->targets[ti];
+                if (fused[ti]) continue;
                 u64* tc = counts + target_count_base(ex, ti);
                 for (size_t pos = 0; pos < t.rules.size(); ++pos) {
                     const size_t k = t.rules[pos];
@@ -1358,20 +1419,18 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                              kThreads, 0, s>>>(a);
                     SPK_CUDA(cudaGetLastError(), "join_fused_kernel");
                     ex->stats.total_launches += 1;
+                    join_launches += 1;
                 }
             }
-            ex->end(join_timing, s, 0.0, ex->rules.size());
+            ex->end(join_timing, s, 0.0, join_launches);
             std::vector<int> hist_t(ex->targets.size(), -1), pass_t(ex->targets.size(), -1),
-                anti_t(ex->targets.size(), -1);
+                anti_t(ex->targets.size(), -1), fused_t(ex->targets.size(), -1);
             // Distinct (radix sort) + unique/anti-join per target. The sort
             // reads the clamped candidate count from the device.
             for (size_t ti = 0; ti < ex->targets.size(); ++ti) {
                 TargetRT& t = ex->targets[ti];
                 u64* tc = counts + target_count_base(ex, ti);
                 u64* jn = tc + t.rules.size();
-                int rc = radix_sort(t.j_a.as<u64>(), t.j_b.as<u64>(), jn, t.j_cap, t.sort, ex, err, s, &hist_t[ti],
-                                    &pass_t[ti]);
-                if (rc) return rc;
                 RelState& tr = *st->find(t.id);
                 u64 dir_launches = 0;
                 {
@@ -1389,38 +1448,94 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                     lv.buckets[lv.n] = tr.dir_buckets[l];
                     ++lv.n;
                 }
+                const u64* cand = nullptr;  // sorted candidates for the anti-join
+                const u32* cand_sel = nullptr;
+                if (fused[ti]) {
+                    // Join + distinct in one kernel: the sorted distinct
+                    // candidates land in j_a, their count in jn, the join
+                    // output's size in the target's first count word.
+                    const size_t k = t.rules[0];
+                    const sparkalog_rule_plan& p = ex->rules[k];
+                    RelState& d = *st->find(p.delta_input);
+                    RelState& right = *st->find(p.right_input);
+                    IndexCache& ic = ex->index[k];
+                    spk::FusedRoundArgs a{};
+                    a.delta = d.delta.as<u64>();
+                    a.delta_rows = ex->host_rule_delta[k];
+                    a.rows_per_tile = t.fused_rows;
+                    a.left_key = p.left_key;
+                    if (ic.bucketed) {
+                        a.bucket_dir = ic.bucket_dir.as<u32>();
+                        a.bucket_shift = ic.bucket_shift;
+                        a.buckets = ic.buckets;
+                        a.keys32 = ic.keys32.as<u32>();
+                    } else {
+                        a.dense_offsets = ic.offsets.as<u32>();
+                        a.dense_keys = ic.num_keys;
+                    }
+                    a.rows = ic.identity ? nullptr : ic.rows.as<u32>();
+                    a.right = right.level[0].as<u64>();
+                    a.v1_side = p.proj_side[1];
+                    a.v1_col = p.proj_col[1];
+                    a.v1_bits = static_cast<u32>(32 - __builtin_clz(st->max_value | 1));
+                    a.out = t.j_a.as<u64>();
+                    a.out_count = jn;
+                    a.join_rows = reinterpret_cast<unsigned long long*>(tc);
+                    a.status = ex->status.as<u64>();
+                    a.tile_counter = counters + counter_slot++;
+                    a.epoch = ex->epoch++;
+                    a.err = err;
+                    a.fallback = err + kFusedFlagBase + ti;
+                    const size_t tiles = (a.delta_rows + a.rows_per_tile - 1) / a.rows_per_tile;
+                    fused_t[ti] = ex->begin(SPARKALOG_K_FUSED, s);
+                    int rc = launch_fused(a, tiles, s);
+                    if (rc) return rc;
+                    ex->end(fused_t[ti], s, 0.0, 1);
+                    ex->stats.total_launches += 1;
+                    cand = t.j_a.as<u64>();
+                } else {
+                    int rc = radix_sort(t.j_a.as<u64>(), t.j_b.as<u64>(), jn, t.j_cap, t.sort, ex, err, s,
+                                        &hist_t[ti], &pass_t[ti]);
+                    if (rc) return rc;
+                    cand = t.j_a.as<u64>();
+                    cand_sel = &t.sort.plan.as<spk::RadixPlan>()->final_sel;
+                }
                 auto kernel = spk::anti_join_levels_kernel<kThreads, kSetItems, kLevelStage>;
                 const size_t tiles = (t.j_cap + kSetTile - 1) / kSetTile;
-                const u32* sel = &t.sort.plan.as<spk::RadixPlan>()->final_sel;
                 anti_t[ti] = ex->begin(SPARKALOG_K_ANTI_JOIN, s);
                 kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, std::max<size_t>(tiles, 1)),
-                         kThreads, 0, s>>>(t.j_a.as<u64>(), t.j_b.as<u64>(), sel, jn, lv, tr.newt.as<u64>(),
+                         kThreads, 0, s>>>(cand, t.j_b.as<u64>(), cand_sel, jn, lv, tr.newt.as<u64>(),
                                            tc + t.rules.size() + 1, ex->status.as<u64>(), counters + counter_slot++,
                                            ex->epoch++, err);
                 SPK_CUDA(cudaGetLastError(), "anti_join_levels_kernel");
                 ex->end(anti_t[ti], s, 0.0, 1);
                 ex->stats.total_launches += 1 + dir_launches;
-                SPK_CUDA(cudaMemcpyAsync(ex->host_active + ti * spk::kMaxPasses, t.sort.plan.as<spk::RadixPlan>()->active,
-                                         spk::kMaxPasses * 4, cudaMemcpyDeviceToHost, s),
-                         "cudaMemcpyAsync");
+                if (!fused[ti])
+                    SPK_CUDA(cudaMemcpyAsync(ex->host_active + ti * spk::kMaxPasses,
+                                             t.sort.plan.as<spk::RadixPlan>()->active, spk::kMaxPasses * 4,
+                                             cudaMemcpyDeviceToHost, s),
+                             "cudaMemcpyAsync");
             }
             // The round's only host synchronisation: counts and error bits.
             SPK_CUDA(cudaMemcpyAsync(ex->host_counts, counts, ex->counts_words * 8, cudaMemcpyDeviceToHost, s),
                      "cudaMemcpyAsync");
-            SPK_CUDA(cudaMemcpyAsync(ex->host_counts + ex->counts_words, err, 4, cudaMemcpyDeviceToHost, s),
+            SPK_CUDA(cudaMemcpyAsync(ex->host_counts + ex->counts_words, err,
+                                     (kFusedFlagBase + kFusedMaxTargets) * 4, cudaMemcpyDeviceToHost, s),
                      "cudaMemcpyAsync");
             SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
             const u32 bits = static_cast<u32>(ex->host_counts[ex->counts_words] & 0xffffffffu);
+            const u32* flags = reinterpret_cast<const u32*>(ex->host_counts + ex->counts_words) + kFusedFlagBase;
             if (ex->profiling) {
                 // Algorithmic bytes (each input row read once, each output written once).
                 double join_bytes = 0.0;
-                for (size_t k = 0; k < ex->rules.size(); ++k) join_bytes += 16.0 * ex->host_rule_delta[k];
                 for (size_t ti = 0; ti < ex->targets.size(); ++ti) {
                     const TargetRT& t = ex->targets[ti];
+                    if (!fused[ti])
+                        for (size_t k : t.rules) join_bytes += 16.0 * ex->host_rule_delta[k];
                     const double jn = static_cast<double>(ex->host_counts[target_count_base(ex, ti) + t.rules.size()]);
                     const double nn =
                         static_cast<double>(ex->host_counts[target_count_base(ex, ti) + t.rules.size() + 1]);
-                    join_bytes += 12.0 * jn;
+                    if (!fused[ti]) join_bytes += 12.0 * jn;
                     u64 active = 0;
                     for (int p = 0; p < spk::kMaxPasses; ++p) active += ex->host_active[ti * spk::kMaxPasses + p] ? 1 : 0;
                     if (hist_t[ti] >= 0) ex->timings[hist_t[ti]].bytes = 8.0 * jn;
@@ -1429,9 +1544,30 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                         ex->timings[pass_t[ti]].launches = active;
                     }
                     if (anti_t[ti] >= 0) ex->timings[anti_t[ti]].bytes = 8.0 * jn + 8.0 * nn;
+                    if (fused_t[ti] >= 0) {
+                        // DELTA rows and their index entries, the joined right
+                        // rows, the distinct candidates out.
+                        const double delta_rows = static_cast<double>(ex->host_rule_delta[t.rules[0]]);
+                        const double joined = static_cast<double>(ex->host_counts[target_count_base(ex, ti)]);
+                        ex->timings[fused_t[ti]].bytes = 16.0 * delta_rows + 8.0 * joined + 8.0 * jn;
+                    }
                 }
                 if (join_timing >= 0) ex->timings[join_timing].bytes = join_bytes;
                 ex->collect();
+            }
+            bool redo_generic = false;
+            for (size_t ti = 0; ti < ex->targets.size(); ++ti) {
+                if (!fused[ti] || !flags[ti]) continue;
+                // A fused tile overflowed shared memory: redo this round with the
+                // general kernels and use smaller tiles from now on.
+                TargetRT& t = ex->targets[ti];
+                t.force_generic = true;
+                if (t.fused_rows > 64) t.fused_rows /= 2;
+                redo_generic = true;
+            }
+            if (redo_generic) {
+                SPK_CUDA(cudaMemsetAsync(err, 0, 4, s), "cudaMemsetAsync");
+                continue;
             }
             if (!(bits & spk::kErrCapacity)) break;
             // A candidate buffer overflowed: grow it and redo the round (no
@@ -1445,6 +1581,7 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
             SPK_CUDA(cudaMemsetAsync(err, 0, 4, s), "cudaMemsetAsync");
         }
 
+        for (auto& t : ex->targets) t.force_generic = false;
         const u32 err_bits = static_cast<u32>(ex->host_counts[ex->counts_words] & 0xffffffffu);
         if (err_bits & ~spk::kErrCapacity)
             return fail(SPARKALOG_E_DEVICE_FAULT, "device error bits " + std::to_string(err_bits));

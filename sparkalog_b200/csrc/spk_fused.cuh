@@ -1,0 +1,361 @@
+// Fused join -> distinct for rules whose join output starts with DELTA's
+// first column (the transitive-closure shape path(x, z) :- path(x, y),
+// edge(y, z)): the candidate rows of a round never reach HBM unsorted.
+//
+// DELTA is sorted by (first, second), and the join emits DELTA-row-major, so
+// the join output is already ordered by its first column x. A tile takes a
+// range of DELTA rows aligned to x boundaries, so its join output is a set of
+// complete x-runs: ordering the tile's output in shared memory orders it
+// globally (x-runs of different tiles never interleave). Within an x-run the
+// rows are placed by rank (a row's position is the number of smaller rows of
+// its run, ties broken by emission order) when every run is short, else the
+// tile is sorted by (run, second column) with a stable LSD radix sort in
+// shared memory over only the bits that vary. Adjacent duplicates are dropped
+// and the unique rows compacted with a decoupled look-back in tile order,
+// which is x order: the output is the sorted distinct candidate set that the
+// anti-join against FULL consumes.
+//
+// A tile whose x-run is longer than the tile's row capacity, or whose output
+// exceeds the shared-memory capacity, sets *fallback; the host then redoes
+// the round with the general kernels (join, radix sort, anti-join).
+#pragma once
+
+#include "spk_common.cuh"
+#include "spk_engine_kernels.cuh"
+#include "spk_join.cuh"
+#include "spk_setops.cuh"
+
+namespace spk {
+
+struct FusedRoundArgs {
+    const u64* delta;
+    u64 delta_rows;
+    u32 rows_per_tile;        // nominal DELTA rows per tile (x boundaries move it)
+    u32 left_key;             // DELTA column joined on the right relation's key
+    // Index of the right relation on the join key (DELTA's second column).
+    const u32* dense_offsets;
+    u64 dense_keys;
+    const u32* bucket_dir;
+    u32 bucket_shift;
+    u64 buckets;
+    const u32* keys32;
+    const u32* rows;          // null: identity
+    const u64* right;
+    u32 v1_side;              // 0: DELTA column, 1: right column
+    u32 v1_col;
+    u32 v1_bits;              // significant bits of the second output column
+    u64* out;                 // sorted distinct join output
+    u64* out_count;
+    unsigned long long* join_rows;  // total join output rows (statistics)
+    u64* status;
+    u32* tile_counter;
+    u32 epoch;
+    u32* err;
+    u32* fallback;
+};
+
+__device__ __forceinline__ void index_lookup(const FusedRoundArgs& a, u32 key, u32* begin, u32* count) {
+    *begin = 0;
+    *count = 0;
+    if (a.dense_offsets) {
+        if (key < a.dense_keys) {
+            *begin = a.dense_offsets[key];
+            *count = a.dense_offsets[key + 1] - *begin;
+        }
+        return;
+    }
+    const u64 b = static_cast<u64>(key) >> a.bucket_shift;
+    if (b >= a.buckets) return;
+    u64 lo = a.bucket_dir[b], hi = a.bucket_dir[b + 1];
+    while (lo < hi) {
+        const u64 mid = (lo + hi) >> 1;
+        if (a.keys32[mid] < key) lo = mid + 1;
+        else hi = mid;
+    }
+    u64 up = lo, top = a.bucket_dir[b + 1];
+    while (up < top) {
+        const u64 mid = (up + top) >> 1;
+        if (a.keys32[mid] <= key) up = mid + 1;
+        else top = mid;
+    }
+    *begin = static_cast<u32>(lo);
+    *count = static_cast<u32>(up - lo);
+}
+
+// Shared-memory layout of one CTA (dynamic shared memory).
+template <int THREADS, int CAP, int ROWCAP>
+struct FusedLayout {
+    static constexpr int kWarps = THREADS / kWarp;
+    static constexpr size_t kKeysA = 0;
+    static constexpr size_t kKeysB = kKeysA + CAP * sizeof(u64);
+    static constexpr size_t kRowOffset = kKeysB + CAP * sizeof(u64);          // u32[ROWCAP + 1]
+    static constexpr size_t kRowBegin = kRowOffset + (ROWCAP + 4) * sizeof(u32);  // u32[ROWCAP]
+    static constexpr size_t kRunX = kRowBegin + ROWCAP * sizeof(u32);          // u32[ROWCAP]
+    static constexpr size_t kRunOff = kRunX + ROWCAP * sizeof(u32);            // u32[ROWCAP + 1]
+    static constexpr size_t kRowRank = kRunOff + (ROWCAP + 4) * sizeof(u32);   // u16[ROWCAP]
+    static constexpr size_t kRank = kRowRank + ROWCAP * sizeof(unsigned short); // u16[CAP]
+    static constexpr size_t kWarpCount = kRank + CAP * sizeof(unsigned short);  // u16[kWarps][256]
+    static constexpr size_t kDigitStart = kWarpCount + kWarps * 256 * sizeof(unsigned short);
+    static constexpr size_t kBytes = kDigitStart + 256 * sizeof(u32);
+};
+
+// Stable LSD radix sort of n <= CAP keys in shared memory over the 8-bit
+// digits at `shifts`. Keys start in *src; on return *src points at the
+// sorted keys (the buffers alternate). Must be called by all threads.
+template <int THREADS, int CAP>
+__device__ void smem_radix_sort(u64** src, u64** dst, u32 n, const int* shifts, int passes, unsigned short* rank,
+                                unsigned short* warp_count, u32* digit_start, u32* scan_scratch) {
+    constexpr int kWarps = THREADS / kWarp;
+    const u32 lane = lane_id(), warp = warp_id();
+    const u32 chunk = ((n + kWarps - 1) / kWarps + kWarp - 1) / kWarp * kWarp;  // per-warp run, multiple of 32
+    for (int p = 0; p < passes; ++p) {
+        const int sh = shifts[p];
+        u64* a = *src;
+        u64* b = *dst;
+        for (int i = threadIdx.x; i < kWarps * 256; i += THREADS) warp_count[i] = 0;
+        __syncthreads();
+        const u32 w0 = warp * chunk;
+        for (u32 j = 0; j < chunk; j += kWarp) {
+            const u32 pos = w0 + j + lane;
+            const bool valid = pos < n;
+            const u32 d = valid ? static_cast<u32>((a[pos] >> sh) & 255) : 256u;
+            const u32 peers = __match_any_sync(0xffffffffu, d);
+            const u32 before = __popc(peers & lanemask_lt());
+            u32 base = 0;
+            if (valid) base = warp_count[warp * 256 + d];
+            __syncwarp();
+            if (valid && before == 0) warp_count[warp * 256 + d] = static_cast<unsigned short>(base + __popc(peers));
+            __syncwarp();
+            if (valid) rank[pos] = static_cast<unsigned short>(base + before);
+        }
+        __syncthreads();
+        // Digit t: exclusive prefix over warps, then over digits.
+        u32 running = 0;
+        if (threadIdx.x < 256) {
+            for (int w = 0; w < kWarps; ++w) {
+                const u32 c = warp_count[w * 256 + threadIdx.x];
+                warp_count[w * 256 + threadIdx.x] = static_cast<unsigned short>(running);
+                running += c;
+            }
+        }
+        u32 total;
+        const u32 start = block_exclusive_scan<THREADS>(threadIdx.x < 256 ? running : 0u, scan_scratch, &total);
+        if (threadIdx.x < 256) digit_start[threadIdx.x] = start;
+        __syncthreads();
+        for (u32 pos = threadIdx.x; pos < n; pos += THREADS) {
+            const u64 k = a[pos];
+            const u32 d = static_cast<u32>((k >> sh) & 255);
+            b[digit_start[d] + warp_count[(pos / chunk) * 256 + d] + rank[pos]] = k;
+        }
+        __syncthreads();
+        *src = b;
+        *dst = a;
+    }
+}
+
+// Shared-memory radix passes for a tile: the digits of the second column's
+// significant bits, then those of the x-run rank.
+__device__ __forceinline__ int fused_sort_shifts(u32 v1_bits, u32 runs, int* shifts) {
+    int passes = 0;
+    for (int b = 0; b < static_cast<int>(v1_bits); b += 8) shifts[passes++] = b;
+    const int rbits = runs > 1 ? 32 - __clz(runs - 1) : 0;  // one x-run: nothing to sort on
+    for (int b = 0; b < rbits; b += 8) shifts[passes++] = 32 + b;
+    return passes;
+}
+
+// Runs with at most this many output rows are placed by rank.
+constexpr u32 kRankRun = 48;
+
+template <int THREADS, int CAP, int ROWCAP>
+__global__ void __launch_bounds__(THREADS, 2) fused_join_distinct_kernel(FusedRoundArgs a) {
+    using L = FusedLayout<THREADS, CAP, ROWCAP>;
+    constexpr int kRowItems = ROWCAP / THREADS;
+    constexpr int kItems = CAP / THREADS;
+    static_assert(kItems <= 32, "keep mask is 32 bits");
+    static_assert(ROWCAP < 65536 && CAP < 65536, "16-bit ranks and counts");
+    extern __shared__ __align__(16) unsigned char smem[];
+    u64* keys_a = reinterpret_cast<u64*>(smem + L::kKeysA);
+    u64* keys_b = reinterpret_cast<u64*>(smem + L::kKeysB);
+    u32* row_offset = reinterpret_cast<u32*>(smem + L::kRowOffset);
+    u32* row_begin = reinterpret_cast<u32*>(smem + L::kRowBegin);
+    u32* run_x = reinterpret_cast<u32*>(smem + L::kRunX);
+    u32* run_off = reinterpret_cast<u32*>(smem + L::kRunOff);
+    unsigned short* row_rank = reinterpret_cast<unsigned short*>(smem + L::kRowRank);
+    unsigned short* rank = reinterpret_cast<unsigned short*>(smem + L::kRank);
+    unsigned short* warp_count = reinterpret_cast<unsigned short*>(smem + L::kWarpCount);
+    u32* digit_start = reinterpret_cast<u32*>(smem + L::kDigitStart);
+    __shared__ u32 scan_scratch[THREADS / kWarp + 1];
+    __shared__ CompactShared<THREADS> cs;
+    __shared__ u64 bounds[2];
+    __shared__ u32 bail;
+
+    const u64 n = a.delta_rows;
+    const u64 R = a.rows_per_tile;
+    const u64 num_tiles = (n + R - 1) / R;
+    if (num_tiles == 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) *a.out_count = 0;
+        return;
+    }
+    for (;;) {
+        if (threadIdx.x == 0) {
+            cs.tile = atomicAdd(a.tile_counter, 1u);
+            bail = 0;
+        }
+        __syncthreads();
+        const u64 tile = cs.tile;
+        if (tile >= num_tiles) break;
+
+        // 1. Rows [B(tile), B(tile + 1)): the first x boundary at or after each
+        // nominal start (warp 0: begin, warp 1: end), scanning <= ROWCAP rows.
+        if (warp_id() < 2) {
+            const u64 p0 = (tile + warp_id()) * R;
+            u64 found = ~0ull;
+            if (p0 == 0) {
+                found = 0;
+            } else if (p0 >= n) {
+                found = n;
+            } else {
+                for (u64 base = p0; base < p0 + ROWCAP && found == ~0ull; base += kWarp) {
+                    const u64 p = base + lane_id();
+                    const bool boundary = p >= n || (a.delta[p] >> 32) != (a.delta[p - 1] >> 32);
+                    const u32 m = __ballot_sync(0xffffffffu, boundary);
+                    if (m) found = base + (__ffs(m) - 1);
+                }
+                if (found != ~0ull && found > n) found = n;
+            }
+            if (lane_id() == 0) bounds[warp_id()] = found;
+        }
+        __syncthreads();
+        const u64 row0 = bounds[0], row1 = bounds[1];
+        const bool rows_ok = row0 != ~0ull && row1 != ~0ull && row1 - row0 <= static_cast<u64>(ROWCAP);
+        const u32 nrows = rows_ok ? static_cast<u32>(row1 - row0) : 0u;
+
+        // 2. Match counts per row and their scan; x-runs: value, rank, offset.
+        const u32 local0 = threadIdx.x * kRowItems;
+        u32 cnt[kRowItems];
+        u32 starts = 0, sum = 0;
+#pragma unroll
+        for (int i = 0; i < kRowItems; ++i) {
+            const u32 r = local0 + i;
+            cnt[i] = 0;
+            if (r < nrows) {
+                const u64 row = a.delta[row0 + r];
+                u32 begin, c;
+                index_lookup(a, pair_col(row, a.left_key), &begin, &c);
+                row_begin[r] = begin;
+                cnt[i] = c;
+                starts += (r == 0 || (row >> 32) != (a.delta[row0 + r - 1] >> 32)) ? 1u : 0u;
+            }
+            sum += cnt[i];
+        }
+        u32 total, runs;
+        u32 off = block_exclusive_scan<THREADS>(sum, scan_scratch, &total);
+        __syncthreads();
+        u32 rk = block_exclusive_scan<THREADS>(starts, scan_scratch, &runs);
+#pragma unroll
+        for (int i = 0; i < kRowItems; ++i) {
+            const u32 r = local0 + i;
+            if (r < nrows) {
+                const u64 row = a.delta[row0 + r];
+                if (r == 0 || (row >> 32) != (a.delta[row0 + r - 1] >> 32)) {
+                    run_x[rk] = static_cast<u32>(row >> 32);
+                    run_off[rk] = off;
+                    ++rk;
+                }
+                row_rank[r] = static_cast<unsigned short>(rk - 1);
+            }
+            row_offset[r] = off;
+            off += cnt[i];
+        }
+        if (threadIdx.x == 0) {
+            row_offset[ROWCAP] = total;
+            run_off[runs] = total;
+            if (!rows_ok || total > static_cast<u32>(CAP)) bail = 1;
+            else if (total) atomicAdd(a.join_rows, static_cast<unsigned long long>(total));
+        }
+        __syncthreads();
+        const bool ok = bail == 0;
+        if (!ok) total = 0;
+        int long_run = 0;
+        for (u32 r = threadIdx.x; r < (ok ? runs : 0u); r += THREADS)
+            long_run |= run_off[r + 1] - run_off[r] > kRankRun ? 1 : 0;
+
+        // 3. Emit (x-run rank << 32 | second column) keys into shared memory.
+        for (u32 o = threadIdx.x; o < total; o += THREADS) {
+            u32 lo = 0, hi = ROWCAP;
+            while (hi - lo > 1) {
+                const u32 mid = (lo + hi) >> 1;
+                if (row_offset[mid] <= o) lo = mid;
+                else hi = mid;
+            }
+            const u32 m = row_begin[lo] + (o - row_offset[lo]);
+            const u32 right_row = a.rows ? a.rows[m] : m;
+            const u32 v1 = a.v1_side == 1 ? pair_col(a.right[right_row], a.v1_col)
+                                          : pair_col(a.delta[row0 + lo], a.v1_col);
+            keys_a[o] = (static_cast<u64>(row_rank[lo]) << 32) | v1;
+        }
+        long_run = __syncthreads_or(long_run);
+
+        // 4. Order the tile by (x, second column) into `sorted`.
+        u64* sorted;
+        u64* spare;
+        if (!long_run) {
+            // Rank placement within each (short) x-run.
+            for (u32 o = threadIdx.x; o < total; o += THREADS) {
+                const u64 k = keys_a[o];
+                const u32 r = static_cast<u32>(k >> 32), v = static_cast<u32>(k);
+                const u32 s0 = run_off[r], s1 = run_off[r + 1];
+                u32 before = 0;
+                for (u32 j = s0; j < s1; ++j) {
+                    const u32 w = static_cast<u32>(keys_a[j]);
+                    before += (w < v || (w == v && j < o)) ? 1u : 0u;
+                }
+                keys_b[s0 + before] = (static_cast<u64>(run_x[r]) << 32) | v;
+            }
+            sorted = keys_b;
+            spare = keys_a;
+        } else {
+            int shifts[8];
+            const int passes = fused_sort_shifts(a.v1_bits, runs, shifts);
+            u64* src = keys_a;
+            u64* dst = keys_b;
+            smem_radix_sort<THREADS, CAP>(&src, &dst, total, shifts, passes, rank, warp_count, digit_start,
+                                          scan_scratch);
+            for (u32 o = threadIdx.x; o < total; o += THREADS) {
+                const u64 k = src[o];
+                src[o] = (static_cast<u64>(run_x[k >> 32]) << 32) | static_cast<u32>(k);
+            }
+            sorted = src;
+            spare = dst;
+        }
+        __syncthreads();
+
+        // 5. Unique (each thread owns kItems consecutive sorted rows; runs of
+        // different tiles never share a row) and compaction in tile order.
+        u32 keep = 0;
+        u64 v[kItems];
+        const u32 base = threadIdx.x * kItems;
+#pragma unroll
+        for (int i = 0; i < kItems; ++i) {
+            const u32 o = base + i;
+            v[i] = 0;
+            if (o < total) {
+                v[i] = sorted[o];
+                if (o == 0 || v[i] != sorted[o - 1]) keep |= 1u << i;
+            }
+        }
+        u32 excl, kept;
+        const u64 out_off = compact_offsets<THREADS>(__popc(keep), &excl, &kept, tile, a.status, a.epoch, a.err, cs);
+        if (!ok && threadIdx.x == 0) atomicOr(a.fallback, 1u);
+        u32 w = excl;
+#pragma unroll
+        for (int i = 0; i < kItems; ++i)
+            if (keep & (1u << i)) spare[w++] = v[i];
+        __syncthreads();
+        for (u32 j = threadIdx.x; j < kept; j += THREADS) a.out[out_off + j] = spare[j];
+        if (tile == num_tiles - 1 && threadIdx.x == 0) *a.out_count = out_off + kept;
+        __syncthreads();
+    }
+}
+
+}  // namespace spk

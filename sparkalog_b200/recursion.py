@@ -276,6 +276,10 @@ class RecursiveExecutor:
         """Times every kernel class with CUDA events on the store's stream."""
         _check(_native.load().sparkalog_executor_set_profiling(self._h, 1 if enable else 0))
 
+    def set_fused(self, enable: bool) -> None:
+        """Enables (default) or disables the fused join + distinct kernel; results are identical."""
+        _check(_native.load().sparkalog_executor_set_fused(self._h, 1 if enable else 0))
+
     def stats(self, reset: bool = False) -> dict:
         """Per-kernel-class launches, milliseconds and algorithmic bytes, plus total launches."""
         s = _native.KernelStatsC()

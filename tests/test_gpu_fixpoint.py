@@ -203,3 +203,94 @@ def test_device_inputs_and_reads(cuda):
     (w0, w1), _, _ = oracle.transitive_closure(src, dst, threads=8)
     assert np.array_equal(o0.cpu().numpy().view(np.uint32), w0)
     assert np.array_equal(o1.cpu().numpy().view(np.uint32), w1)
+
+
+def _tc_with_stats(e0, e1, rule=None, oracle_rule=None):
+    R = rec()
+    from sparkalog_b200.relational import RecursiveSccPlan
+
+    store = R.RelationStore()
+    store.insert_static(0, (e0, e1))
+    store.insert_recursive(1, (e0, e1), (e0, e1))
+    plan = R.transitive_closure_scc(_rid(1), _rid(0)) if rule is None else RecursiveSccPlan([_rid(1)], [rule])
+    ex = R.RecursiveExecutor.compile(plan, store)
+    ex.set_profiling(True)
+    summary = ex.run(store, 10_000)
+    stats = ex.stats()
+    st = oracle.Store()
+    st.insert_static(0, (e0, e1))
+    st.insert_recursive(1, (e0, e1), (e0, e1))
+    it, new = st.run_scc([1], [oracle_rule or oracle.tc_rule(1, 0)])
+    assert summary.iterations == it and summary.total_new_rows == new
+    assert pairs(store.full(1)) == pairs(st.full(1))
+    return stats
+
+
+def test_fused_join_distinct_only_on_sparse_chain(cuda):
+    # Every round of a chain fits the fused kernel's tiles: no general join.
+    src = np.arange(700, dtype=np.uint32)
+    stats = _tc_with_stats(src, src + 1)
+    assert stats["classes"]["join_distinct"]["launches"] == stats["rounds"]
+    assert stats["classes"]["join"]["launches"] == 0
+
+
+def test_fused_join_distinct_falls_back_on_hub(cuda):
+    # Node 0 reaches 6000 nodes in one step and a chain hangs off them, so its
+    # x-run outgrows a fused tile: those rounds redo on the general kernels and
+    # the result stays exact.
+    hub = np.zeros(6000, dtype=np.uint32), np.arange(1, 6001, dtype=np.uint32)
+    chain = np.arange(1, 400, dtype=np.uint32)
+    er0, er1 = generators.er_edges(8000, 6000, 13)
+    e0, e1 = oracle.btree_pairs(np.concatenate([hub[0], chain, er0]), np.concatenate([hub[1], chain + 1, er1]))
+    stats = _tc_with_stats(e0, e1)
+    assert stats["classes"]["join_distinct"]["launches"] > 0
+    assert stats["classes"]["join"]["launches"] > 0
+
+
+def test_fused_join_distinct_join_on_first_column(cuda):
+    # p(x, y) :- p(x, z), e(x, y): the join key is DELTA's first column.
+    from sparkalog_b200.relational import BinaryEqualityJoin, JoinInput, JoinProjection, RecursiveRulePlan
+
+    src, dst = generators.er_edges(4000, 6000, 17)
+    e0, e1 = oracle.btree_pairs(src, dst)
+    join = BinaryEqualityJoin(0, 0, (JoinProjection(JoinInput.LEFT, 0), JoinProjection(JoinInput.RIGHT, 1)))
+    rule = RecursiveRulePlan(_rid(1), _rid(1), _rid(0), join)
+    stats = _tc_with_stats(e0, e1, rule,
+                           oracle.rule_plan(1, 1, 0, left_key=0, right_key=0, projection=((0, 0), (1, 1))))
+    assert stats["classes"]["join_distinct"]["launches"] > 0
+
+
+def test_fused_join_distinct_projects_delta_columns(cuda):
+    # p(x, y) :- p(x, y), e(y, z): the output is DELTA itself, nothing new.
+    from sparkalog_b200.relational import BinaryEqualityJoin, JoinInput, JoinProjection, RecursiveRulePlan
+
+    src, dst = generators.er_edges(3000, 4000, 19)
+    e0, e1 = oracle.btree_pairs(src, dst)
+    join = BinaryEqualityJoin(1, 0, (JoinProjection(JoinInput.LEFT, 0), JoinProjection(JoinInput.LEFT, 1)))
+    rule = RecursiveRulePlan(_rid(1), _rid(1), _rid(0), join)
+    _tc_with_stats(e0, e1, rule, oracle.rule_plan(1, 1, 0, left_key=1, right_key=0, projection=((0, 0), (0, 1))))
+
+
+@pytest.mark.parametrize("n,e,seed", [(2000, 8000, 1), (50_000, 60_000, 4), (300_000, 262_500, 6)])
+def test_fused_and_general_rounds_agree(cuda, n, e, seed):
+    # The fused join + distinct kernel and the general join / radix sort give
+    # the same FULL, iteration count and new-row count (dense graphs also
+    # exercise tile overflow and the smaller tiles that follow it).
+    R = rec()
+    src, dst = generators.er_edges(n, e, seed)
+    e0, e1 = oracle.btree_pairs(src, dst)
+    out = []
+    for fused in (True, False):
+        store = R.RelationStore()
+        store.insert_static(0, (e0, e1))
+        store.insert_recursive(1, (e0, e1), (e0, e1))
+        ex = R.RecursiveExecutor.compile(R.transitive_closure_scc(_rid(1), _rid(0)), store)
+        ex.set_fused(fused)
+        ex.set_profiling(True)
+        summary = ex.run(store, 10_000)
+        stats = ex.stats()
+        assert (stats["classes"]["join_distinct"]["launches"] > 0) == fused
+        f0, f1 = store.full(1)
+        out.append((summary.iterations, summary.total_new_rows, f0, f1))
+    assert out[0][:2] == out[1][:2]
+    assert np.array_equal(out[0][2], out[1][2]) and np.array_equal(out[0][3], out[1][3])
