@@ -66,7 +66,11 @@ constexpr int kSetItems = 8;
 constexpr int kSetTile = kThreads * kSetItems;
 constexpr int kJoinItems = 8;
 constexpr int kJoinTile = kThreads * kJoinItems;
-constexpr int kLevelStage = 4096;  // level rows staged in shared memory per anti-join tile
+constexpr int kLevelStage = 2048;  // level rows per shared-memory chunk of the anti-join (two buffers)
+constexpr int kSparseThreads = 128;  // anti-join of small candidate sets
+constexpr int kSparseItems = 4;
+constexpr int kSparseTile = kSparseThreads * kSparseItems;
+constexpr u64 kSparseCandidates = 1ull << 22;
 constexpr int kMergeItems = 8;
 constexpr int kMergeTile = kThreads * kMergeItems;
 constexpr int kSortThreads = spk::RadixSortConfig::kThreads;
@@ -309,7 +313,7 @@ struct TargetRT {
     DevArray j_a, j_b;     // candidate buffers (sort ping-pong)
     u64 j_cap = 0;         // elements
     SortScratch sort;
-    u32 fused_rows = 1024; // nominal DELTA rows per fused tile (halved when tiles overflow)
+    u32 fused_rows = 896;  // nominal DELTA rows per fused tile (halved when tiles overflow)
     bool force_generic = false;  // redo the current round with the general kernels
 };
 
@@ -439,9 +443,9 @@ size_t target_count_base(const sparkalog_executor* ex, size_t t) {
     return base;
 }
 
-constexpr int kFusedThreads = 256;
-constexpr int kFusedCap = 3840;     // join output rows per fused tile (shared memory)
-constexpr int kFusedRowCap = 2048;  // DELTA rows per fused tile
+constexpr int kFusedThreads = 128;
+constexpr int kFusedCap = 1920;     // join output rows per fused tile (shared memory)
+constexpr int kFusedRowCap = 1024;  // DELTA rows per fused tile
 constexpr size_t kFusedFlagBase = 8;      // fallback flags live at err + 8 + target
 constexpr size_t kFusedMaxTargets = 48;
 
@@ -1355,8 +1359,10 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
         for (;;) {
             for (auto& t : ex->targets) {
                 SPK_CUDA(st->find(t.id)->newt.ensure(t.j_cap * 8, s), "cudaMallocAsync");
-                max_status_words = std::max<size_t>(max_status_words, (t.j_cap + kSetTile - 1) / kSetTile + 1);
-                // Fused tiles are DELTA-row tiles: one status word each.
+                // One status word per anti-join tile (the sparse kernel's
+                // tiles are the smallest)...
+                max_status_words = std::max<size_t>(max_status_words, (t.j_cap + kSparseTile - 1) / kSparseTile + 1);
+                // ...and per fused tile, which are DELTA-row tiles.
                 u64 delta_rows = 0;
                 for (size_t k : t.rules) delta_rows += ex->host_rule_delta[k];
                 max_status_words = std::max<size_t>(max_status_words, (delta_rows + t.fused_rows - 1) / t.fused_rows + 1);
@@ -1500,14 +1506,29 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                     cand = t.j_a.as<u64>();
                     cand_sel = &t.sort.plan.as<spk::RadixPlan>()->final_sel;
                 }
-                auto kernel = spk::anti_join_levels_kernel<kThreads, kSetItems, kLevelStage>;
-                const size_t tiles = (t.j_cap + kSetTile - 1) / kSetTile;
                 anti_t[ti] = ex->begin(SPARKALOG_K_ANTI_JOIN, s);
-                kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, std::max<size_t>(tiles, 1)),
-                         kThreads, 0, s>>>(cand, t.j_b.as<u64>(), cand_sel, jn, lv, tr.newt.as<u64>(),
-                                           tc + t.rules.size() + 1, ex->status.as<u64>(), counters + counter_slot++,
-                                           ex->epoch++, err);
-                SPK_CUDA(cudaGetLastError(), "anti_join_levels_kernel");
+                u64 cand_bound = 0;  // the join output bound: candidates never exceed it
+                for (size_t k : t.rules)
+                    cand_bound += ex->host_rule_delta[k] * static_cast<u64>(std::max<u32>(ex->index[k].max_degree, 1));
+                if (cand_bound <= kSparseCandidates) {
+                    // Few candidates, far apart in every level: look each up
+                    // in all levels at once.
+                    auto kernel = spk::anti_join_levels_sparse_kernel<kSparseThreads, kSparseItems>;
+                    const size_t tiles = (cand_bound + kSparseTile - 1) / kSparseTile;
+                    kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kSparseThreads, std::max<size_t>(tiles, 1)),
+                             kSparseThreads, 0, s>>>(cand, t.j_b.as<u64>(), cand_sel, jn, lv, tr.newt.as<u64>(),
+                                                     tc + t.rules.size() + 1, ex->status.as<u64>(),
+                                                     counters + counter_slot++, ex->epoch++, err);
+                    SPK_CUDA(cudaGetLastError(), "anti_join_levels_sparse_kernel");
+                } else {
+                    auto kernel = spk::anti_join_levels_kernel<kThreads, kSetItems, kLevelStage>;
+                    const size_t tiles = (t.j_cap + kSetTile - 1) / kSetTile;
+                    kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, std::max<size_t>(tiles, 1)),
+                             kThreads, 0, s>>>(cand, t.j_b.as<u64>(), cand_sel, jn, lv, tr.newt.as<u64>(),
+                                               tc + t.rules.size() + 1, ex->status.as<u64>(), counters + counter_slot++,
+                                               ex->epoch++, err);
+                    SPK_CUDA(cudaGetLastError(), "anti_join_levels_kernel");
+                }
                 ex->end(anti_t[ti], s, 0.0, 1);
                 ex->stats.total_launches += 1 + dir_launches;
                 if (!fused[ti])

@@ -29,6 +29,18 @@ __device__ __forceinline__ u32 lanemask_lt() {
 }
 
 __device__ __forceinline__ u32 lane_id() { return threadIdx.x & (kWarp - 1); }
+
+// Asynchronous 8-byte global -> shared copies (cp.async, L1-allocating), so a
+// thread keeps many loads in flight without holding them in registers.
+__device__ __forceinline__ void cp_async_8(void* smem, const void* gmem) {
+    const u32 s = static_cast<u32>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
 __device__ __forceinline__ u32 warp_id() { return threadIdx.x / kWarp; }
 
 __device__ __forceinline__ u64 ld_volatile(const u64* p) {

@@ -57,16 +57,38 @@ static __global__ void level_directory_kernel(const u64* keys, u64 n, u32 shift,
 }
 
 // NEWT = unique(sorted candidates) - FULL, where FULL is the union of the
-// levels. Candidates come from the radix sort's final buffer. This fuses the
-// reference's BinaryDistinct unique step with SortedBinaryAntiJoin.
+// levels. This fuses the reference's BinaryDistinct unique step with
+// SortedBinaryAntiJoin (crates/sparkalog-operators/src/lib.rs, the sorted
+// anti-join over packed rows).
 //
-// Per tile of candidates and per level, one warp finds the level's slice
-// that covers the tile's key span (warp_lower_bound, ~log32 dependent loads).
-// A slice that fits in shared memory is staged there with coalesced loads and
-// every thread merges its sorted candidates against it; a larger slice (a
-// sparse tile against a big level) is searched per candidate with galloping
-// searches in global memory. Kept rows are compacted with a decoupled
-// look-back, so NEWT stays sorted.
+// Per tile of candidates and per level, the slice of the level that can hold
+// the tile's keys is read off the level's directory (the bucket of the first
+// key to the bucket of the last: two loads, no search). A slice of up to
+// STAGE * kStreamChunks rows is streamed through shared memory in chunks of
+// STAGE rows (asynchronous copies, double-buffered: the next chunk is in
+// flight while the current one is searched), and each thread searches its
+// sorted candidates in the chunk that spans them; a larger slice (a sparse
+// tile against a big level) is searched per candidate from its directory
+// bucket, all ITEMS candidates in lock step. Kept rows are compacted with a
+// decoupled look-back, so NEWT stays sorted.
+constexpr u64 kStreamChunks = 2;
+
+// Directory bounds of a tile's keys [first, last] in every level: the rows of
+// first's bucket through last's bucket (threads 0 .. 2 * levels.n - 1).
+__device__ __forceinline__ void level_slices(const Levels& levels, u64 first, u64 last, u64* range_lo, u64* range_hi) {
+    const int l = static_cast<int>(threadIdx.x >> 1);
+    if (l < levels.n) {
+        u64 lo, hi;
+        if ((threadIdx.x & 1) == 0) {
+            dir_range(levels, l, first, &lo, &hi);
+            range_lo[l] = lo;
+        } else {
+            dir_range(levels, l, last, &lo, &hi);
+            range_hi[l] = hi;
+        }
+    }
+}
+
 template <int THREADS, int ITEMS, int STAGE>
 __global__ void __launch_bounds__(THREADS) anti_join_levels_kernel(const u64* buf_a, const u64* buf_b,
                                                                    const u32* final_sel, const u64* n_ptr,
@@ -76,7 +98,7 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_kernel(const u64* bu
     constexpr int kTile = THREADS * ITEMS;
     static_assert(STAGE >= kTile, "the output stage reuses the level stage");
     __shared__ CompactShared<THREADS> cs;
-    __shared__ u64 stage[STAGE];
+    __shared__ __align__(16) u64 stage[2 * STAGE];
     __shared__ u64 range_lo[kMaxLevels], range_hi[kMaxLevels];
     const u64* keys = (final_sel && *final_sel) ? buf_b : buf_a;
     const u64 n = *n_ptr;
@@ -91,16 +113,8 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_kernel(const u64* bu
         const u64 tile = cs.tile;
         if (tile >= num_tiles) break;
         const u64 tile_begin = tile * kTile;
-        if (threadIdx.x < static_cast<u32>(levels.n)) {
-            // The tile's slice of level l: from the lower bound of its first
-            // key to just past the lower bound of its last key.
-            const int l = static_cast<int>(threadIdx.x);
-            const u64 c = levels.count[l];
-            const u64 last = keys[(tile_begin + kTile < n ? tile_begin + kTile : n) - 1];
-            range_lo[l] = dir_lower_bound(levels, l, keys[tile_begin]);
-            const u64 hi = dir_lower_bound(levels, l, last) + 1;
-            range_hi[l] = hi < c ? hi : c;
-        }
+        const u64 tile_end = tile_begin + kTile < n ? tile_begin + kTile : n;
+        if (threadIdx.x < 2u * levels.n) level_slices(levels, keys[tile_begin], keys[tile_end - 1], range_lo, range_hi);
         const u64 base = tile_begin + static_cast<u64>(threadIdx.x) * ITEMS;
         u64 v[ITEMS];
         u32 keep = 0;
@@ -119,25 +133,44 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_kernel(const u64* bu
         __syncthreads();
         for (int l = 0; l < levels.n; ++l) {
             const u64 lo = range_lo[l];
-            const u64 len = range_hi[l] - lo;
+            const u64 hi = range_hi[l];
             const PackedKeys lv{levels.keys[l]};
-            if (len <= static_cast<u64>(STAGE)) {
-                for (u32 t = threadIdx.x; t < len; t += THREADS) stage[t] = lv(lo + t);
-                __syncthreads();
-                if (keep) {
-                    const SmemKeys sk{stage};
-                    u64 cur = 0;
-                    bool have = false;
+            if (hi - lo <= static_cast<u64>(STAGE) * kStreamChunks) {
+                const u32 chunks = static_cast<u32>((hi - lo + STAGE - 1) / STAGE);
+                const u64* level_keys = levels.keys[l];
+                auto issue = [&](u32 c) {
+                    const u64 c0 = lo + static_cast<u64>(c) * STAGE;
+                    const u32 clen = static_cast<u32>(hi - c0 < static_cast<u64>(STAGE) ? hi - c0 : STAGE);
+                    u64* buf = stage + (c & 1) * STAGE;
+                    for (u32 t = threadIdx.x; t < clen; t += THREADS) cp_async_8(buf + t, level_keys + c0 + t);
+                    cp_async_commit();
+                };
+                if (chunks) issue(0);
+                for (u32 c = 0; c < chunks; ++c) {
+                    if (c + 1 < chunks) {
+                        issue(c + 1);
+                        cp_async_wait<1>();
+                    } else {
+                        cp_async_wait<0>();
+                    }
+                    __syncthreads();
+                    const u64 c0 = lo + static_cast<u64>(c) * STAGE;
+                    const u32 clen = static_cast<u32>(hi - c0 < static_cast<u64>(STAGE) ? hi - c0 : STAGE);
+                    const u64* buf = stage + (c & 1) * STAGE;
+                    const u64 first = buf[0], last = buf[clen - 1];
+                    if (keep && v[0] <= last) {
+                        const SmemKeys sk{buf};
+                        u64 cur = 0;
 #pragma unroll
-                    for (int i = 0; i < ITEMS; ++i) {
-                        if (keep & (1u << i)) {
-                            cur = have ? gallop_lower_bound(sk, cur, len, v[i]) : lower_bound_keys(sk, 0, len, v[i]);
-                            have = true;
-                            if (cur < len && stage[cur] == v[i]) keep &= ~(1u << i);
+                        for (int i = 0; i < ITEMS; ++i) {
+                            if ((keep & (1u << i)) && v[i] >= first && v[i] <= last) {
+                                cur = gallop_lower_bound(sk, cur, clen, v[i]);
+                                if (cur < clen && buf[cur] == v[i]) keep &= ~(1u << i);
+                            }
                         }
                     }
+                    __syncthreads();
                 }
-                __syncthreads();
             } else if (keep) {
                 // Sparse tile against a large slice: each candidate's search
                 // starts from its directory bucket (two loads of a small
@@ -173,6 +206,103 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_kernel(const u64* bu
                         const u64 p = pos[i] + (lv(pos[i]) < v[i] ? 1 : 0);
                         if (p < end[i] && lv(p) == v[i]) keep &= ~(1u << i);
                     }
+                }
+            }
+        }
+        u32 excl, total;
+        const u64 off = compact_offsets<THREADS>(__popc(keep), &excl, &total, tile, status, epoch, err, cs);
+        u32 wpos = excl;
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i)
+            if (keep & (1u << i)) stage[wpos++] = v[i];
+        __syncthreads();
+        for (u32 j = threadIdx.x; j < total; j += THREADS) out[off + j] = stage[j];
+        if (tile == num_tiles - 1 && threadIdx.x == 0) *out_count = off + total;
+        __syncthreads();
+    }
+}
+
+// The same anti-join for small candidate sets, whose keys lie far apart in
+// every level (the tail rounds of a fixpoint): each thread looks its ITEMS
+// candidates up in all levels at once, so a tile's dependent chain is one
+// bucket search long instead of one per level.
+template <int THREADS, int ITEMS>
+__global__ void __launch_bounds__(THREADS) anti_join_levels_sparse_kernel(const u64* buf_a, const u64* buf_b,
+                                                                          const u32* final_sel, const u64* n_ptr,
+                                                                          Levels levels, u64* out, u64* out_count,
+                                                                          u64* status, u32* tile_counter, u32 epoch,
+                                                                          u32* err) {
+    constexpr int kTile = THREADS * ITEMS;
+    __shared__ CompactShared<THREADS> cs;
+    __shared__ u64 stage[kTile];
+    const u64* keys = (final_sel && *final_sel) ? buf_b : buf_a;
+    const u64 n = *n_ptr;
+    const u64 num_tiles = (n + kTile - 1) / kTile;
+    if (num_tiles == 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) *out_count = 0;
+        return;
+    }
+    for (;;) {
+        if (threadIdx.x == 0) cs.tile = atomicAdd(tile_counter, 1u);
+        __syncthreads();
+        const u64 tile = cs.tile;
+        if (tile >= num_tiles) break;
+        const u64 base = tile * kTile + static_cast<u64>(threadIdx.x) * ITEMS;
+        u64 v[ITEMS];
+        u32 keep = 0;
+        u64 prev = (base > 0 && base - 1 < n) ? keys[base - 1] : 0;
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i) {
+            const u64 idx = base + i;
+            v[i] = 0;
+            if (idx < n) {
+                const u64 k = keys[idx];
+                v[i] = k;
+                if (idx == 0 || k != prev) keep |= 1u << i;
+                prev = k;
+            }
+        }
+        u64 pos[kMaxLevels][ITEMS];
+        u32 span[kMaxLevels][ITEMS], bucket[kMaxLevels][ITEMS];
+        u32 max_span = 0;
+#pragma unroll
+        for (int l = 0; l < kMaxLevels; ++l) {
+#pragma unroll
+            for (int i = 0; i < ITEMS; ++i) {
+                pos[l][i] = 0;
+                span[l][i] = bucket[l][i] = 0;
+                if (l < levels.n && (keep & (1u << i))) {
+                    u64 lo, hi;
+                    dir_range(levels, l, v[i], &lo, &hi);
+                    pos[l][i] = lo;
+                    span[l][i] = bucket[l][i] = static_cast<u32>(hi - lo);
+                    max_span = span[l][i] > max_span ? span[l][i] : max_span;
+                }
+            }
+        }
+        while (max_span > 1) {
+#pragma unroll
+            for (int l = 0; l < kMaxLevels; ++l) {
+#pragma unroll
+                for (int i = 0; i < ITEMS; ++i) {
+                    if (span[l][i] > 1) {
+                        const u32 half = span[l][i] >> 1;
+                        pos[l][i] = levels.keys[l][pos[l][i] + half - 1] < v[i] ? pos[l][i] + half : pos[l][i];
+                        span[l][i] -= half;
+                    }
+                }
+            }
+            max_span -= max_span >> 1;
+        }
+#pragma unroll
+        for (int l = 0; l < kMaxLevels; ++l) {
+#pragma unroll
+            for (int i = 0; i < ITEMS; ++i) {
+                if (bucket[l][i] > 0) {
+                    // The lower bound is pos or pos + 1; past the bucket's end
+                    // the keys belong to later buckets and cannot equal v.
+                    const u64 p = pos[l][i] + (levels.keys[l][pos[l][i]] < v[i] ? 1 : 0);
+                    if (p < levels.count[l] && levels.keys[l][p] == v[i]) keep &= ~(1u << i);
                 }
             }
         }

@@ -106,6 +106,8 @@ template <int THREADS, int CAP>
 __device__ void smem_radix_sort(u64** src, u64** dst, u32 n, const int* shifts, int passes, unsigned short* rank,
                                 unsigned short* warp_count, u32* digit_start, u32* scan_scratch) {
     constexpr int kWarps = THREADS / kWarp;
+    constexpr int kDigits = THREADS >= 256 ? 1 : 256 / THREADS;
+    static_assert(THREADS >= 256 || 256 % THREADS == 0, "digits split evenly over threads");
     const u32 lane = lane_id(), warp = warp_id();
     const u32 chunk = ((n + kWarps - 1) / kWarps + kWarp - 1) / kWarp * kWarp;  // per-warp run, multiple of 32
     for (int p = 0; p < passes; ++p) {
@@ -129,18 +131,32 @@ __device__ void smem_radix_sort(u64** src, u64** dst, u32 n, const int* shifts, 
             if (valid) rank[pos] = static_cast<unsigned short>(base + before);
         }
         __syncthreads();
-        // Digit t: exclusive prefix over warps, then over digits.
-        u32 running = 0;
-        if (threadIdx.x < 256) {
-            for (int w = 0; w < kWarps; ++w) {
-                const u32 c = warp_count[w * 256 + threadIdx.x];
-                warp_count[w * 256 + threadIdx.x] = static_cast<unsigned short>(running);
-                running += c;
+        // Each thread owns kDigits consecutive digits: exclusive prefix of a
+        // digit over warps, then over digits.
+        u32 digit_total[kDigits];
+        u32 thread_sum = 0;
+#pragma unroll
+        for (int j = 0; j < kDigits; ++j) {
+            const u32 d = threadIdx.x * kDigits + j;
+            u32 running = 0;
+            if (d < 256) {
+                for (int w = 0; w < kWarps; ++w) {
+                    const u32 c = warp_count[w * 256 + d];
+                    warp_count[w * 256 + d] = static_cast<unsigned short>(running);
+                    running += c;
+                }
             }
+            digit_total[j] = running;
+            thread_sum += running;
         }
         u32 total;
-        const u32 start = block_exclusive_scan<THREADS>(threadIdx.x < 256 ? running : 0u, scan_scratch, &total);
-        if (threadIdx.x < 256) digit_start[threadIdx.x] = start;
+        u32 start = block_exclusive_scan<THREADS>(thread_sum, scan_scratch, &total);
+#pragma unroll
+        for (int j = 0; j < kDigits; ++j) {
+            const u32 d = threadIdx.x * kDigits + j;
+            if (d < 256) digit_start[d] = start;
+            start += digit_total[j];
+        }
         __syncthreads();
         for (u32 pos = threadIdx.x; pos < n; pos += THREADS) {
             const u64 k = a[pos];
@@ -167,7 +183,7 @@ __device__ __forceinline__ int fused_sort_shifts(u32 v1_bits, u32 runs, int* shi
 constexpr u32 kRankRun = 48;
 
 template <int THREADS, int CAP, int ROWCAP>
-__global__ void __launch_bounds__(THREADS, 2) fused_join_distinct_kernel(FusedRoundArgs a) {
+__global__ void __launch_bounds__(THREADS, 512 / THREADS) fused_join_distinct_kernel(FusedRoundArgs a) {
     using L = FusedLayout<THREADS, CAP, ROWCAP>;
     constexpr int kRowItems = ROWCAP / THREADS;
     constexpr int kItems = CAP / THREADS;
