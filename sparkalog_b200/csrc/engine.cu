@@ -66,6 +66,7 @@ constexpr int kSetItems = 8;
 constexpr int kSetTile = kThreads * kSetItems;
 constexpr int kJoinItems = 8;
 constexpr int kJoinTile = kThreads * kJoinItems;
+constexpr u64 kMaxRelationRows = 0xffffffffull;  // row ids are u32
 constexpr int kLevelStage = 2048;  // level rows per shared-memory chunk of the anti-join (two buffers)
 constexpr int kSparseThreads = 128;  // anti-join of small candidate sets
 constexpr int kSparseItems = 4;
@@ -443,7 +444,7 @@ size_t target_count_base(const sparkalog_executor* ex, size_t t) {
     return base;
 }
 
-constexpr int kFusedThreads = 128;
+constexpr int kFusedThreads = 256;
 constexpr int kFusedCap = 1920;     // join output rows per fused tile (shared memory)
 constexpr int kFusedRowCap = 1024;  // DELTA rows per fused tile
 constexpr size_t kFusedFlagBase = 8;      // fallback flags live at err + 8 + target
@@ -497,14 +498,23 @@ struct StoreOps {
 
 namespace {
 
-StoreOps& store_ops(sparkalog_store* st) {
+// The store's operation scratch, created on first use; null (with the error
+// recorded) when its buffers cannot be allocated.
+StoreOps* store_ops(sparkalog_store* st) {
     if (!st->ops) {
         auto* ops = new StoreOps();
         cudaStream_t s = st->stream;
-        ops->counts.ensure(256, s);
-        ops->counters.ensure(256, s);
-        cudaMemsetAsync(ops->counters.ptr, 0, 256, s);
-        cudaMallocHost(&ops->host, 256);
+        cudaError_t e = ops->counts.ensure(256, s);
+        if (e == cudaSuccess) e = ops->counters.ensure(256, s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(ops->counters.ptr, 0, 256, s);
+        if (e == cudaSuccess) e = cudaMallocHost(&ops->host, 256);
+        if (e != cudaSuccess) {
+            ops->counts.release(s);
+            ops->counters.release(s);
+            delete ops;
+            fail(static_cast<int>(e), std::string("store scratch: ") + cudaGetErrorString(e));
+            return nullptr;
+        }
         st->ops = ops;
     }
     StoreOps& ops = *st->ops;
@@ -514,7 +524,7 @@ StoreOps& store_ops(sparkalog_store* st) {
         if (ops.ex.index_sort.status.ptr) cudaMemsetAsync(ops.ex.index_sort.status.ptr, 0, ops.ex.index_sort.status.bytes, s);
         ops.ex.epoch = 1;
     }
-    return ops;
+    return &ops;
 }
 
 void release_store_ops(sparkalog_store* st) {
@@ -537,7 +547,9 @@ int refresh_directories(sparkalog_store* st, RelState& r, cudaStream_t s, u64* l
 // append). ops.b is the sort's second buffer.
 int sorted_difference(sparkalog_store* st, u64 n, RelState& right, DevArray& out, u64* out_n) {
     cudaStream_t s = st->stream;
-    StoreOps& ops = store_ops(st);
+    StoreOps* ops_ptr = store_ops(st);
+    if (!ops_ptr) return static_cast<int>(cudaErrorMemoryAllocation);
+    StoreOps& ops = *ops_ptr;
     u32* err = ops.counters.as<u32>() + 32;
     SPK_CUDA(ops.b.ensure(n * 8, s), "cudaMallocAsync");
     SPK_CUDA(out.ensure(std::max<u64>(n, 1) * 8, s), "cudaMallocAsync");
@@ -580,7 +592,9 @@ int sorted_difference(sparkalog_store* st, u64 n, RelState& right, DevArray& out
 // Sorts and deduplicates DELTA of r in place (it may have been inserted unsorted).
 int sort_unique_delta(sparkalog_store* st, RelState& r) {
     cudaStream_t s = st->stream;
-    StoreOps& ops = store_ops(st);
+    StoreOps* ops_ptr = store_ops(st);
+    if (!ops_ptr) return static_cast<int>(cudaErrorMemoryAllocation);
+    StoreOps& ops = *ops_ptr;
     if (r.delta_n) {
         SPK_CUDA(ops.a.ensure(r.delta_n * 8, s), "cudaMallocAsync");
         SPK_CUDA(cudaMemcpyAsync(ops.a.ptr, r.delta.ptr, r.delta_n * 8, cudaMemcpyDeviceToDevice, s),
@@ -769,7 +783,7 @@ int sparkalog_store_insert_static(sparkalog_store* st, u32 id, const u32* first,
                                   int location) {
     if (!st) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null store");
     if (st->find(id)) return fail(SPARKALOG_E_DUPLICATE, "relation " + std::to_string(id) + " is already registered");
-    if (rows > 0xffffffffull) return fail(SPARKALOG_E_TOO_MANY_ROWS, "too many rows for u32 row ids");
+    if (rows > kMaxRelationRows) return fail(SPARKALOG_E_TOO_MANY_ROWS, "too many rows for u32 row ids");
     RelState r;
     int rc = pack_columns(st, first, second, rows, location, r.level[0], &r.sorted, &r.has_dups);
     if (rc) return rc;
@@ -783,7 +797,7 @@ int sparkalog_store_insert_recursive(sparkalog_store* st, u32 id, const u32* ful
                                      size_t delta_rows, int location) {
     if (!st) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null store");
     if (st->find(id)) return fail(SPARKALOG_E_DUPLICATE, "relation " + std::to_string(id) + " is already registered");
-    if (full_rows > 0xffffffffull || delta_rows > 0xffffffffull)
+    if (full_rows > kMaxRelationRows || delta_rows > kMaxRelationRows)
         return fail(SPARKALOG_E_TOO_MANY_ROWS, "too many rows for u32 row ids");
     RelState r;
     r.recursive = true;
@@ -880,7 +894,9 @@ int sparkalog_store_anti_join(sparkalog_store* st, u32 left_id, u32 right_id, u3
     RelState out;
     u64 out_n = 0;
     if (n > 0) {
-        StoreOps& ops = store_ops(st);
+        StoreOps* ops_ptr = store_ops(st);
+    if (!ops_ptr) return static_cast<int>(cudaErrorMemoryAllocation);
+    StoreOps& ops = *ops_ptr;
         SPK_CUDA(ops.a.ensure(n * 8, s), "cudaMallocAsync");
         SPK_CUDA(cudaMemcpyAsync(ops.a.ptr, left->level[0].ptr, n * 8, cudaMemcpyDeviceToDevice, s), "cudaMemcpyAsync");
         rc = sorted_difference(st, n, *right, out.level[0], &out_n);
@@ -900,7 +916,7 @@ int sparkalog_store_append(sparkalog_store* st, u32 id, const u32* first, const 
     if (!st) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null store");
     RelState* r = st->find(id);
     if (!r) return fail(SPARKALOG_E_MISSING, "relation " + std::to_string(id) + " is not registered");
-    if (rows > 0xffffffffull) return fail(SPARKALOG_E_TOO_MANY_ROWS, "too many rows for u32 row ids");
+    if (rows > kMaxRelationRows) return fail(SPARKALOG_E_TOO_MANY_ROWS, "too many rows for u32 row ids");
     if (rows == 0) return 0;
     cudaStream_t s = st->stream;
     if (!r->sorted || r->has_dups) {
@@ -908,7 +924,9 @@ int sparkalog_store_append(sparkalog_store* st, u32 id, const u32* first, const 
         if (rc) return rc;
         if (!r->sorted) return fail(SPARKALOG_E_UNSORTED_FULL, "FULL of relation " + std::to_string(id) + " is not sorted");
     }
-    StoreOps& ops = store_ops(st);
+    StoreOps* ops_ptr = store_ops(st);
+    if (!ops_ptr) return static_cast<int>(cudaErrorMemoryAllocation);
+    StoreOps& ops = *ops_ptr;
     bool sorted_in, dups_in;
     int rc = pack_columns(st, first, second, rows, location, ops.a, &sorted_in, &dups_in);
     if (rc) return rc;
@@ -917,6 +935,8 @@ int sparkalog_store_append(sparkalog_store* st, u32 id, const u32* first, const 
     rc = sorted_difference(st, rows, *r, fresh, &fresh_n);
     if (rc) return rc;
     if (fresh_n > 0) {
+        if (r->full_rows() + fresh_n > kMaxRelationRows)
+            return fail(SPARKALOG_E_TOO_MANY_ROWS, "relation would exceed 2^32 - 1 rows (u32 row ids)");
         // FULL: new rows are disjoint from every level, so they merge into TAIL
         // (level 0 for a static relation, which keeps a single run).
         const int l = r->recursive ? spk::kMaxLevels - 1 : 0;
@@ -968,7 +988,9 @@ int sparkalog_store_extract_segment(sparkalog_store* st, u32 id, u32 shift, u32 
         lv.count[lv.n] = r->level_n[l];
         ++lv.n;
     }
-    StoreOps& ops = store_ops(st);
+    StoreOps* ops_ptr = store_ops(st);
+    if (!ops_ptr) return static_cast<int>(cudaErrorMemoryAllocation);
+    StoreOps& ops = *ops_ptr;
     u64 bounds[2 * spk::kMaxLevels] = {0};
     if (lv.n) {
         spk::level_bounds_kernel<<<1, 32, 0, s>>>(lv, lo_key, hi_key, ops.counts.as<u64>());
@@ -1027,7 +1049,9 @@ int sparkalog_store_remove_segments(sparkalog_store* st, u32 id, u32 shift, cons
         if (segments[k] >= segs) return fail(SPARKALOG_E_INVALID_ARGUMENT, "segment out of range");
         bitmap[segments[k] >> 5] |= 1u << (segments[k] & 31);
     }
-    StoreOps& ops = store_ops(st);
+    StoreOps* ops_ptr = store_ops(st);
+    if (!ops_ptr) return static_cast<int>(cudaErrorMemoryAllocation);
+    StoreOps& ops = *ops_ptr;
     SPK_CUDA(ops.bitmap.ensure(words * 4, s), "cudaMallocAsync");
     SPK_CUDA(cudaMemcpyAsync(ops.bitmap.ptr, bitmap.data(), words * 4, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
     auto filter = [&](DevArray& buf, u64& n, DevArray& spare) -> int {
@@ -1606,6 +1630,15 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
         const u32 err_bits = static_cast<u32>(ex->host_counts[ex->counts_words] & 0xffffffffu);
         if (err_bits & ~spk::kErrCapacity)
             return fail(SPARKALOG_E_DEVICE_FAULT, "device error bits " + std::to_string(err_bits));
+
+        // Row ids (directories, join indexes) are u32: refuse the round before
+        // any relation changes if a FULL would outgrow them.
+        for (size_t ti = 0; ti < ex->targets.size(); ++ti) {
+            const TargetRT& t = ex->targets[ti];
+            const u64 newt_n = ex->host_counts[target_count_base(ex, ti) + t.rules.size() + 1];
+            if (st->find(t.id)->full_rows() + newt_n > kMaxRelationRows)
+                return fail(SPARKALOG_E_TOO_MANY_ROWS, "relation would exceed 2^32 - 1 rows (u32 row ids)");
+        }
 
         // TargetRuntime::apply: FULL u= NEWT (into the levels), DELTA <- NEWT.
         for (size_t ti = 0; ti < ex->targets.size(); ++ti) {

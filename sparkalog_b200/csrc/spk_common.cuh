@@ -30,11 +30,15 @@ __device__ __forceinline__ u32 lanemask_lt() {
 
 __device__ __forceinline__ u32 lane_id() { return threadIdx.x & (kWarp - 1); }
 
-// Asynchronous 8-byte global -> shared copies (cp.async, L1-allocating), so a
+// Asynchronous 8- and 4-byte global -> shared copies (cp.async, L1-allocating), so a
 // thread keeps many loads in flight without holding them in registers.
 __device__ __forceinline__ void cp_async_8(void* smem, const void* gmem) {
     const u32 s = static_cast<u32>(__cvta_generic_to_shared(smem));
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_4(void* smem, const void* gmem) {
+    const u32 s = static_cast<u32>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
@@ -110,17 +114,20 @@ __device__ __forceinline__ u64 lookback_exclusive(u64* status, size_t stride, u6
     return exclusive;
 }
 
-// Warp-cooperative look-back for a single channel (used by compaction
-// kernels): lane i inspects tile (tile - 1 - i) so 32 predecessors are read per
-// step. Must be called by all 32 lanes of one warp; every lane gets the result.
-__device__ __forceinline__ u64 warp_lookback_exclusive(u64* status, u64 tile, u64 aggregate, u32 epoch,
-                                                       u32* err) {
+// First half of a decoupled look-back: publishes a tile's aggregate (tile 0:
+// its inclusive prefix) as soon as it is known, so successors can move on
+// while this tile still works. Called by one thread.
+__device__ __forceinline__ void lookback_publish(u64* status, u64 tile, u64 aggregate, u32 epoch) {
+    st_volatile(status + tile, make_status(epoch, tile == 0 ? kFlagInclusive : kFlagAggregate, aggregate));
+}
+
+// Second half: the exclusive prefix from the predecessors' words (lane i
+// inspects tile (tile - 1 - i), so 32 predecessors are read per step), then
+// the tile's inclusive prefix is published. Must be called by all 32 lanes of
+// one warp; every lane gets the result.
+__device__ __forceinline__ u64 warp_lookback_resolve(u64* status, u64 tile, u64 aggregate, u32 epoch, u32* err) {
     const u32 lane = lane_id();
-    if (tile == 0) {
-        if (lane == 0) st_volatile(status, make_status(epoch, kFlagInclusive, aggregate));
-        return 0;
-    }
-    if (lane == 0) st_volatile(status + tile, make_status(epoch, kFlagAggregate, aggregate));
+    if (tile == 0) return 0;
     u64 exclusive = 0;
     long long base = static_cast<long long>(tile) - 1;
     u32 spins = 0;
@@ -161,6 +168,15 @@ __device__ __forceinline__ u64 warp_lookback_exclusive(u64* status, u64 tile, u6
     }
     if (lane == 0) st_volatile(status + tile, make_status(epoch, kFlagInclusive, exclusive + aggregate));
     return exclusive;
+}
+
+// Warp-cooperative look-back for a single channel (used by compaction
+// kernels): publish and resolve back to back. Must be called by all 32 lanes
+// of one warp; every lane gets the result.
+__device__ __forceinline__ u64 warp_lookback_exclusive(u64* status, u64 tile, u64 aggregate, u32 epoch,
+                                                       u32* err) {
+    if (lane_id() == 0) lookback_publish(status, tile, aggregate, epoch);
+    return warp_lookback_resolve(status, tile, aggregate, epoch, err);
 }
 
 // ---------------------------------------------------------------------------

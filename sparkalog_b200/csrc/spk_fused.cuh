@@ -1,6 +1,6 @@
-// Fused join -> distinct for rules whose join output starts with DELTA's
-// first column (the transitive-closure shape path(x, z) :- path(x, y),
-// edge(y, z)): the candidate rows of a round never reach HBM unsorted.
+// Fused join -> order for rules whose join output starts with DELTA's first
+// column (the transitive-closure shape path(x, z) :- path(x, y), edge(y, z)):
+// the candidate rows of a round reach HBM only once, already sorted.
 //
 // DELTA is sorted by (first, second), and the join emits DELTA-row-major, so
 // the join output is already ordered by its first column x. A tile takes a
@@ -10,10 +10,11 @@
 // rows are placed by rank (a row's position is the number of smaller rows of
 // its run, ties broken by emission order) when every run is short, else the
 // tile is sorted by (run, second column) with a stable LSD radix sort in
-// shared memory over only the bits that vary. Adjacent duplicates are dropped
-// and the unique rows compacted with a decoupled look-back in tile order,
-// which is x order: the output is the sorted distinct candidate set that the
-// anti-join against FULL consumes.
+// shared memory over only the bits that vary. Tiles are placed with a
+// decoupled look-back in tile order, which is x order; a tile publishes its
+// size as soon as its join count is known, so the wait overlaps its ordering
+// work. Equal rows stay adjacent: the anti-join against FULL that consumes
+// this output keeps the first of each run of equal rows (BinaryDistinct).
 //
 // A tile whose x-run is longer than the tile's row capacity, or whose output
 // exceeds the shared-memory capacity, sets *fallback; the host then redoes
@@ -86,15 +87,14 @@ __device__ __forceinline__ void index_lookup(const FusedRoundArgs& a, u32 key, u
 template <int THREADS, int CAP, int ROWCAP>
 struct FusedLayout {
     static constexpr int kWarps = THREADS / kWarp;
-    static constexpr size_t kKeysA = 0;
-    static constexpr size_t kKeysB = kKeysA + CAP * sizeof(u64);
-    static constexpr size_t kRowOffset = kKeysB + CAP * sizeof(u64);          // u32[ROWCAP + 1]
-    static constexpr size_t kRowBegin = kRowOffset + (ROWCAP + 4) * sizeof(u32);  // u32[ROWCAP]
-    static constexpr size_t kRunX = kRowBegin + ROWCAP * sizeof(u32);          // u32[ROWCAP]
-    static constexpr size_t kRunOff = kRunX + ROWCAP * sizeof(u32);            // u32[ROWCAP + 1]
-    static constexpr size_t kRowRank = kRunOff + (ROWCAP + 4) * sizeof(u32);   // u16[ROWCAP]
-    static constexpr size_t kRank = kRowRank + ROWCAP * sizeof(unsigned short); // u16[CAP]
-    static constexpr size_t kWarpCount = kRank + CAP * sizeof(unsigned short);  // u16[kWarps][256]
+    static constexpr size_t kKeysA = 0;                                        // u64[CAP]
+    static constexpr size_t kKeysB = kKeysA + CAP * sizeof(u64);               // u64[CAP]
+    static constexpr size_t kRangeLo = kKeysB + CAP * sizeof(u64);             // u32[ROWCAP]
+    static constexpr size_t kRangeHi = kRangeLo + ROWCAP * sizeof(u32);        // u32[ROWCAP]
+    static constexpr size_t kRunX = kRangeHi + ROWCAP * sizeof(u32);           // u32[ROWCAP]
+    static constexpr size_t kRunOff = kRunX + ROWCAP * sizeof(u32);            // u32[ROWCAP + 4]
+    static constexpr size_t kRank = kRunOff + (ROWCAP + 4) * sizeof(u32);      // u16[CAP]
+    static constexpr size_t kWarpCount = kRank + CAP * sizeof(unsigned short); // u16[kWarps][256]
     static constexpr size_t kDigitStart = kWarpCount + kWarps * 256 * sizeof(unsigned short);
     static constexpr size_t kBytes = kDigitStart + 256 * sizeof(u32);
 };
@@ -182,28 +182,32 @@ __device__ __forceinline__ int fused_sort_shifts(u32 v1_bits, u32 runs, int* shi
 // Runs with at most this many output rows are placed by rank.
 constexpr u32 kRankRun = 48;
 
+// Packed per-thread scan value: match count in the low kCountBits, x-run
+// starts above (a tile has fewer than 2048 rows, so starts fit in 11 bits).
+constexpr int kCountBits = 52;
+constexpr u64 kCountMask = (1ull << kCountBits) - 1;
+
 template <int THREADS, int CAP, int ROWCAP>
-__global__ void __launch_bounds__(THREADS, 512 / THREADS) fused_join_distinct_kernel(FusedRoundArgs a) {
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS) fused_join_distinct_kernel(FusedRoundArgs a) {
     using L = FusedLayout<THREADS, CAP, ROWCAP>;
     constexpr int kRowItems = ROWCAP / THREADS;
-    constexpr int kItems = CAP / THREADS;
-    static_assert(kItems <= 32, "keep mask is 32 bits");
-    static_assert(ROWCAP < 65536 && CAP < 65536, "16-bit ranks and counts");
+    static_assert(ROWCAP % THREADS == 0, "rows split evenly over threads");
+    static_assert(ROWCAP < 2048 && CAP < 65536, "11-bit run starts, 16-bit ranks and counts");
+    static_assert(ROWCAP <= CAP, "DELTA rows are staged in the second key buffer");
     extern __shared__ __align__(16) unsigned char smem[];
     u64* keys_a = reinterpret_cast<u64*>(smem + L::kKeysA);
     u64* keys_b = reinterpret_cast<u64*>(smem + L::kKeysB);
-    u32* row_offset = reinterpret_cast<u32*>(smem + L::kRowOffset);
-    u32* row_begin = reinterpret_cast<u32*>(smem + L::kRowBegin);
+    u32* range_lo = reinterpret_cast<u32*>(smem + L::kRangeLo);
+    u32* range_hi = reinterpret_cast<u32*>(smem + L::kRangeHi);
     u32* run_x = reinterpret_cast<u32*>(smem + L::kRunX);
     u32* run_off = reinterpret_cast<u32*>(smem + L::kRunOff);
-    unsigned short* row_rank = reinterpret_cast<unsigned short*>(smem + L::kRowRank);
     unsigned short* rank = reinterpret_cast<unsigned short*>(smem + L::kRank);
     unsigned short* warp_count = reinterpret_cast<unsigned short*>(smem + L::kWarpCount);
     u32* digit_start = reinterpret_cast<u32*>(smem + L::kDigitStart);
-    __shared__ u32 scan_scratch[THREADS / kWarp + 1];
-    __shared__ CompactShared<THREADS> cs;
+    __shared__ u64 scan_scratch[THREADS / kWarp + 1];
+    __shared__ u32 scan_scratch32[THREADS / kWarp + 1];
     __shared__ u64 bounds[2];
-    __shared__ u32 bail;
+    __shared__ u64 tile_shared, out_base;
 
     const u64 n = a.delta_rows;
     const u64 R = a.rows_per_tile;
@@ -213,12 +217,9 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) fused_join_distinct_ke
         return;
     }
     for (;;) {
-        if (threadIdx.x == 0) {
-            cs.tile = atomicAdd(a.tile_counter, 1u);
-            bail = 0;
-        }
+        if (threadIdx.x == 0) tile_shared = atomicAdd(a.tile_counter, 1u);
         __syncthreads();
-        const u64 tile = cs.tile;
+        const u64 tile = tile_shared;
         if (tile >= num_tiles) break;
 
         // 1. Rows [B(tile), B(tile + 1)): the first x boundary at or after each
@@ -246,77 +247,117 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) fused_join_distinct_ke
         const bool rows_ok = row0 != ~0ull && row1 != ~0ull && row1 - row0 <= static_cast<u64>(ROWCAP);
         const u32 nrows = rows_ok ? static_cast<u32>(row1 - row0) : 0u;
 
-        // 2. Match counts per row and their scan; x-runs: value, rank, offset.
-        const u32 local0 = threadIdx.x * kRowItems;
-        u32 cnt[kRowItems];
-        u32 starts = 0, sum = 0;
-#pragma unroll
-        for (int i = 0; i < kRowItems; ++i) {
-            const u32 r = local0 + i;
-            cnt[i] = 0;
-            if (r < nrows) {
-                const u64 row = a.delta[row0 + r];
-                u32 begin, c;
-                index_lookup(a, pair_col(row, a.left_key), &begin, &c);
-                row_begin[r] = begin;
-                cnt[i] = c;
-                starts += (r == 0 || (row >> 32) != (a.delta[row0 + r - 1] >> 32)) ? 1u : 0u;
-            }
-            sum += cnt[i];
-        }
-        u32 total, runs;
-        u32 off = block_exclusive_scan<THREADS>(sum, scan_scratch, &total);
+        // 2. The tile's DELTA rows into shared memory (keys_b is free until
+        // the emitted keys are ordered), then every row's index range,
+        // gathered with asynchronous copies (each thread issues all of its
+        // gathers, then waits once).
+        u64* trow = keys_b;
+        for (u32 r = threadIdx.x; r < nrows; r += THREADS) cp_async_8(trow + r, a.delta + row0 + r);
+        cp_async_commit();
+        cp_async_wait<0>();
         __syncthreads();
-        u32 rk = block_exclusive_scan<THREADS>(starts, scan_scratch, &runs);
+        if (a.dense_offsets) {
+            for (u32 r = threadIdx.x; r < nrows; r += THREADS) {
+                const u32 key = pair_col(trow[r], a.left_key);
+                if (key < a.dense_keys) {
+                    cp_async_4(range_lo + r, a.dense_offsets + key);
+                    cp_async_4(range_hi + r, a.dense_offsets + key + 1);
+                } else {
+                    range_lo[r] = range_hi[r] = 0;
+                }
+            }
+            cp_async_commit();
+            cp_async_wait<0>();
+        } else {
+            for (u32 r = threadIdx.x; r < nrows; r += THREADS) {
+                u32 f, c;
+                index_lookup(a, pair_col(trow[r], a.left_key), &f, &c);
+                range_lo[r] = f;
+                range_hi[r] = f + c;
+            }
+        }
+        __syncthreads();
+
+        // 3. One scan of (x-run starts, match counts) over the rows (each
+        // thread owns kRowItems consecutive rows), then every thread emits
+        // its rows' matches: the run's rank per output and the right row (or
+        // DELTA row) gathered into keys_a.
+        const u32 local0 = threadIdx.x * kRowItems;
+        u64 packed = 0;
 #pragma unroll
         for (int i = 0; i < kRowItems; ++i) {
             const u32 r = local0 + i;
             if (r < nrows) {
-                const u64 row = a.delta[row0 + r];
-                if (r == 0 || (row >> 32) != (a.delta[row0 + r - 1] >> 32)) {
-                    run_x[rk] = static_cast<u32>(row >> 32);
-                    run_off[rk] = off;
-                    ++rk;
-                }
-                row_rank[r] = static_cast<unsigned short>(rk - 1);
+                const u64 start = (r == 0 || (trow[r] >> 32) != (trow[r - 1] >> 32)) ? 1u : 0u;
+                packed += (start << kCountBits) + (range_hi[r] - range_lo[r]);
             }
-            row_offset[r] = off;
-            off += cnt[i];
+        }
+        u64 packed_total;
+        const u64 packed_excl = block_exclusive_scan<THREADS>(packed, scan_scratch, &packed_total);
+        const u64 total64 = packed_total & kCountMask;
+        const u32 runs = static_cast<u32>(packed_total >> kCountBits);
+        const bool ok = rows_ok && total64 <= static_cast<u64>(CAP);
+        const u32 total = ok ? static_cast<u32>(total64) : 0u;
+        u32* match_row = reinterpret_cast<u32*>(keys_a) + CAP;  // row ids of an indexed right relation
+        if (ok) {
+            u32 off = static_cast<u32>(packed_excl & kCountMask);
+            u32 rk = static_cast<u32>(packed_excl >> kCountBits);
+#pragma unroll
+            for (int i = 0; i < kRowItems; ++i) {
+                const u32 r = local0 + i;
+                if (r < nrows) {
+                    const u64 row = trow[r];
+                    if (r == 0 || (row >> 32) != (trow[r - 1] >> 32)) {
+                        run_x[rk] = static_cast<u32>(row >> 32);
+                        run_off[rk] = off;
+                        ++rk;
+                    }
+                    const u32 first = range_lo[r], count = range_hi[r] - first;
+                    for (u32 k = 0; k < count; ++k) {
+                        const u32 o = off + k;
+                        rank[o] = static_cast<unsigned short>(rk - 1);
+                        if (a.v1_side != 1) keys_a[o] = row;
+                        else if (a.rows) cp_async_4(match_row + o, a.rows + first + k);
+                        else cp_async_8(keys_a + o, a.right + first + k);
+                    }
+                    off += count;
+                }
+            }
         }
         if (threadIdx.x == 0) {
-            row_offset[ROWCAP] = total;
-            run_off[runs] = total;
-            if (!rows_ok || total > static_cast<u32>(CAP)) bail = 1;
-            else if (total) atomicAdd(a.join_rows, static_cast<unsigned long long>(total));
+            run_off[runs < ROWCAP ? runs : ROWCAP] = total;
+            if (ok && total) atomicAdd(a.join_rows, static_cast<unsigned long long>(total));
+            if (!ok) atomicOr(a.fallback, 1u);
+            // Publish the tile's output size now: successors resolve their
+            // offsets while this tile still orders its rows.
+            lookback_publish(a.status, tile, total, a.epoch);
         }
+        cp_async_commit();
+        cp_async_wait<0>();
         __syncthreads();
-        const bool ok = bail == 0;
-        if (!ok) total = 0;
+        if (a.v1_side == 1 && a.rows) {
+            // Indexed right relation: the row ids arrived, now the rows (into
+            // keys_b; the DELTA rows are no longer needed).
+            for (u32 o = threadIdx.x; o < total; o += THREADS) cp_async_8(keys_b + o, a.right + match_row[o]);
+            cp_async_commit();
+            cp_async_wait<0>();
+            __syncthreads();
+        }
         int long_run = 0;
-        for (u32 r = threadIdx.x; r < (ok ? runs : 0u); r += THREADS)
-            long_run |= run_off[r + 1] - run_off[r] > kRankRun ? 1 : 0;
-
-        // 3. Emit (x-run rank << 32 | second column) keys into shared memory.
-        for (u32 o = threadIdx.x; o < total; o += THREADS) {
-            u32 lo = 0, hi = ROWCAP;
-            while (hi - lo > 1) {
-                const u32 mid = (lo + hi) >> 1;
-                if (row_offset[mid] <= o) lo = mid;
-                else hi = mid;
-            }
-            const u32 m = row_begin[lo] + (o - row_offset[lo]);
-            const u32 right_row = a.rows ? a.rows[m] : m;
-            const u32 v1 = a.v1_side == 1 ? pair_col(a.right[right_row], a.v1_col)
-                                          : pair_col(a.delta[row0 + lo], a.v1_col);
-            keys_a[o] = (static_cast<u64>(row_rank[lo]) << 32) | v1;
+        {
+            const u64* raw = (a.v1_side == 1 && a.rows) ? keys_b : keys_a;
+            for (u32 o = threadIdx.x; o < total; o += THREADS)
+                keys_a[o] = (static_cast<u64>(rank[o]) << 32) | pair_col(raw[o], a.v1_col);
+            for (u32 r = threadIdx.x; r < (ok ? runs : 0u); r += THREADS)
+                long_run |= run_off[r + 1] - run_off[r] > kRankRun ? 1 : 0;
         }
         long_run = __syncthreads_or(long_run);
 
         // 4. Order the tile by (x, second column) into `sorted`.
         u64* sorted;
-        u64* spare;
         if (!long_run) {
-            // Rank placement within each (short) x-run.
+            // Rank placement within each (short) x-run; equal rows keep
+            // their emission order, so every output slot is written once.
             for (u32 o = threadIdx.x; o < total; o += THREADS) {
                 const u64 k = keys_a[o];
                 const u32 r = static_cast<u32>(k >> 32), v = static_cast<u32>(k);
@@ -329,47 +370,31 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) fused_join_distinct_ke
                 keys_b[s0 + before] = (static_cast<u64>(run_x[r]) << 32) | v;
             }
             sorted = keys_b;
-            spare = keys_a;
         } else {
             int shifts[8];
             const int passes = fused_sort_shifts(a.v1_bits, runs, shifts);
             u64* src = keys_a;
             u64* dst = keys_b;
             smem_radix_sort<THREADS, CAP>(&src, &dst, total, shifts, passes, rank, warp_count, digit_start,
-                                          scan_scratch);
+                                          scan_scratch32);
             for (u32 o = threadIdx.x; o < total; o += THREADS) {
                 const u64 k = src[o];
                 src[o] = (static_cast<u64>(run_x[k >> 32]) << 32) | static_cast<u32>(k);
             }
             sorted = src;
-            spare = dst;
         }
-        __syncthreads();
 
-        // 5. Unique (each thread owns kItems consecutive sorted rows; runs of
-        // different tiles never share a row) and compaction in tile order.
-        u32 keep = 0;
-        u64 v[kItems];
-        const u32 base = threadIdx.x * kItems;
-#pragma unroll
-        for (int i = 0; i < kItems; ++i) {
-            const u32 o = base + i;
-            v[i] = 0;
-            if (o < total) {
-                v[i] = sorted[o];
-                if (o == 0 || v[i] != sorted[o - 1]) keep |= 1u << i;
-            }
+        // 5. The tile's offset (its predecessors have mostly published by
+        // now), then the ordered rows out, coalesced. Duplicates stay: the
+        // anti-join that consumes this output drops adjacent equal rows.
+        if (warp_id() == 0) {
+            const u64 g = warp_lookback_resolve(a.status, tile, total, a.epoch, a.err);
+            if (lane_id() == 0) out_base = g;
         }
-        u32 excl, kept;
-        const u64 out_off = compact_offsets<THREADS>(__popc(keep), &excl, &kept, tile, a.status, a.epoch, a.err, cs);
-        if (!ok && threadIdx.x == 0) atomicOr(a.fallback, 1u);
-        u32 w = excl;
-#pragma unroll
-        for (int i = 0; i < kItems; ++i)
-            if (keep & (1u << i)) spare[w++] = v[i];
         __syncthreads();
-        for (u32 j = threadIdx.x; j < kept; j += THREADS) a.out[out_off + j] = spare[j];
-        if (tile == num_tiles - 1 && threadIdx.x == 0) *a.out_count = out_off + kept;
+        const u64 base = out_base;
+        for (u32 o = threadIdx.x; o < total; o += THREADS) a.out[base + o] = sorted[o];
+        if (tile == num_tiles - 1 && threadIdx.x == 0) *a.out_count = base + total;
         __syncthreads();
     }
 }

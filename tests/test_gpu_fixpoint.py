@@ -294,3 +294,17 @@ def test_fused_and_general_rounds_agree(cuda, n, e, seed):
         out.append((summary.iterations, summary.total_new_rows, f0, f1))
     assert out[0][:2] == out[1][:2]
     assert np.array_equal(out[0][2], out[1][2]) and np.array_equal(out[0][3], out[1][3])
+
+
+def test_fused_join_distinct_through_sorted_index(cuda):
+    # p(x, z) :- p(x, y), e(z, y): the right relation is indexed on its second
+    # column, so the fused kernel gathers right rows through the index's row ids.
+    from sparkalog_b200.relational import BinaryEqualityJoin, JoinInput, JoinProjection, RecursiveRulePlan
+
+    src, dst = generators.er_edges(5000, 5200, 23)
+    e0, e1 = oracle.btree_pairs(src, dst)
+    join = BinaryEqualityJoin(1, 1, (JoinProjection(JoinInput.LEFT, 0), JoinProjection(JoinInput.RIGHT, 0)))
+    rule = RecursiveRulePlan(_rid(1), _rid(1), _rid(0), join)
+    stats = _tc_with_stats(e0, e1, rule,
+                           oracle.rule_plan(1, 1, 0, left_key=1, right_key=1, projection=((0, 0), (1, 0))))
+    assert stats["classes"]["join_distinct"]["launches"] > 0
