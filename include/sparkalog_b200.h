@@ -292,6 +292,16 @@ SPARKALOG_API int sparkalog_executor_set_profiling(sparkalog_executor* executor,
  * runs the general join, radix sort and anti-join; results are identical. No
  * counterpart in the reference. */
 SPARKALOG_API int sparkalog_executor_set_fused(sparkalog_executor* executor, int enable);
+
+/* Enables or disables (default) FULL's hash set for recursive relations. With
+ * it, the anti-join of a round's candidates against FULL is one hash probe per
+ * candidate instead of a search of each sorted level; the set is built from
+ * the levels on first use (128 bytes of slots per row of FULL, only when the
+ * device has that much free memory) and takes every round's NEWT. Results are
+ * identical either way; on sorted candidates the level search keeps cache
+ * locality that hashing gives up, so the set is opt-in. No counterpart in the
+ * reference. */
+SPARKALOG_API int sparkalog_executor_set_member_set(sparkalog_executor* executor, int enable);
 SPARKALOG_API int sparkalog_executor_stats(sparkalog_executor* executor, sparkalog_kernel_stats* out, int reset);
 
 /* Grows the current device's stream-ordered memory pool to at least `bytes`

@@ -51,6 +51,7 @@ TIER_B = [
     "sparkalog_executor_segment_stats",
     "sparkalog_executor_set_profiling",
     "sparkalog_executor_set_fused",
+    "sparkalog_executor_set_member_set",
     "sparkalog_executor_stats",
     "sparkalog_reserve_device_memory",
     "sparkalog_last_error",
@@ -178,6 +179,8 @@ def load() -> ctypes.CDLL:
     L.sparkalog_executor_set_profiling.restype = i
     L.sparkalog_executor_set_fused.argtypes = [vp, i]
     L.sparkalog_executor_set_fused.restype = i
+    L.sparkalog_executor_set_member_set.argtypes = [vp, i]
+    L.sparkalog_executor_set_member_set.restype = i
     L.sparkalog_executor_stats.argtypes = [vp, ctypes.POINTER(KernelStatsC), i]
     L.sparkalog_executor_stats.restype = i
     L.sparkalog_reserve_device_memory.argtypes = [ctypes.c_size_t, vp]

@@ -27,6 +27,7 @@
 #include "spk_join.cuh"
 #include "spk_radix.cuh"
 #include "spk_fused.cuh"
+#include "spk_member.cuh"
 #include "spk_setops.cuh"
 
 #include <algorithm>
@@ -148,6 +149,14 @@ struct RelState {
     DevArray delta, newt;
     u64 delta_n = 0;
     bool delta_sorted = true;  // DELTA is sorted and unique (always after a round)
+    // FULL as a hash set (spk::MemberSet) for the anti-join of recursive
+    // relations; built lazily from the levels, kept in step with every round's
+    // NEWT, dropped when FULL changes otherwise or the load passes one half.
+    DevArray member;         // 4 * member_groups u64 slots
+    DevArray member_flag;    // u32: the row spk::kEmptySlot is a member
+    u64 member_groups = 0;   // power of two
+    u64 member_count = 0;    // rows inserted
+    bool member_valid = false;
 
     u64 full_rows() const {
         u64 n = 0;
@@ -283,6 +292,65 @@ int refresh_directories(sparkalog_store* st, RelState& r, cudaStream_t s, u64* l
     return 0;
 }
 
+// FULL's hash set (spk::MemberSet). The host keeps its load at most one half
+// and builds it with sixteen slots per row, so a recursive FULL can grow
+// eightfold before the set is rebuilt.
+constexpr u64 kMemberMinGroups = 4096;
+
+spk::MemberSet member_set(RelState& r) {
+    return spk::MemberSet{r.member.as<u64>(), r.member_groups - 1, r.member_flag.as<u32>()};
+}
+
+// Builds the set from every level of FULL. Leaves member_valid false (and
+// returns 0) when the device has too little free memory for it; the caller
+// then searches the sorted levels instead.
+int member_build(RelState& r, u32* err, cudaStream_t s, u64* launches) {
+    const u64 rows = r.full_rows();
+    u64 groups = kMemberMinGroups;
+    while (groups < 4 * rows) groups <<= 1;
+    const size_t bytes = groups * 32;
+    r.member_valid = false;
+    if (bytes > r.member.bytes) {
+        size_t free_bytes = 0, total_bytes = 0;
+        if (cudaMemGetInfo(&free_bytes, &total_bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return 0;
+        }
+        if (bytes > free_bytes / 2) return 0;
+    }
+    SPK_CUDA(r.member.ensure(bytes, s), "cudaMallocAsync");
+    SPK_CUDA(r.member_flag.ensure(256, s), "cudaMallocAsync");
+    SPK_CUDA(cudaMemsetAsync(r.member.ptr, 0xff, bytes, s), "cudaMemsetAsync");
+    SPK_CUDA(cudaMemsetAsync(r.member_flag.ptr, 0, 4, s), "cudaMemsetAsync");
+    r.member_groups = groups;
+    const spk::MemberSet set = member_set(r);
+    for (int l = 0; l < spk::kMaxLevels; ++l) {
+        if (r.level_n[l] == 0) continue;
+        spk::member_insert_kernel<<<simple_grid(r.level_n[l]), 256, 0, s>>>(r.level[l].as<u64>(), r.level_n[l], set,
+                                                                           err);
+        SPK_CUDA(cudaGetLastError(), "member_insert_kernel");
+        if (launches) *launches += 1;
+    }
+    r.member_count = rows;
+    r.member_valid = true;
+    return 0;
+}
+
+// Adds rows (new to FULL, distinct) to a valid set; drops the set instead
+// when they would push its load past one half.
+int member_add(RelState& r, const u64* rows, u64 n, u32* err, cudaStream_t s, u64* launches) {
+    if (!r.member_valid || n == 0) return 0;
+    if ((r.member_count + n) * 2 > r.member_groups * 4) {
+        r.member_valid = false;
+        return 0;
+    }
+    spk::member_insert_kernel<<<simple_grid(n), 256, 0, s>>>(rows, n, member_set(r), err);
+    SPK_CUDA(cudaGetLastError(), "member_insert_kernel");
+    if (launches) *launches += 1;
+    r.member_count += n;
+    return 0;
+}
+
 struct SortScratch {
     DevArray plan;     // RadixPlan
     DevArray status;   // look-back words
@@ -352,6 +420,7 @@ struct sparkalog_executor {
     };
     bool profiling = false;
     bool fused_enabled = true;
+    bool member_enabled = false;  // anti-join through FULL's hash set (opt-in)
     std::vector<cudaEvent_t> free_events;
     std::vector<Timing> timings;
     sparkalog_kernel_stats stats{};
@@ -449,6 +518,7 @@ constexpr int kFusedCap = 1920;     // join output rows per fused tile (shared m
 constexpr int kFusedRowCap = 1024;  // DELTA rows per fused tile
 constexpr size_t kFusedFlagBase = 8;      // fallback flags live at err + 8 + target
 constexpr size_t kFusedMaxTargets = 48;
+constexpr size_t kMemberErrWord = kCounterWords + kFusedFlagBase + kFusedMaxTargets + 4;
 
 // The fused round applies to a target with one rule whose join output starts
 // with DELTA's first column (then the join output is sorted by it) while
@@ -768,6 +838,8 @@ void sparkalog_store_destroy(sparkalog_store* st) {
         kv.second.spare.release(s);
         kv.second.delta.release(s);
         kv.second.newt.release(s);
+        kv.second.member.release(s);
+        kv.second.member_flag.release(s);
     }
     st->scratch_u32[0].release(s);
     st->scratch_u32[1].release(s);
@@ -948,6 +1020,8 @@ int sparkalog_store_append(sparkalog_store* st, u32 id, const u32* first, const 
         swap_arrays(r->level[l], r->spare);
         r->level_n[l] = tn;
         r->dir_valid[l] = false;
+        rc = member_add(*r, fresh.as<u64>(), fresh_n, ops.counters.as<u32>() + 33, s, nullptr);
+        if (rc) return rc;
         if (r->recursive) {
             // DELTA u= fresh rows (DELTA is part of FULL, so they are disjoint).
             if (!r->delta_sorted) {
@@ -964,8 +1038,13 @@ int sparkalog_store_append(sparkalog_store* st, u32 id, const u32* first, const 
         }
         r->version += 1;
     }
+    SPK_CUDA(cudaMemcpyAsync(ops.host + 2, ops.counters.as<u32>() + 33, 4, cudaMemcpyDeviceToHost, s),
+             "cudaMemcpyAsync");
     SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
     fresh.release(s);
+    const u32 member_bits = static_cast<u32>(ops.host[2] & 0xffffffffu);
+    if (member_bits)
+        return fail(SPARKALOG_E_DEVICE_FAULT, "device error bits " + std::to_string(member_bits) + " (hash set of FULL)");
     return 0;
 }
 
@@ -1076,6 +1155,7 @@ int sparkalog_store_remove_segments(sparkalog_store* st, u32 id, u32 shift, cons
         if (rc) return rc;
         r->dir_valid[l] = false;
     }
+    r->member_valid = false;  // the hash set cannot drop rows: rebuilt on next use
     if (r->recursive) {
         int rc = filter(r->delta, r->delta_n, r->newt);
         if (rc) return rc;
@@ -1239,6 +1319,12 @@ int sparkalog_executor_set_fused(sparkalog_executor* ex, int enable) {
     return 0;
 }
 
+int sparkalog_executor_set_member_set(sparkalog_executor* ex, int enable) {
+    if (!ex) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null executor");
+    ex->member_enabled = enable != 0;
+    return 0;
+}
+
 int sparkalog_executor_stats(sparkalog_executor* ex, sparkalog_kernel_stats* out, int reset) {
     if (!ex || !out) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null argument");
     *out = ex->stats;
@@ -1270,6 +1356,10 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
     u32* counters = ex->counters.as<u32>();
     u32* err = counters + kErrWord;
     u64* counts = ex->counts.as<u64>();
+    // Errors of hash-set inserts, which run after a round's check: a word the
+    // per-round clearing leaves alone, read once when the run ends.
+    u32* member_err = counters + kMemberErrWord;
+    SPK_CUDA(cudaMemsetAsync(member_err, 0, 4, s), "cudaMemsetAsync");
 
     // FULL of each SCC relation must be a sorted run before the first merge;
     // duplicates inside it are removed the way the reference's first union
@@ -1309,6 +1399,7 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                 r.level_n[0] = ex->host_counts[0];
                 r.has_dups = false;
                 r.dir_valid[0] = false;
+                r.member_valid = false;
             }
         }
     }
@@ -1463,7 +1554,15 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                 u64* jn = tc + t.rules.size();
                 RelState& tr = *st->find(t.id);
                 u64 dir_launches = 0;
-                {
+                bool use_member = false;
+                if (ex->member_enabled && tr.recursive) {
+                    if (!tr.member_valid) {
+                        int rc = member_build(tr, member_err, s, &dir_launches);
+                        if (rc) return rc;
+                    }
+                    use_member = tr.member_valid;
+                }
+                if (!use_member) {
                     int rc = refresh_directories(st, tr, s, &dir_launches);
                     if (rc) return rc;
                 }
@@ -1534,7 +1633,15 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                 u64 cand_bound = 0;  // the join output bound: candidates never exceed it
                 for (size_t k : t.rules)
                     cand_bound += ex->host_rule_delta[k] * static_cast<u64>(std::max<u32>(ex->index[k].max_degree, 1));
-                if (cand_bound <= kSparseCandidates) {
+                if (use_member) {
+                    auto kernel = spk::anti_join_member_kernel<kThreads, kSetItems>;
+                    const size_t tiles = (t.j_cap + kSetTile - 1) / kSetTile;
+                    kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, std::max<size_t>(tiles, 1)),
+                             kThreads, 0, s>>>(cand, t.j_b.as<u64>(), cand_sel, jn, member_set(tr),
+                                               tr.newt.as<u64>(), tc + t.rules.size() + 1, ex->status.as<u64>(),
+                                               counters + counter_slot++, ex->epoch++, err);
+                    SPK_CUDA(cudaGetLastError(), "anti_join_member_kernel");
+                } else if (cand_bound <= kSparseCandidates) {
                     // Few candidates, far apart in every level: look each up
                     // in all levels at once.
                     auto kernel = spk::anti_join_levels_sparse_kernel<kSparseThreads, kSparseItems>;
@@ -1690,6 +1797,14 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                     tr.dir_valid[l - 1] = tr.dir_valid[l] = false;
                 }
             }
+            {
+                // FULL's hash set takes the round's new rows (or is dropped
+                // and rebuilt larger next round).
+                u64 launched = 0;
+                int rc = member_add(tr, tr.newt.as<u64>(), newt_n, member_err, s, &launched);
+                if (rc) return rc;
+                ex->stats.total_launches += launched;
+            }
             if (ex->seg_count && newt_n > 0) {
                 spk::segment_activity_kernel<<<simple_grid(newt_n), 256, 0, s>>>(
                     tr.newt.as<u64>(), newt_n, ex->seg_shift, ex->seg_count, static_cast<u32>(ex->rounds_total + 1),
@@ -1707,8 +1822,13 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
         ex->stats.rounds += 1;
         ex->rounds_total += 1;
     }
+    u32* member_err_host = reinterpret_cast<u32*>(ex->host_counts + ex->counts_words + 30);
+    SPK_CUDA(cudaMemcpyAsync(member_err_host, member_err, 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
     SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
     ex->collect();
+    if (*member_err_host)
+        return fail(SPARKALOG_E_DEVICE_FAULT, "device error bits " + std::to_string(*member_err_host) +
+                                                  " (hash set of FULL)");
     if (summary) {
         summary->iterations = iterations;
         summary->total_new_rows = total_new;

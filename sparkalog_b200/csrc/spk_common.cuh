@@ -20,6 +20,7 @@ enum : u32 {
     kErrLookbackTimeout = 1u << 0,   // a decoupled look-back spin hit its cap
     kErrCapacity = 1u << 1,          // an output did not fit its buffer
     kErrIndexRange = 1u << 2,        // a key outside the dense index range
+    kErrMemberProbe = 1u << 3,       // a hash-set probe walked every group (the set was full)
 };
 
 __device__ __forceinline__ u32 lanemask_lt() {

@@ -280,6 +280,10 @@ class RecursiveExecutor:
         """Enables (default) or disables the fused join + distinct kernel; results are identical."""
         _check(_native.load().sparkalog_executor_set_fused(self._h, 1 if enable else 0))
 
+    def set_member_set(self, enable: bool) -> None:
+        """Enables or disables (default) FULL's hash set for the anti-join; results are identical."""
+        _check(_native.load().sparkalog_executor_set_member_set(self._h, 1 if enable else 0))
+
     def stats(self, reset: bool = False) -> dict:
         """Per-kernel-class launches, milliseconds and algorithmic bytes, plus total launches."""
         s = _native.KernelStatsC()

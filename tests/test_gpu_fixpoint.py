@@ -205,7 +205,7 @@ def test_device_inputs_and_reads(cuda):
     assert np.array_equal(o1.cpu().numpy().view(np.uint32), w1)
 
 
-def _tc_with_stats(e0, e1, rule=None, oracle_rule=None):
+def _tc_with_stats(e0, e1, rule=None, oracle_rule=None, member=False):
     R = rec()
     from sparkalog_b200.relational import RecursiveSccPlan
 
@@ -214,6 +214,7 @@ def _tc_with_stats(e0, e1, rule=None, oracle_rule=None):
     store.insert_recursive(1, (e0, e1), (e0, e1))
     plan = R.transitive_closure_scc(_rid(1), _rid(0)) if rule is None else RecursiveSccPlan([_rid(1)], [rule])
     ex = R.RecursiveExecutor.compile(plan, store)
+    ex.set_member_set(member)
     ex.set_profiling(True)
     summary = ex.run(store, 10_000)
     stats = ex.stats()
@@ -308,3 +309,56 @@ def test_fused_join_distinct_through_sorted_index(cuda):
     stats = _tc_with_stats(e0, e1, rule,
                            oracle.rule_plan(1, 1, 0, left_key=1, right_key=1, projection=((0, 0), (1, 0))))
     assert stats["classes"]["join_distinct"]["launches"] > 0
+
+
+@pytest.mark.parametrize("n,e,seed", [(2000, 8000, 1), (60_000, 55_000, 8), (300_000, 262_500, 6)])
+def test_member_set_and_level_search_agree(cuda, n, e, seed):
+    # FULL's hash set and the directory search of the sorted levels give the
+    # same fixpoint (the set is rebuilt larger several times as FULL grows).
+    R = rec()
+    src, dst = generators.er_edges(n, e, seed)
+    e0, e1 = oracle.btree_pairs(src, dst)
+    out = []
+    for member in (True, False):
+        store = R.RelationStore()
+        store.insert_static(0, (e0, e1))
+        store.insert_recursive(1, (e0, e1), (e0, e1))
+        ex = R.RecursiveExecutor.compile(R.transitive_closure_scc(_rid(1), _rid(0)), store)
+        ex.set_member_set(member)
+        summary = ex.run(store, 10_000)
+        out.append((summary.iterations, summary.total_new_rows) + store.full(1))
+    assert out[0][:2] == out[1][:2]
+    assert np.array_equal(out[0][2], out[1][2]) and np.array_equal(out[0][3], out[1][3])
+
+
+def test_member_set_holds_the_all_ones_row(cuda):
+    # The row (0xffffffff, 0xffffffff) equals the hash set's empty-slot marker
+    # and is tracked apart from the slots.
+    top = 0xFFFFFFFF
+    pairs_in = [[1, top], [top, top], [top, 2], [2, 3], [3, 1]]
+    e0, e1 = oracle.btree_pairs(*cols(pairs_in))
+    _tc_with_stats(e0, e1, member=True)
+    _tc_with_stats(e0, e1, member=False)
+
+
+def test_member_set_follows_appends(cuda):
+    # A resident fixpoint continued after store.append: the appended rows go
+    # into FULL's hash set, and the closure equals a fresh run from the union.
+    R = rec()
+    src, dst = generators.er_edges(20_000, 16_000, 31)
+    e0, e1 = oracle.btree_pairs(src, dst)
+    extra0, extra1 = generators.uniform_pairs(20_000, 3_000, 32)
+    store = R.RelationStore()
+    store.insert_static(0, (e0, e1))
+    store.insert_recursive(1, (e0, e1), (e0, e1))
+    ex = R.RecursiveExecutor.compile(R.transitive_closure_scc(_rid(1), _rid(0)), store)
+    ex.set_member_set(True)
+    ex.run(store, 10_000)
+    store.append(1, (extra0, extra1))
+    ex.run(store, 10_000)
+    s0, s1 = oracle.btree_pairs(np.concatenate([e0, extra0]), np.concatenate([e1, extra1]))
+    st = oracle.Store()
+    st.insert_static(0, (e0, e1))
+    st.insert_recursive(1, (s0, s1), (s0, s1))
+    st.run_scc([1], [oracle.tc_rule(1, 0)])
+    assert pairs(store.full(1)) == pairs(st.full(1))
