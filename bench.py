@@ -54,6 +54,56 @@ WORKLOADS = {
 CPU_SAMPLE_ROUNDS = {"er_16m_14_68m": 4, "er_2000_8000": 13}
 
 
+# DRAM traffic measured by ncu for one fixpoint of a smaller graph of the same
+# family (a summary table: kernel, launches, total ms, read GB, write GB, ...);
+# scaled to this run by derived tuples.
+TRAFFIC_PROFILE = ROOT / "profiles" / "traffic_tc_er4m.txt"
+CLASS_KERNELS = {
+    "anti_join": ("anti_join_levels_kernel", "anti_join_levels_sparse_kernel", "anti_join_member_kernel"),
+    "join_distinct": ("fused_join_distinct_kernel",),
+    "merge": ("merge_disjoint_kernel", "merge_partition_kernel"),
+}
+
+
+def profiled_traffic(kernel_class, new_rows):
+    """Per-launch DRAM bytes of a kernel class from the ncu summary, scaled by
+    derived tuples to this run; (None, reason) when there is no summary."""
+    import re
+
+    if not TRAFFIC_PROFILE.exists() or kernel_class not in CLASS_KERNELS:
+        return None, "no ncu traffic summary for this kernel class"
+    text = TRAFFIC_PROFILE.read_text()
+    m = re.search(r"derived tuples: (\d+)", text)
+    if not m:
+        return None, "ncu traffic summary without a derived-tuple count"
+    launches, nbytes = 0, 0.0
+    for line in text.splitlines():
+        cells = [c.strip() for c in line.strip().strip("|").split("|")]
+        if len(cells) < 5 or not cells[0].startswith("`"):
+            continue
+        name = cells[0].strip("`").split("<")[0]
+        if name in CLASS_KERNELS[kernel_class]:
+            launches += int(cells[1])
+            nbytes += (float(cells[3]) + float(cells[4])) * 1e9
+    if launches == 0:
+        return None, "kernel class absent from the ncu traffic summary"
+    scale = new_rows / int(m.group(1))
+    return nbytes / launches * scale, (f"{TRAFFIC_PROFILE.relative_to(ROOT)}: {launches} launches, "
+                                       f"scaled x{scale:.2f} by derived tuples")
+
+
+def pipeline_bytes(trace):
+    """Algorithmic bytes of the reference's operator pipeline over the run's
+    rounds, pairs as 8 B: join 16D + 12J, distinct 8J + 8U, anti-join in merge
+    form 8(U + FULL) + 8N, union 8(FULL + N) + 8 FULL'."""
+    total = 0
+    for r in trace:
+        d, j, u, n, after = r["delta_rows"], r["join_rows"], r["unique_rows"], r["new_rows"], r["full_rows"]
+        before = after - n
+        total += 16 * d + 12 * j + 8 * j + 8 * u + 8 * (u + before) + 8 * n + 8 * (before + n) + 8 * after
+    return total
+
+
 def parse_args():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -228,6 +278,7 @@ def run_ours(args):
             ex.set_profiling(True)
         summary = ex.run(store)
         stats = ex.stats()
+        stats["trace"] = ex.trace() if profile else []
         ex.close()
         store.close()
         return summary, stats
@@ -276,6 +327,12 @@ def run_ours(args):
     per_launch_ms = dom["ms"] / max(dom["launches"], 1)
     per_launch_bytes = dom["bytes"] / max(dom["launches"], 1)
     achieved = per_launch_bytes / (per_launch_ms / 1e3) / 1e9 if per_launch_ms > 0 else 0.0
+    traffic, traffic_source = profiled_traffic(dominant, float(new_rows) / max(world, 1))
+    pipe = float(pipeline_bytes(pstats["trace"]))
+    if dist is not None:
+        t = torch.tensor([pipe], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        pipe = float(t[0])
 
     # End to end through the public API: pinned host buffers, H2D + run + D2H.
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
@@ -339,12 +396,19 @@ def run_ours(args):
             "e2e": {"value": e2e_value, "unit": "tuples/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": e2e_local},
             "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved / 1.0, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "traffic_source": traffic_source,
                          "peak_kind": peak_kind,
                          "per_launch_ms": per_launch_ms, "per_launch_algorithmic_bytes": per_launch_bytes,
                          "classes": {k: {"ms": v["ms"], "launches": v["launches"],
                                          "gbs": (v["bytes"] / (v["ms"] / 1e3) / 1e9) if v["ms"] > 0 else 0.0}
                                      for k, v in classes.items()}},
+            "pipeline": {"algorithmic_bytes": pipe,
+                         "achieved_gbs": pipe / (ms / args.steps / 1e3) / 1e9,
+                         "frac": pipe / (ms / args.steps / 1e3) / 1e9 / peak,
+                         "what": "bytes the reference's per-round operators would move (join 16D+12J, distinct "
+                                 "8J+8U, anti-join 8(U+FULL)+8N, union 8(FULL+N)+8FULL'), from the round trace, "
+                                 "over the measured step time"},
             "gpu_launches": launches,
             "clocks": clock,
         }

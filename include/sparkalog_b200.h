@@ -304,6 +304,24 @@ SPARKALOG_API int sparkalog_executor_set_fused(sparkalog_executor* executor, int
 SPARKALOG_API int sparkalog_executor_set_member_set(sparkalog_executor* executor, int enable);
 SPARKALOG_API int sparkalog_executor_stats(sparkalog_executor* executor, sparkalog_kernel_stats* out, int reset);
 
+/* Per-round trace of an executor (the operator cardinalities of each round,
+ * summed over the SCC's targets): the figures the reference's benchmark CSVs
+ * report per operator. No counterpart in the reference's ABI. */
+typedef struct sparkalog_round_trace {
+    uint64_t round;        /* 1-based round number within the executor's lifetime */
+    uint64_t delta_rows;   /* DELTA rows joined, over all rules */
+    uint64_t join_rows;    /* BinaryEqualityJoin output rows */
+    uint64_t unique_rows;  /* BinaryDistinct output rows (distinct join rows) */
+    uint64_t new_rows;     /* SortedBinaryAntiJoin output rows (NEWT) */
+    uint64_t full_rows;    /* FULL rows after the round (SortedBinaryUnion output) */
+} sparkalog_round_trace;
+
+/* Copies up to `capacity` recorded rounds (oldest first) to `out` (which may
+ * be null when capacity is 0) and sets *count to the number recorded; with
+ * reset != 0 the record is cleared afterwards. */
+SPARKALOG_API int sparkalog_executor_trace(sparkalog_executor* executor, sparkalog_round_trace* out,
+                                           size_t capacity, size_t* count, int reset);
+
 /* Grows the current device's stream-ordered memory pool to at least `bytes`
  * and keeps it (relations are allocated from it), so a long-running process
  * does not pay for pool growth inside its first large requests. */

@@ -53,6 +53,7 @@ TIER_B = [
     "sparkalog_executor_set_fused",
     "sparkalog_executor_set_member_set",
     "sparkalog_executor_stats",
+    "sparkalog_executor_trace",
     "sparkalog_reserve_device_memory",
     "sparkalog_last_error",
 ]
@@ -103,6 +104,13 @@ class KernelStatsC(ctypes.Structure):
         ("total_launches", ctypes.c_uint64),
         ("rounds", ctypes.c_uint64),
     ]
+
+
+class RoundTraceC(ctypes.Structure):
+    """sparkalog_round_trace."""
+
+    _fields_ = [(name, ctypes.c_uint64) for name in
+                ("round", "delta_rows", "join_rows", "unique_rows", "new_rows", "full_rows")]
 
 
 _lib = None
@@ -183,6 +191,8 @@ def load() -> ctypes.CDLL:
     L.sparkalog_executor_set_member_set.restype = i
     L.sparkalog_executor_stats.argtypes = [vp, ctypes.POINTER(KernelStatsC), i]
     L.sparkalog_executor_stats.restype = i
+    L.sparkalog_executor_trace.argtypes = [vp, ctypes.POINTER(RoundTraceC), ctypes.c_size_t, c_sizep, i]
+    L.sparkalog_executor_trace.restype = i
     L.sparkalog_reserve_device_memory.argtypes = [ctypes.c_size_t, vp]
     L.sparkalog_reserve_device_memory.restype = i
     L.sparkalog_last_error.argtypes = []

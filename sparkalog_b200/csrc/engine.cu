@@ -384,6 +384,7 @@ struct TargetRT {
     SortScratch sort;
     u32 fused_rows = 896;  // nominal DELTA rows per fused tile (halved when tiles overflow)
     bool force_generic = false;  // redo the current round with the general kernels
+    bool fused_last = false;     // the round just applied ran the fused kernel
 };
 
 }  // namespace
@@ -421,6 +422,7 @@ struct sparkalog_executor {
     bool profiling = false;
     bool fused_enabled = true;
     bool member_enabled = false;  // anti-join through FULL's hash set (opt-in)
+    std::vector<sparkalog_round_trace> trace;  // per-round operator cardinalities
     std::vector<cudaEvent_t> free_events;
     std::vector<Timing> timings;
     sparkalog_kernel_stats stats{};
@@ -507,9 +509,9 @@ constexpr size_t kCounterWords = 1024;  // per-round tile counters
 constexpr size_t kErrWord = kCounterWords;
 
 size_t target_count_base(const sparkalog_executor* ex, size_t t) {
-    // Layout per target: [rules + 1 join counts][newt count]
+    // Layout per target: [rules + 1 join counts][newt count][distinct join rows]
     size_t base = 0;
-    for (size_t i = 0; i < t; ++i) base += ex->targets[i].rules.size() + 2;
+    for (size_t i = 0; i < t; ++i) base += ex->targets[i].rules.size() + 3;
     return base;
 }
 
@@ -518,6 +520,7 @@ constexpr int kFusedCap = 1920;     // join output rows per fused tile (shared m
 constexpr int kFusedRowCap = 1024;  // DELTA rows per fused tile
 constexpr size_t kFusedFlagBase = 8;      // fallback flags live at err + 8 + target
 constexpr size_t kFusedMaxTargets = 48;
+constexpr size_t kMaxTraceRounds = 1u << 20;
 constexpr size_t kMemberErrWord = kCounterWords + kFusedFlagBase + kFusedMaxTargets + 4;
 
 // The fused round applies to a target with one rule whose join output starts
@@ -648,7 +651,8 @@ int sorted_difference(sparkalog_store* st, u64 n, RelState& right, DevArray& out
     const size_t tiles = (n + kSetTile - 1) / kSetTile;
     kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, tiles), kThreads, 0, s>>>(
         ops.a.as<u64>(), ops.b.as<u64>(), &ops.ex.index_sort.plan.as<spk::RadixPlan>()->final_sel, nptr, lv,
-        out.as<u64>(), ops.counts.as<u64>(), ops.status.as<u64>(), ops.counters.as<u32>(), ops.ex.epoch++, err);
+        out.as<u64>(), ops.counts.as<u64>(), ops.status.as<u64>(), ops.counters.as<u32>(), ops.ex.epoch++, err,
+        nullptr);
     SPK_CUDA(cudaGetLastError(), "anti_join_levels_kernel");
     SPK_CUDA(cudaMemcpyAsync(ops.host, ops.counts.ptr, 8, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
     SPK_CUDA(cudaMemcpyAsync(ops.host + 1, err, 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
@@ -1226,7 +1230,7 @@ int sparkalog_executor_compile(sparkalog_store* st, const u32* relations, size_t
     }
     ex->index.resize(rule_count);
     ex->counts_words = 0;
-    for (auto& t : ex->targets) ex->counts_words += t.rules.size() + 2;
+    for (auto& t : ex->targets) ex->counts_words += t.rules.size() + 3;
     cudaStream_t s = st->stream;
     cudaError_t e = ex->counts.ensure(ex->counts_words * 8, s);
     if (e == cudaSuccess) e = ex->counters.ensure((kCounterWords + 64) * 4, s);
@@ -1319,6 +1323,16 @@ int sparkalog_executor_set_fused(sparkalog_executor* ex, int enable) {
     return 0;
 }
 
+int sparkalog_executor_trace(sparkalog_executor* ex, sparkalog_round_trace* out, size_t capacity, size_t* count,
+                             int reset) {
+    if (!ex || !count || (capacity && !out)) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null argument");
+    *count = ex->trace.size();
+    const size_t n = std::min(capacity, ex->trace.size());
+    for (size_t i = 0; i < n; ++i) out[i] = ex->trace[i];
+    if (reset) ex->trace.clear();
+    return 0;
+}
+
 int sparkalog_executor_set_member_set(sparkalog_executor* ex, int enable) {
     if (!ex) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null executor");
     ex->member_enabled = enable != 0;
@@ -1390,7 +1404,7 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                 const size_t tiles = (n + kSetTile - 1) / kSetTile;
                 kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, tiles), kThreads, 0, s>>>(
                     r.level[0].as<u64>(), r.level[0].as<u64>(), nullptr, nptr, none, r.spare.as<u64>(), counts,
-                    ex->status.as<u64>(), counters, ex->epoch++, err);
+                    ex->status.as<u64>(), counters, ex->epoch++, err, nullptr);
                 SPK_CUDA(cudaGetLastError(), "anti_join_levels_kernel");
                 ex->stats.total_launches += 1;
                 SPK_CUDA(cudaMemcpyAsync(ex->host_counts, counts, 8, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
@@ -1633,13 +1647,15 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                 u64 cand_bound = 0;  // the join output bound: candidates never exceed it
                 for (size_t k : t.rules)
                     cand_bound += ex->host_rule_delta[k] * static_cast<u64>(std::max<u32>(ex->index[k].max_degree, 1));
+                // Distinct join rows of the target (round trace).
+                unsigned long long* unique_word = reinterpret_cast<unsigned long long*>(tc + t.rules.size() + 2);
                 if (use_member) {
                     auto kernel = spk::anti_join_member_kernel<kThreads, kSetItems>;
                     const size_t tiles = (t.j_cap + kSetTile - 1) / kSetTile;
                     kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, std::max<size_t>(tiles, 1)),
                              kThreads, 0, s>>>(cand, t.j_b.as<u64>(), cand_sel, jn, member_set(tr),
                                                tr.newt.as<u64>(), tc + t.rules.size() + 1, ex->status.as<u64>(),
-                                               counters + counter_slot++, ex->epoch++, err);
+                                               counters + counter_slot++, ex->epoch++, err, unique_word);
                     SPK_CUDA(cudaGetLastError(), "anti_join_member_kernel");
                 } else if (cand_bound <= kSparseCandidates) {
                     // Few candidates, far apart in every level: look each up
@@ -1649,7 +1665,7 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                     kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kSparseThreads, std::max<size_t>(tiles, 1)),
                              kSparseThreads, 0, s>>>(cand, t.j_b.as<u64>(), cand_sel, jn, lv, tr.newt.as<u64>(),
                                                      tc + t.rules.size() + 1, ex->status.as<u64>(),
-                                                     counters + counter_slot++, ex->epoch++, err);
+                                                     counters + counter_slot++, ex->epoch++, err, unique_word);
                     SPK_CUDA(cudaGetLastError(), "anti_join_levels_sparse_kernel");
                 } else {
                     auto kernel = spk::anti_join_levels_kernel<kThreads, kSetItems, kLevelStage>;
@@ -1657,7 +1673,7 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                     kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, std::max<size_t>(tiles, 1)),
                              kThreads, 0, s>>>(cand, t.j_b.as<u64>(), cand_sel, jn, lv, tr.newt.as<u64>(),
                                                tc + t.rules.size() + 1, ex->status.as<u64>(), counters + counter_slot++,
-                                               ex->epoch++, err);
+                                               ex->epoch++, err, unique_word);
                     SPK_CUDA(cudaGetLastError(), "anti_join_levels_kernel");
                 }
                 ex->end(anti_t[ti], s, 0.0, 1);
@@ -1721,6 +1737,7 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                 SPK_CUDA(cudaMemsetAsync(err, 0, 4, s), "cudaMemsetAsync");
                 continue;
             }
+            for (size_t ti = 0; ti < ex->targets.size(); ++ti) ex->targets[ti].fused_last = fused[ti] != 0;
             if (!(bits & spk::kErrCapacity)) break;
             // A candidate buffer overflowed: grow it and redo the round (no
             // relation state has changed yet).
@@ -1821,6 +1838,22 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
         iterations += 1;
         ex->stats.rounds += 1;
         ex->rounds_total += 1;
+        {
+            sparkalog_round_trace rec{};
+            rec.round = ex->rounds_total;
+            for (size_t ti = 0; ti < ex->targets.size(); ++ti) {
+                const TargetRT& t = ex->targets[ti];
+                const u64* c = ex->host_counts + target_count_base(ex, ti);
+                for (size_t k : t.rules) rec.delta_rows += ex->host_rule_delta[k];
+                // A fused target counts its join rows in the first word; the
+                // general join chains its per-rule counts up to word rules.
+                rec.join_rows += t.fused_last ? c[0] : c[t.rules.size()];
+                rec.new_rows += c[t.rules.size() + 1];
+                rec.unique_rows += c[t.rules.size() + 2];
+                rec.full_rows += st->find(t.id)->full_rows();
+            }
+            if (ex->trace.size() < kMaxTraceRounds) ex->trace.push_back(rec);
+        }
     }
     u32* member_err_host = reinterpret_cast<u32*>(ex->host_counts + ex->counts_words + 30);
     SPK_CUDA(cudaMemcpyAsync(member_err_host, member_err, 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");

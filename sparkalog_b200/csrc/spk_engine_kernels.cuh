@@ -73,6 +73,14 @@ static __global__ void level_directory_kernel(const u64* keys, u64 n, u32 shift,
 // decoupled look-back, so NEWT stays sorted.
 constexpr u64 kStreamChunks = 2;
 
+// Adds the rows a warp keeps after the unique step (BinaryDistinct's output
+// size) to *unique_count, when given. Called by every thread.
+__device__ __forceinline__ void count_unique(u32 keep, unsigned long long* unique_count) {
+    if (!unique_count) return;
+    const u32 c = __reduce_add_sync(0xffffffffu, static_cast<u32>(__popc(keep)));
+    if (lane_id() == 0 && c) atomicAdd(unique_count, static_cast<unsigned long long>(c));
+}
+
 // Directory bounds of a tile's keys [first, last] in every level: the rows of
 // first's bucket through last's bucket (threads 0 .. 2 * levels.n - 1).
 __device__ __forceinline__ void level_slices(const Levels& levels, u64 first, u64 last, u64* range_lo, u64* range_hi) {
@@ -94,7 +102,7 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_kernel(const u64* bu
                                                                    const u32* final_sel, const u64* n_ptr,
                                                                    Levels levels, u64* out, u64* out_count,
                                                                    u64* status, u32* tile_counter, u32 epoch,
-                                                                   u32* err) {
+                                                                   u32* err, unsigned long long* unique_count) {
     constexpr int kTile = THREADS * ITEMS;
     static_assert(STAGE >= kTile, "the output stage reuses the level stage");
     __shared__ CompactShared<THREADS> cs;
@@ -130,6 +138,7 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_kernel(const u64* bu
                 prev = k;
             }
         }
+        count_unique(keep, unique_count);
         __syncthreads();
         for (int l = 0; l < levels.n; ++l) {
             const u64 lo = range_lo[l];
@@ -231,7 +240,7 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_sparse_kernel(const 
                                                                           const u32* final_sel, const u64* n_ptr,
                                                                           Levels levels, u64* out, u64* out_count,
                                                                           u64* status, u32* tile_counter, u32 epoch,
-                                                                          u32* err) {
+                                                                          u32* err, unsigned long long* unique_count) {
     constexpr int kTile = THREADS * ITEMS;
     __shared__ CompactShared<THREADS> cs;
     __shared__ u64 stage[kTile];
@@ -262,6 +271,7 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_sparse_kernel(const 
                 prev = k;
             }
         }
+        count_unique(keep, unique_count);
         u64 pos[kMaxLevels][ITEMS];
         u32 span[kMaxLevels][ITEMS], bucket[kMaxLevels][ITEMS];
         u32 max_span = 0;

@@ -20,6 +20,7 @@
 #pragma once
 
 #include "spk_common.cuh"
+#include "spk_engine_kernels.cuh"
 #include "spk_setops.cuh"
 
 namespace spk {
@@ -104,7 +105,7 @@ __global__ void __launch_bounds__(THREADS) anti_join_member_kernel(const u64* bu
                                                                    const u32* final_sel, const u64* n_ptr,
                                                                    MemberSet set, u64* out, u64* out_count,
                                                                    u64* status, u32* tile_counter, u32 epoch,
-                                                                   u32* err) {
+                                                                   u32* err, unsigned long long* unique_count) {
     constexpr int kTile = THREADS * ITEMS;
     __shared__ CompactShared<THREADS> cs;
     __shared__ u64 stage[kTile];
@@ -136,6 +137,7 @@ __global__ void __launch_bounds__(THREADS) anti_join_member_kernel(const u64* bu
                 prev = k;
             }
         }
+        count_unique(keep, unique_count);
         ulonglong2 lo[ITEMS], hi[ITEMS];
         u64 group[ITEMS];
 #pragma unroll

@@ -280,6 +280,15 @@ class RecursiveExecutor:
         """Enables (default) or disables the fused join + distinct kernel; results are identical."""
         _check(_native.load().sparkalog_executor_set_fused(self._h, 1 if enable else 0))
 
+    def trace(self, reset: bool = False) -> list[dict]:
+        """Per-round operator cardinalities (delta, join, unique, new and FULL rows)."""
+        L = _native.load()
+        n = ctypes.c_size_t(0)
+        _check(L.sparkalog_executor_trace(self._h, None, 0, ctypes.byref(n), 0))
+        buf = (_native.RoundTraceC * max(n.value, 1))()
+        _check(L.sparkalog_executor_trace(self._h, buf, n.value, ctypes.byref(n), 1 if reset else 0))
+        return [{f: int(getattr(buf[i], f)) for f, _ in _native.RoundTraceC._fields_} for i in range(n.value)]
+
     def set_member_set(self, enable: bool) -> None:
         """Enables or disables (default) FULL's hash set for the anti-join; results are identical."""
         _check(_native.load().sparkalog_executor_set_member_set(self._h, 1 if enable else 0))

@@ -362,3 +362,36 @@ def test_member_set_follows_appends(cuda):
     st.insert_recursive(1, (s0, s1), (s0, s1))
     st.run_scc([1], [oracle.tc_rule(1, 0)])
     assert pairs(store.full(1)) == pairs(st.full(1))
+
+
+@pytest.mark.parametrize("fused", [True, False])
+def test_round_trace_cardinalities(cuda, fused):
+    # Per-round operator cardinalities against a plain semi-naive loop in
+    # Python: |DELTA|, |join|, |distinct|, |NEWT| and |FULL| after the round.
+    R = rec()
+    src, dst = generators.er_edges(1500, 1900, 41)
+    e0, e1 = oracle.btree_pairs(src, dst)
+    adj = {}
+    for a, b in zip(e0.tolist(), e1.tolist()):
+        adj.setdefault(a, []).append(b)
+    full = set(zip(e0.tolist(), e1.tolist()))
+    delta = sorted(full)
+    expect = []
+    while delta:
+        joined = [(x, z) for x, y in delta for z in adj.get(y, ())]
+        unique = set(joined)
+        new = unique - full
+        full |= new
+        expect.append((len(delta), len(joined), len(unique), len(new), len(full)))
+        delta = sorted(new)
+    store = R.RelationStore()
+    store.insert_static(0, (e0, e1))
+    store.insert_recursive(1, (e0, e1), (e0, e1))
+    ex = R.RecursiveExecutor.compile(R.transitive_closure_scc(_rid(1), _rid(0)), store)
+    ex.set_fused(fused)
+    summary = ex.run(store, 10_000)
+    got = [(r["delta_rows"], r["join_rows"], r["unique_rows"], r["new_rows"], r["full_rows"]) for r in ex.trace()]
+    assert summary.iterations == len(expect)
+    assert got == expect
+    assert [r["round"] for r in ex.trace(reset=True)] == list(range(1, len(expect) + 1))
+    assert ex.trace() == []
