@@ -88,6 +88,23 @@ SPARKALOG_API int sparkalog_anti_join_u32(const uint32_t* left_first, const uint
                                           uint32_t* selected_rows, uint32_t* output_first, uint32_t* output_second,
                                           void* temporary, size_t temporary_bytes, void* stream);
 
+/* Filter: output[] = ascending row ids i with compare(input[i], operation,
+ * operand), flags[i] = 1 / 0, *count = u32 number of ids. Operation codes:
+ * 0 ==, 1 !=, 2 <, 3 <=, 4 >, 5 >=, anything else matches no row.
+ * column_ops.cu:252-318; lib.rs:33-52. */
+SPARKALOG_API int sparkalog_filter_u32_temporary_bytes(const uint32_t* flags, uint32_t* output, uint32_t* count,
+                                                       size_t len, size_t* temporary_bytes, void* stream);
+SPARKALOG_API int sparkalog_filter_u32(const uint32_t* input, size_t len, uint32_t operation, uint32_t operand,
+                                       uint32_t* flags, uint32_t* output, uint32_t* count, void* temporary,
+                                       size_t temporary_bytes, void* stream);
+
+/* output[i] = i % modulus. column_ops.cu:320-336; lib.rs:53-58. */
+SPARKALOG_API int sparkalog_fill_mod_u32(uint32_t* output, size_t len, uint32_t modulus, void* stream);
+
+/* data[i] += 1 (the reference's workspace smoke test). column_ops.cu:231-246;
+ * lib.rs:31. */
+SPARKALOG_API int sparkalog_add_one_i32(int32_t* data, size_t len, void* stream);
+
 /* column_ops.cu:643-690; lib.rs:140-150. */
 SPARKALOG_API int sparkalog_union_u32_temporary_bytes(const uint64_t* left, size_t left_rows, const uint64_t* right,
                                                       size_t right_rows, uint64_t* merged, uint64_t* unique,

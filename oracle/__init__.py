@@ -495,3 +495,39 @@ def reference_cuda() -> ctypes.CDLL | None:
     if not REF_CUDA_PATH.exists():
         return None
     return ctypes.CDLL(str(REF_CUDA_PATH))
+
+
+# ---------------------------------------------------------------------------
+# Filter (crates/sparkalog-execution/src/lib.rs:1681-1760): ascending row ids
+# whose value satisfies the predicate; operation codes 0 ==, 1 !=, 2 <, 3 <=,
+# 4 >, 5 >= (crates/sparkalog-relational/src/lib.rs:144-164).
+# ---------------------------------------------------------------------------
+def _filter_matches(value: int, op: int, operand: int) -> bool:
+    return {0: value == operand, 1: value != operand, 2: value < operand, 3: value <= operand,
+            4: value > operand, 5: value >= operand}.get(op, False)
+
+
+def filter_serial(values, op: int, operand: int) -> np.ndarray:
+    """filter_cpu_serial (lib.rs:1681-1702): one pass, row ids in order."""
+    return np.array([row for row, v in enumerate(np.asarray(values).tolist()) if _filter_matches(v, op, operand)],
+                    dtype=np.uint32)
+
+
+def filter_parallel(values, op: int, operand: int, workers: int = 8) -> np.ndarray:
+    """filter_cpu_parallel (lib.rs:1705-1760): per-chunk flags, an exclusive scan
+    of the chunk counts, ids written at the chunk offsets."""
+    v = np.asarray(values, dtype=np.uint32)
+    n = len(v)
+    if n == 0:
+        return np.zeros(0, dtype=np.uint32)
+    chunk = -(-n // min(workers, n))
+    cmp = {0: np.equal, 1: np.not_equal, 2: np.less, 3: np.less_equal, 4: np.greater, 5: np.greater_equal}
+    flags = [cmp[op](v[i:i + chunk], np.uint32(operand)) if op in cmp else np.zeros(len(v[i:i + chunk]), bool)
+             for i in range(0, n, chunk)]
+    counts = [int(f.sum()) for f in flags]
+    out = np.zeros(sum(counts), dtype=np.uint32)
+    off = 0
+    for c, (i, f) in enumerate(zip(range(0, n, chunk), flags)):
+        out[off:off + counts[c]] = np.nonzero(f)[0].astype(np.uint32) + np.uint32(i)
+        off += counts[c]
+    return out

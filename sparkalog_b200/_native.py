@@ -27,6 +27,10 @@ TIER_A = [
     "sparkalog_distinct_u32",
     "sparkalog_anti_join_u32_temporary_bytes",
     "sparkalog_anti_join_u32",
+    "sparkalog_filter_u32_temporary_bytes",
+    "sparkalog_filter_u32",
+    "sparkalog_fill_mod_u32",
+    "sparkalog_add_one_i32",
     "sparkalog_union_u32_temporary_bytes",
     "sparkalog_union_u32",
     "sparkalog_anti_join_u32_no_alloc",
@@ -138,6 +142,11 @@ def load() -> ctypes.CDLL:
     L.sparkalog_anti_join_u32_temporary_bytes.argtypes = [vp, vp, vp, ctypes.c_size_t, c_sizep, vp]
     L.sparkalog_anti_join_u32.argtypes = [vp, vp, ctypes.c_size_t, vp, vp, ctypes.c_size_t, vp, vp, vp, vp, vp, vp,
                                           ctypes.c_size_t, vp]
+    L.sparkalog_filter_u32_temporary_bytes.argtypes = [vp, vp, vp, ctypes.c_size_t, c_sizep, vp]
+    L.sparkalog_filter_u32.argtypes = [vp, ctypes.c_size_t, ctypes.c_uint32, ctypes.c_uint32, vp, vp, vp, vp,
+                                       ctypes.c_size_t, vp]
+    L.sparkalog_fill_mod_u32.argtypes = [vp, ctypes.c_size_t, ctypes.c_uint32, vp]
+    L.sparkalog_add_one_i32.argtypes = [vp, ctypes.c_size_t, vp]
     L.sparkalog_union_u32_temporary_bytes.argtypes = [vp, ctypes.c_size_t, vp, ctypes.c_size_t, vp, vp, vp, c_sizep,
                                                       vp]
     L.sparkalog_union_u32.argtypes = [vp, vp, ctypes.c_size_t, vp, vp, ctypes.c_size_t, vp, vp, vp, vp, vp, vp, vp,

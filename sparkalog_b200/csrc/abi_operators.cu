@@ -20,6 +20,7 @@
 #include "spk_radix.cuh"
 #include "spk_setops.cuh"
 
+#include <algorithm>
 #include <mutex>
 #include <vector>
 
@@ -344,6 +345,57 @@ int sparkalog_anti_join_u32(const u32* left_first, const u32* left_second, size_
     kernel<<<grid, kThreads, 0, s>>>(left_first, left_second, left_rows, right_first, right_second, right_rows, flags,
                                      selected, selected_rows, output_first, output_second, t.status, t.counter, 1u,
                                      err);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Filter, fill and add-one. column_ops.cu:231-246, 252-336.
+// ---------------------------------------------------------------------------
+
+int sparkalog_filter_u32_temporary_bytes(const u32* flags, u32* output, u32* count, size_t len,
+                                         size_t* temporary_bytes, void* stream) {
+    (void)stream;
+    if (temporary_bytes == nullptr || count == nullptr) return cudaErrorInvalidValue;
+    if (len != 0 && (flags == nullptr || output == nullptr)) return cudaErrorInvalidValue;
+    *temporary_bytes = set_temp(nullptr, len).bytes;
+    return cudaSuccess;
+}
+
+int sparkalog_filter_u32(const u32* input, size_t len, u32 operation, u32 operand, u32* flags, u32* output,
+                         u32* count, void* temporary, size_t temporary_bytes, void* stream) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (count == nullptr) return cudaErrorInvalidValue;
+    if (len == 0) return cudaMemsetAsync(count, 0, sizeof(*count), s);
+    if (input == nullptr || flags == nullptr || output == nullptr || temporary == nullptr)
+        return cudaErrorInvalidValue;
+    SetTemp t = set_temp(temporary, len);
+    if (temporary_bytes < t.bytes) return cudaErrorInvalidValue;
+    u32* err = device_error_word();
+    if (!err) return cudaErrorMemoryAllocation;
+    cudaError_t st = cudaMemsetAsync(temporary, 0, t.bytes, s);
+    if (st != cudaSuccess) return st;
+    auto kernel = spk::filter_select_kernel<kThreads, kSetItems>;
+    const size_t tiles = (len + kSetTile - 1) / kSetTile;
+    const unsigned grid = spk::persistent_grid(reinterpret_cast<const void*>(kernel), kThreads, 0, tiles);
+    kernel<<<grid, kThreads, 0, s>>>(input, len, operation, operand, flags, output, count, t.status, t.counter, 1u,
+                                     err);
+    return cudaGetLastError();
+}
+
+int sparkalog_fill_mod_u32(u32* output, size_t len, u32 modulus, void* stream) {
+    if (modulus == 0 || (output == nullptr && len != 0)) return cudaErrorInvalidValue;
+    if (len == 0) return cudaSuccess;
+    const size_t blocks = std::min<size_t>((len + 255) / 256, static_cast<size_t>(spk::device_sm_count()) * 8);
+    spk::fill_mod_kernel<<<static_cast<unsigned>(blocks), 256, 0, static_cast<cudaStream_t>(stream)>>>(output, len,
+                                                                                                        modulus);
+    return cudaGetLastError();
+}
+
+int sparkalog_add_one_i32(int32_t* data, size_t len, void* stream) {
+    if (data == nullptr && len != 0) return cudaErrorInvalidValue;
+    if (len == 0) return cudaSuccess;
+    const size_t blocks = std::min<size_t>((len + 255) / 256, static_cast<size_t>(spk::device_sm_count()) * 8);
+    spk::add_one_kernel<<<static_cast<unsigned>(blocks), 256, 0, static_cast<cudaStream_t>(stream)>>>(data, len);
     return cudaGetLastError();
 }
 

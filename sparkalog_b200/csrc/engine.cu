@@ -68,6 +68,7 @@ constexpr int kSetTile = kThreads * kSetItems;
 constexpr int kJoinItems = 8;
 constexpr int kJoinTile = kThreads * kJoinItems;
 constexpr u64 kMaxRelationRows = 0xffffffffull;  // row ids are u32
+constexpr size_t kCounterWords = 1024;  // per-round tile counters
 constexpr int kLevelStage = 2048;  // level rows per shared-memory chunk of the anti-join (two buffers)
 constexpr int kSparseThreads = 128;  // anti-join of small candidate sets
 constexpr int kSparseItems = 4;
@@ -201,7 +202,7 @@ unsigned simple_grid(size_t n) {
 // a parallel diagonal-split pre-pass, then the merge. Returns the number of
 // kernels launched through *launches.
 cudaError_t launch_merge(const u64* a, u64 na, const u64* b, u64 nb, u64* out, DevArray& splits, cudaStream_t s,
-                         u64* launches = nullptr) {
+                         u64* launches = nullptr, spk::MergeDirectory md = spk::MergeDirectory{nullptr, 0, 0}) {
     const u64 total = na + nb;
     if (launches) *launches = 0;
     if (total == 0) return cudaSuccess;
@@ -215,7 +216,7 @@ cudaError_t launch_merge(const u64* a, u64 na, const u64* b, u64 nb, u64* out, D
     if (st != cudaSuccess) return st;
     auto kernel = spk::merge_disjoint_kernel<kThreads, kMergeItems>;
     kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, tiles), kThreads, 0, s>>>(
-        a, na, b, nb, splits.as<u64>(), out);
+        a, na, b, nb, splits.as<u64>(), out, md);
     if (launches) *launches = 2;
     return cudaGetLastError();
 }
@@ -271,15 +272,20 @@ int pack_columns(sparkalog_store* st, const u32* c0, const u32* c1, size_t rows,
 // Rebuilds the bucket directory of every non-empty level whose rows changed.
 // The bucket width comes from the store's largest value, which bounds every
 // key: ~64 rows per bucket.
-int refresh_directories(sparkalog_store* st, RelState& r, cudaStream_t s, u64* launches) {
+void directory_shape(const sparkalog_store* st, u64 rows, u32* shift, u64* buckets) {
     const u64 key_max = (static_cast<u64>(st->max_value) << 32) | st->max_value;
-    int key_bits = 64 - __builtin_clzll(key_max | 1);
+    const int key_bits = 64 - __builtin_clzll(key_max | 1);
+    const int target_bits = 64 - __builtin_clzll(std::max<u64>(rows / 64, 1));
+    *shift = static_cast<u32>(std::max(0, key_bits - target_bits));
+    *buckets = (key_max >> *shift) + 1;
+}
+
+int refresh_directories(sparkalog_store* st, RelState& r, cudaStream_t s, u64* launches) {
     for (int l = 0; l < spk::kMaxLevels; ++l) {
         if (r.level_n[l] == 0 || r.dir_valid[l]) continue;
-        const u64 target = std::max<u64>(r.level_n[l] / 64, 1);
-        const int target_bits = 64 - __builtin_clzll(target);
-        const u32 shift = static_cast<u32>(std::max(0, key_bits - target_bits));
-        const u64 buckets = (key_max >> shift) + 1;
+        u32 shift;
+        u64 buckets;
+        directory_shape(st, r.level_n[l], &shift, &buckets);
         SPK_CUDA(r.dir[l].ensure((buckets + 1) * 4, s), "cudaMallocAsync");
         spk::level_directory_kernel<<<simple_grid(buckets + 1), 256, 0, s>>>(r.level[l].as<u64>(), r.level_n[l], shift,
                                                                             buckets, r.dir[l].as<u32>());
@@ -289,6 +295,29 @@ int refresh_directories(sparkalog_store* st, RelState& r, cudaStream_t s, u64* l
         r.dir_valid[l] = true;
         if (launches) *launches += 1;
     }
+    return 0;
+}
+
+// Merges two disjoint sorted runs into level l of r (through r.spare) and
+// writes the merged level's directory on the way when the merge runs a kernel.
+int merge_into_level(sparkalog_store* st, RelState& r, int l, const u64* a, u64 na, const u64* b, u64 nb,
+                     cudaStream_t s, u64* launches) {
+    const u64 n = na + nb;
+    SPK_CUDA(r.spare.ensure(n * 8, s), "cudaMallocAsync");
+    u32 shift;
+    u64 buckets;
+    directory_shape(st, n, &shift, &buckets);
+    SPK_CUDA(r.dir[l].ensure((buckets + 1) * 4, s), "cudaMallocAsync");
+    u64 launched = 0;
+    SPK_CUDA(launch_merge(a, na, b, nb, r.spare.as<u64>(), st->merge_splits, s, &launched,
+                          spk::MergeDirectory{r.dir[l].as<u32>(), shift, buckets}),
+             "merge_disjoint_kernel");
+    swap_arrays(r.level[l], r.spare);
+    r.level_n[l] = n;
+    r.dir_valid[l] = launched > 0;  // a plain copy (one side empty) wrote no directory
+    r.dir_shift[l] = shift;
+    r.dir_buckets[l] = buckets;
+    if (launches) *launches += launched;
     return 0;
 }
 
@@ -394,7 +423,6 @@ struct sparkalog_executor {
     std::vector<sparkalog_rule_plan> rules;
     std::vector<TargetRT> targets;
     std::vector<IndexCache> index;
-    DevArray counts;       // device: per target [rules+1] join counts, sort count, newt count
     DevArray counters;     // device: tile counters, error word
     DevArray status;       // shared look-back words for join / anti-join
     u64* host_counts = nullptr;  // pinned mirror of `counts`
@@ -421,6 +449,14 @@ struct sparkalog_executor {
     };
     bool profiling = false;
     bool fused_enabled = true;
+    // `counters` holds, in this order: the per-round tile counters
+    // (kCounterWords u32), the per-target counts (counts_words u64), the error
+    // word and the fused kernels' fallback flags, then a few words that the
+    // per-round clearing leaves alone. One memset clears a round's words and
+    // one copy brings its counts and error bits to the host.
+    u32* tile_counters() const { return counters.as<u32>(); }
+    u64* count_words() const { return reinterpret_cast<u64*>(counters.as<u32>() + kCounterWords); }
+    u32* err_words() const { return counters.as<u32>() + kCounterWords + 2 * counts_words; }
     bool member_enabled = false;  // anti-join through FULL's hash set (opt-in)
     std::vector<sparkalog_round_trace> trace;  // per-round operator cardinalities
     std::vector<cudaEvent_t> free_events;
@@ -505,8 +541,6 @@ int radix_sort(u64* a, u64* b, const u64* n_dev, u64 n_host_bound, SortScratch& 
     return 0;
 }
 
-constexpr size_t kCounterWords = 1024;  // per-round tile counters
-constexpr size_t kErrWord = kCounterWords;
 
 size_t target_count_base(const sparkalog_executor* ex, size_t t) {
     // Layout per target: [rules + 1 join counts][newt count][distinct join rows]
@@ -521,7 +555,7 @@ constexpr int kFusedRowCap = 1024;  // DELTA rows per fused tile
 constexpr size_t kFusedFlagBase = 8;      // fallback flags live at err + 8 + target
 constexpr size_t kFusedMaxTargets = 48;
 constexpr size_t kMaxTraceRounds = 1u << 20;
-constexpr size_t kMemberErrWord = kCounterWords + kFusedFlagBase + kFusedMaxTargets + 4;
+constexpr size_t kMemberErrOffset = kFusedFlagBase + kFusedMaxTargets + 4;  // from the error word
 
 // The fused round applies to a target with one rule whose join output starts
 // with DELTA's first column (then the join output is sorted by it) while
@@ -715,7 +749,7 @@ int build_index_impl(sparkalog_executor* ex, sparkalog_store* st, IndexCache& ic
         if (n) {
             spk::key_row_pairs_kernel<<<simple_grid(n), 256, 0, s>>>(rows, n, column, ex->index_pairs[0].as<u64>());
             SPK_CUDA(cudaGetLastError(), "key_row_pairs_kernel");
-            u32* err = ex->counters.as<u32>() + kErrWord;
+            u32* err = ex->err_words();
             int rc = radix_sort(ex->index_pairs[0].as<u64>(), ex->index_pairs[1].as<u64>(), nullptr, n, ex->index_sort,
                                 ex, err, s, nullptr, nullptr);
             if (rc) return rc;
@@ -741,7 +775,7 @@ int build_index_impl(sparkalog_executor* ex, sparkalog_store* st, IndexCache& ic
         SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
     }
     ic.num_keys = n ? (last >> 32) + 1 : 0;
-    u32* maxdeg = ex->counters.as<u32>() + kErrWord + 1;
+    u32* maxdeg = ex->err_words() + 1;
     SPK_CUDA(cudaMemsetAsync(maxdeg, 0, 4, s), "cudaMemsetAsync");
     ic.bucketed = n && ic.num_keys > std::max<u64>(4 * n, u64(1) << 22);
     if (ic.bucketed) {
@@ -1232,9 +1266,9 @@ int sparkalog_executor_compile(sparkalog_store* st, const u32* relations, size_t
     ex->counts_words = 0;
     for (auto& t : ex->targets) ex->counts_words += t.rules.size() + 3;
     cudaStream_t s = st->stream;
-    cudaError_t e = ex->counts.ensure(ex->counts_words * 8, s);
-    if (e == cudaSuccess) e = ex->counters.ensure((kCounterWords + 64) * 4, s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(ex->counters.ptr, 0, (kCounterWords + 64) * 4, s);
+    const size_t counter_bytes = (kCounterWords + 2 * ex->counts_words + 64) * 4;
+    cudaError_t e = ex->counters.ensure(counter_bytes, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ex->counters.ptr, 0, counter_bytes, s);
     if (e == cudaSuccess) e = cudaMallocHost(&ex->host_counts, ex->counts_words * 8 + 512);
     if (e == cudaSuccess) e = ex->rule_delta.ensure(std::max<size_t>(rule_count, 1) * 8, s);
     if (e == cudaSuccess) e = cudaMallocHost(&ex->host_rule_delta, std::max<size_t>(rule_count, 1) * 8);
@@ -1262,7 +1296,6 @@ void sparkalog_executor_destroy(sparkalog_executor* ex) {
         ic.keys32.release(s);
         ic.bucket_dir.release(s);
     }
-    ex->counts.release(s);
     ex->seg_seen.release(s);
     ex->seg_new.release(s);
     ex->rule_delta.release(s);
@@ -1367,12 +1400,12 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
             p.union_right[0] != 0 || p.union_right[1] != 1)
             return fail(SPARKALOG_E_INVALID_ARGUMENT, "set operators must use columns [0, 1]");
     }
-    u32* counters = ex->counters.as<u32>();
-    u32* err = counters + kErrWord;
-    u64* counts = ex->counts.as<u64>();
+    u32* counters = ex->tile_counters();
+    u32* err = ex->err_words();
+    u64* counts = ex->count_words();
     // Errors of hash-set inserts, which run after a round's check: a word the
     // per-round clearing leaves alone, read once when the run ends.
-    u32* member_err = counters + kMemberErrWord;
+    u32* member_err = err + kMemberErrOffset;
     SPK_CUDA(cudaMemsetAsync(member_err, 0, 4, s), "cudaMemsetAsync");
 
     // FULL of each SCC relation must be a sorted run before the first merge;
@@ -1481,10 +1514,6 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                 t.j_cap = cap;
             }
         }
-        SPK_CUDA(cudaMemcpyAsync(ex->rule_delta.ptr, ex->host_rule_delta, ex->rules.size() * 8,
-                                 cudaMemcpyHostToDevice, s),
-                 "cudaMemcpyAsync");
-
         for (;;) {
             for (auto& t : ex->targets) {
                 SPK_CUDA(st->find(t.id)->newt.ensure(t.j_cap * 8, s), "cudaMallocAsync");
@@ -1497,15 +1526,23 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                 max_status_words = std::max<size_t>(max_status_words, (delta_rows + t.fused_rows - 1) / t.fused_rows + 1);
             }
             SPK_CUDA(ex->status.ensure_zeroed(max_status_words * 8, s), "cudaMallocAsync");
-            SPK_CUDA(cudaMemsetAsync(counters, 0, (kCounterWords + kFusedFlagBase + kFusedMaxTargets) * 4, s),
+            SPK_CUDA(cudaMemsetAsync(counters, 0,
+                                     (kCounterWords + 2 * ex->counts_words + kFusedFlagBase + kFusedMaxTargets) * 4, s),
                      "cudaMemsetAsync");
-            SPK_CUDA(cudaMemsetAsync(counts, 0, ex->counts_words * 8, s), "cudaMemsetAsync");
             size_t counter_slot = 0;
             // Targets whose single rule projects DELTA's first column (the
             // transitive-closure shape) run the fused round kernel; the rest
             // join, radix sort and anti-join with the general kernels.
             std::vector<char> fused(ex->targets.size(), 0);
-            for (size_t ti = 0; ti < ex->targets.size(); ++ti) fused[ti] = fused_eligible(ex, st, ti) ? 1 : 0;
+            bool any_general = false;
+            for (size_t ti = 0; ti < ex->targets.size(); ++ti) {
+                fused[ti] = fused_eligible(ex, st, ti) ? 1 : 0;
+                any_general |= !fused[ti];
+            }
+            if (any_general)  // the general join reads DELTA sizes on the device
+                SPK_CUDA(cudaMemcpyAsync(ex->rule_delta.ptr, ex->host_rule_delta, ex->rules.size() * 8,
+                                         cudaMemcpyHostToDevice, s),
+                         "cudaMemcpyAsync");
             const int join_timing = ex->begin(SPARKALOG_K_JOIN, s);
             u64 join_launches = 0;
             // Joins: every rule appends into its target's candidate buffer.
@@ -1685,10 +1722,9 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                              "cudaMemcpyAsync");
             }
             // The round's only host synchronisation: counts and error bits.
-            SPK_CUDA(cudaMemcpyAsync(ex->host_counts, counts, ex->counts_words * 8, cudaMemcpyDeviceToHost, s),
-                     "cudaMemcpyAsync");
-            SPK_CUDA(cudaMemcpyAsync(ex->host_counts + ex->counts_words, err,
-                                     (kFusedFlagBase + kFusedMaxTargets) * 4, cudaMemcpyDeviceToHost, s),
+            SPK_CUDA(cudaMemcpyAsync(ex->host_counts, counts,
+                                     ex->counts_words * 8 + (kFusedFlagBase + kFusedMaxTargets) * 4,
+                                     cudaMemcpyDeviceToHost, s),
                      "cudaMemcpyAsync");
             SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
             const u32 bits = static_cast<u32>(ex->host_counts[ex->counts_words] & 0xffffffffu);
@@ -1773,19 +1809,15 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                 // TAIL <- TAIL u NEWT
                 const int tail = spk::kMaxLevels - 1;
                 const u64 tn = tr.level_n[tail] + newt_n;
-                SPK_CUDA(tr.spare.ensure(tn * 8, s), "cudaMallocAsync");
                 {
                     u64 launched = 0;
                     const int tm = ex->begin(SPARKALOG_K_MERGE, s);
-                    SPK_CUDA(launch_merge(tr.level[tail].as<u64>(), tr.level_n[tail], tr.newt.as<u64>(), newt_n,
-                                          tr.spare.as<u64>(), st->merge_splits, s, &launched),
-                             "merge_disjoint_kernel");
+                    int rc = merge_into_level(st, tr, tail, tr.level[tail].as<u64>(), tr.level_n[tail],
+                                              tr.newt.as<u64>(), newt_n, s, &launched);
+                    if (rc) return rc;
                     ex->end(tm, s, 16.0 * static_cast<double>(tn), launched);
                     ex->stats.total_launches += launched;
                 }
-                swap_arrays(tr.level[tail], tr.spare);
-                tr.level_n[tail] = tn;
-                tr.dir_valid[tail] = false;
                 // Cascade: a level merges down once it outgrows 1/kLevelRatio of the next.
                 for (int l = tail; l > 0; --l) {
                     if (tr.level_n[l] == 0 || tr.level_n[l] * kLevelRatio <= tr.level_n[l - 1]) continue;
@@ -1800,18 +1832,15 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                         continue;
                     }
                     const u64 mn = tr.level_n[l - 1] + tr.level_n[l];
-                    SPK_CUDA(tr.spare.ensure(mn * 8, s), "cudaMallocAsync");
                     u64 launched = 0;
                     const int tm = ex->begin(SPARKALOG_K_MERGE, s);
-                    SPK_CUDA(launch_merge(tr.level[l - 1].as<u64>(), tr.level_n[l - 1], tr.level[l].as<u64>(),
-                                          tr.level_n[l], tr.spare.as<u64>(), st->merge_splits, s, &launched),
-                             "merge_disjoint_kernel");
+                    int rc = merge_into_level(st, tr, l - 1, tr.level[l - 1].as<u64>(), tr.level_n[l - 1],
+                                              tr.level[l].as<u64>(), tr.level_n[l], s, &launched);
+                    if (rc) return rc;
                     ex->end(tm, s, 16.0 * static_cast<double>(mn), launched);
                     ex->stats.total_launches += launched;
-                    swap_arrays(tr.level[l - 1], tr.spare);
-                    tr.level_n[l - 1] = mn;
                     tr.level_n[l] = 0;
-                    tr.dir_valid[l - 1] = tr.dir_valid[l] = false;
+                    tr.dir_valid[l] = false;
                 }
             }
             {

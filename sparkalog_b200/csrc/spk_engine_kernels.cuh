@@ -464,14 +464,28 @@ static __global__ void merge_partition_kernel(const u64* a, u64 na, const u64* b
     }
 }
 
+// Directory of a merge's output, written by the merge itself (see Levels):
+// dir[b] = first output row whose key >> shift >= b, for b in [0, buckets].
+struct MergeDirectory {
+    u32* dir;  // null: no directory
+    u32 shift;
+    u64 buckets;
+};
+
 // Merge of two sorted, mutually disjoint runs (levels are disjoint by
 // construction: NEWT excludes FULL). Output position = merge diagonal, so no
-// compaction or look-back is needed: pure streaming at HBM rate.
+// compaction or look-back is needed: a tile's two input slices arrive in
+// shared memory by asynchronous copies, each thread merges ITEMS rows from
+// its diagonal, and the tile leaves with coalesced stores. With a directory,
+// every output row that starts a bucket (or a run of empty buckets) writes
+// the directory entries up to its bucket, so the merged level needs no
+// separate directory pass.
 template <int THREADS, int ITEMS>
 __global__ void __launch_bounds__(THREADS) merge_disjoint_kernel(const u64* a, u64 na, const u64* b, u64 nb,
-                                                                 const u64* splits, u64* out) {
+                                                                 const u64* splits, u64* out, MergeDirectory md) {
     constexpr int kTile = THREADS * ITEMS;
-    __shared__ u64 sm[kTile];
+    __shared__ __align__(16) u64 sm[kTile];
+    __shared__ u64 before_tile;  // the output row just before the tile
     const u64 total = na + nb;
     const u64 num_tiles = (total + kTile - 1) / kTile;
     for (u64 tile = blockIdx.x; tile < num_tiles; tile += gridDim.x) {
@@ -480,8 +494,14 @@ __global__ void __launch_bounds__(THREADS) merge_disjoint_kernel(const u64* a, u
         const u64 i0 = splits[tile], i1 = splits[tile + 1];
         const u64 j0 = d0 - i0, j1 = d1 - i1;
         const u32 sa_n = static_cast<u32>(i1 - i0), sb_n = static_cast<u32>(j1 - j0);
-        for (u32 t = threadIdx.x; t < sa_n; t += THREADS) sm[t] = a[i0 + t];
-        for (u32 t = threadIdx.x; t < sb_n; t += THREADS) sm[sa_n + t] = b[j0 + t];
+        for (u32 t = threadIdx.x; t < sa_n; t += THREADS) cp_async_8(sm + t, a + i0 + t);
+        for (u32 t = threadIdx.x; t < sb_n; t += THREADS) cp_async_8(sm + sa_n + t, b + j0 + t);
+        cp_async_commit();
+        if (md.dir && threadIdx.x == 0 && d0 > 0) {
+            const u64 pa = i0 > 0 ? a[i0 - 1] : 0, pb = j0 > 0 ? b[j0 - 1] : 0;
+            before_tile = i0 == 0 ? pb : (j0 == 0 ? pa : (pa > pb ? pa : pb));
+        }
+        cp_async_wait<0>();
         __syncthreads();
         const SmemKeys sa{sm}, sb{sm + sa_n};
         const u32 diag = threadIdx.x * ITEMS;
@@ -504,6 +524,17 @@ __global__ void __launch_bounds__(THREADS) merge_disjoint_kernel(const u64* a, u
             if (diag + i < len) sm[diag + i] = v[i];
         __syncthreads();
         for (u32 j = threadIdx.x; j < len; j += THREADS) out[d0 + j] = sm[j];
+        if (md.dir) {
+            for (u32 j = threadIdx.x; j < len; j += THREADS) {
+                const u64 o = d0 + j;
+                const u64 bucket = sm[j] >> md.shift;
+                u64 from = 0;
+                if (o > 0) from = ((j > 0 ? sm[j - 1] : before_tile) >> md.shift) + 1;
+                for (u64 e = from; e <= bucket && e <= md.buckets; ++e) md.dir[e] = static_cast<u32>(o);
+                if (o == total - 1)
+                    for (u64 e = bucket + 1; e <= md.buckets; ++e) md.dir[e] = static_cast<u32>(total);
+            }
+        }
         __syncthreads();
     }
 }

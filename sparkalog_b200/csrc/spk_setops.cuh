@@ -352,4 +352,73 @@ __global__ void __launch_bounds__(THREADS) union_soa_kernel(const u32* lf, const
     }
 }
 
+// ---------------------------------------------------------------------------
+// Filter (the reference's sparkalog_filter_u32, column_ops.cu:20-43 and
+// 283-318): row ids i, ascending, with compare(input[i], op, operand), and
+// flags[i] = 1 / 0. Operation codes are the ABI's: 0 ==, 1 !=, 2 <, 3 <=,
+// 4 >, 5 >=; any other code matches nothing. Kept ids are compacted in order
+// with a decoupled look-back; the count is u32 like the reference's.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool filter_matches(u32 value, u32 op, u32 operand) {
+    switch (op) {
+        case 0: return value == operand;
+        case 1: return value != operand;
+        case 2: return value < operand;
+        case 3: return value <= operand;
+        case 4: return value > operand;
+        case 5: return value >= operand;
+        default: return false;
+    }
+}
+
+template <int THREADS, int ITEMS>
+__global__ void __launch_bounds__(THREADS) filter_select_kernel(const u32* input, u64 n, u32 op, u32 operand,
+                                                                u32* flags, u32* output, u32* count, u64* status,
+                                                                u32* tile_counter, u32 epoch, u32* err) {
+    constexpr int kTile = THREADS * ITEMS;
+    __shared__ CompactShared<THREADS> cs;
+    __shared__ u32 stage[kTile];
+    const u64 num_tiles = (n + kTile - 1) / kTile;
+    for (;;) {
+        if (threadIdx.x == 0) cs.tile = atomicAdd(tile_counter, 1u);
+        __syncthreads();
+        const u64 tile = cs.tile;
+        if (tile >= num_tiles) break;
+        const u64 base = tile * kTile + static_cast<u64>(threadIdx.x) * ITEMS;
+        u32 keep = 0;
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i) {
+            const u64 idx = base + i;
+            if (idx < n) {
+                const bool m = filter_matches(input[idx], op, operand);
+                flags[idx] = m ? 1u : 0u;
+                keep |= m ? (1u << i) : 0u;
+            }
+        }
+        u32 excl, total;
+        const u64 off = compact_offsets<THREADS>(__popc(keep), &excl, &total, tile, status, epoch, err, cs);
+        u32 w = excl;
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i)
+            if (keep & (1u << i)) stage[w++] = static_cast<u32>(base + i);
+        __syncthreads();
+        for (u32 j = threadIdx.x; j < total; j += THREADS) output[off + j] = stage[j];
+        if (tile == num_tiles - 1 && threadIdx.x == 0) *count = static_cast<u32>(off + total);
+        __syncthreads();
+    }
+}
+
+// output[i] = i % modulus (the reference's sparkalog_fill_mod_u32).
+static __global__ void fill_mod_kernel(u32* output, u64 n, u32 modulus) {
+    const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+    for (u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+        output[i] = static_cast<u32>(i % modulus);
+}
+
+// data[i] += 1 (the reference's sparkalog_add_one_i32, its workspace smoke test).
+static __global__ void add_one_kernel(int* data, u64 n) {
+    const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+    for (u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) data[i] += 1;
+}
+
 }  // namespace spk

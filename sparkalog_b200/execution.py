@@ -17,7 +17,8 @@ import numpy as np
 import torch
 
 from . import _native
-from .relational import BinaryDistinct, BinaryEqualityJoin, JoinInput, SortedBinaryAntiJoin, SortedBinaryUnion
+from .relational import (BinaryDistinct, BinaryEqualityJoin, JoinInput, SortedBinaryAntiJoin, SortedBinaryUnion,
+                         U32Predicate)
 
 U32_MAX = 0xFFFFFFFF
 
@@ -204,6 +205,20 @@ class UnionWorkspace:
         self.temp = _Temp()
 
 
+class FilterWorkspace:
+    """Flags, selection (row ids) and count of a filter (storage/src/lib.rs:499-595)."""
+
+    def __init__(self):
+        self.flags = _dev_u32(0)
+        self.selection = _dev_u32(0)
+        self.count = torch.zeros(1, dtype=torch.int32, device="cuda")
+        self.selected = 0
+        self.temp = _Temp()
+
+    def selection_host(self) -> np.ndarray:
+        return self.selection[:self.selected].cpu().numpy().view(np.uint32)
+
+
 def _grow_u32(t: torch.Tensor, n: int) -> torch.Tensor:
     return t if t.numel() >= max(n, 1) else _dev_u32(n)
 
@@ -216,6 +231,38 @@ def _read_count(t: torch.Tensor, stream: CudaStream) -> int:
     stream.synchronize()
     v = int(t[0].item())
     return v & (U32_MAX if t.dtype == torch.int32 else 0xFFFFFFFFFFFFFFFF)
+
+
+def filter_cuda(column: torch.Tensor, predicate: U32Predicate, operand: int, workspace: FilterWorkspace,
+                stream: CudaStream) -> None:
+    """Ascending row ids whose value satisfies the predicate (filter_cuda, lib.rs:1809-1875, plus its wait)."""
+    L = _native.load()
+    n = int(column.numel())
+    check_row_count(n)
+    ws = workspace
+    ws.flags = _grow_u32(ws.flags, n)
+    ws.selection = _grow_u32(ws.selection, n)
+    temp_bytes = ctypes.c_size_t(0)
+    _check("sparkalog_filter_u32_temporary_bytes",
+           L.sparkalog_filter_u32_temporary_bytes(_ptr(ws.flags), _ptr(ws.selection), _ptr(ws.count), n,
+                                                  ctypes.byref(temp_bytes), stream.raw))
+    temp = ws.temp.reserve(temp_bytes.value)
+    _check("sparkalog_filter_u32",
+           L.sparkalog_filter_u32(_ptr(column), n, int(predicate), int(operand) & U32_MAX, _ptr(ws.flags),
+                                  _ptr(ws.selection), _ptr(ws.count), _ptr(temp), temp_bytes.value, stream.raw))
+    ws.selected = _read_count(ws.count, stream)
+
+
+def fill_mod_u32(column: torch.Tensor, modulus: int, stream: CudaStream) -> None:
+    """column[i] = i % modulus (fill_mod_u32, lib.rs:1926-1950)."""
+    _check("sparkalog_fill_mod_u32", _native.load().sparkalog_fill_mod_u32(_ptr(column), int(column.numel()),
+                                                                            int(modulus), stream.raw))
+
+
+def add_one_i32(column: torch.Tensor, stream: CudaStream) -> None:
+    """column[i] += 1 (add_one_i32, lib.rs:305-320)."""
+    _check("sparkalog_add_one_i32", _native.load().sparkalog_add_one_i32(_ptr(column), int(column.numel()),
+                                                                          stream.raw))
 
 
 def distinct_cuda(input: Relation, plan: BinaryDistinct, workspace: DistinctWorkspace, stream: CudaStream) -> None:

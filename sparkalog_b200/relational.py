@@ -72,6 +72,31 @@ class SortedBinaryUnion:
     right: tuple[int, int] = (0, 1)
 
 
+class U32Predicate(enum.IntEnum):
+    """Comparison of a u32 value with an operand (crates/sparkalog-relational/src/lib.rs:144-164);
+    the integer values are the operation codes of the filter ABI."""
+
+    EQ = 0
+    NE = 1
+    LT = 2
+    LE = 3
+    GT = 4
+    GE = 5
+
+    def matches(self, value: int, operand: int) -> bool:
+        return {0: value == operand, 1: value != operand, 2: value < operand, 3: value <= operand,
+                4: value > operand, 5: value >= operand}[int(self)]
+
+
+@dataclass(frozen=True)
+class Filter:
+    """A filter producing compact row ids (lib.rs:166-171): column, predicate and operand."""
+
+    column: int
+    predicate: U32Predicate
+    operand: int
+
+
 @dataclass
 class RecursiveRulePlan:
     """One semi-naive binary rule lowered to operators (relational/src/lib.rs:72-82)."""

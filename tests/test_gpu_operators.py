@@ -261,3 +261,102 @@ def test_device_error_bits_clear(cuda):
     bits = ctypes.c_uint32(123)
     assert _native.load().sparkalog_b200_device_error(ctypes.byref(bits), 1) == 0
     assert bits.value == 0
+
+
+def test_filter_known_answers_and_oracle(cuda, known_answers):
+    # lib.rs:2015-2027, 2403-2445 plus random columns against the oracle.
+    E = ex()
+    from sparkalog_b200.relational import U32Predicate
+
+    torch = cuda
+    stream = E.CudaStream()
+    ws = E.FilterWorkspace()
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.uint32).view(np.int32)).cuda()
+    for case in known_answers["filter"]:
+        if "values_mod" in case:
+            n, m = case["values_mod"]
+            values = np.arange(n, dtype=np.uint32) % m
+            E.filter_cuda(dev(values), U32Predicate(case["op"]), case["operand"], ws, stream)
+            assert ws.selected == case["expected_count"]
+            assert np.array_equal(ws.selection_host(), oracle.filter_serial(values, case["op"], case["operand"]))
+            continue
+        for op, operand, want in case["cases"]:
+            E.filter_cuda(dev(case["values"]), U32Predicate(op), operand, ws, stream)
+            assert ws.selection_host().tolist() == want, case["source"]
+    rng = np.random.default_rng(77)
+    for n in (1, 2047, 2048, 2049, 1_000_003):
+        values = rng.integers(0, 1 << 32, size=n, dtype=np.uint64).astype(np.uint32)
+        values[::7] = 12345
+        for op in range(6):
+            operand = 12345 if op in (0, 1) else int(values[n // 2])
+            E.filter_cuda(dev(values), U32Predicate(op), operand, ws, stream)
+            assert np.array_equal(ws.selection_host(), oracle.filter_parallel(values, op, operand))
+            flags = ws.flags[:n].cpu().numpy().view(np.uint32)
+            want = np.zeros(n, dtype=np.uint32)
+            want[oracle.filter_parallel(values, op, operand)] = 1
+            assert np.array_equal(flags, want)
+
+
+def test_filter_fill_add_one_edges(cuda, known_answers):
+    from sparkalog_b200 import _native
+
+    E = ex()
+    torch = cuda
+    stream = E.CudaStream()
+    L = _native.load()
+    size = ctypes.c_size_t(0)
+    # Null checks and empty inputs as in column_ops.cu:252-336.
+    assert L.sparkalog_filter_u32_temporary_bytes(None, None, None, 0, ctypes.byref(size), None) == 1
+    assert L.sparkalog_filter_u32(None, 0, 0, 0, None, None, None, None, 0, None) == 1
+    assert L.sparkalog_fill_mod_u32(None, 0, 0, None) == 1
+    assert L.sparkalog_fill_mod_u32(None, 0, 5, None) == 0
+    assert L.sparkalog_add_one_i32(None, 3, None) == 1
+    count = torch.full((1,), 99, dtype=torch.int32, device="cuda")
+    assert L.sparkalog_filter_u32(None, 0, 0, 0, None, None, count.data_ptr(), None, 0, stream.raw) == 0
+    stream.synchronize()
+    assert int(count.item()) == 0
+    # fill_mod: lib.rs:2448-2459.
+    fm = known_answers["fill_mod"]
+    col = torch.zeros(fm["len"], dtype=torch.int32, device="cuda")
+    E.fill_mod_u32(col, fm["modulus"], stream)
+    stream.synchronize()
+    assert col.cpu().numpy().tolist() == [i % fm["modulus"] for i in range(fm["len"])]
+    E.add_one_i32(col, stream)
+    stream.synchronize()
+    assert col.cpu().numpy().tolist() == [i % fm["modulus"] + 1 for i in range(fm["len"])]
+
+
+def test_filter_against_reference_cuda_build(cuda):
+    """The reference's own sparkalog_filter_u32 (column_ops.cu built for sm_100a) agrees."""
+    ref = oracle.reference_cuda()
+    if ref is None:
+        pytest.skip("reference CUDA library not built (oracle/_ref)")
+    E = ex()
+    from sparkalog_b200.relational import U32Predicate
+
+    torch = cuda
+    vp = ctypes.c_void_p
+    ref.sparkalog_filter_u32_temporary_bytes.argtypes = [vp, vp, vp, ctypes.c_size_t,
+                                                         ctypes.POINTER(ctypes.c_size_t), vp]
+    ref.sparkalog_filter_u32.argtypes = [vp, ctypes.c_size_t, ctypes.c_uint32, ctypes.c_uint32, vp, vp, vp, vp,
+                                         ctypes.c_size_t, vp]
+    rng = np.random.default_rng(5)
+    n = 300_000
+    values = rng.integers(0, 1000, size=n).astype(np.uint32)
+    col = torch.from_numpy(values.view(np.int32)).cuda()
+    flags = torch.zeros(n, dtype=torch.int32, device="cuda")
+    out = torch.zeros(n, dtype=torch.int32, device="cuda")
+    count = torch.zeros(1, dtype=torch.int32, device="cuda")
+    tb = ctypes.c_size_t(0)
+    assert ref.sparkalog_filter_u32_temporary_bytes(flags.data_ptr(), out.data_ptr(), count.data_ptr(), n,
+                                                    ctypes.byref(tb), None) == 0
+    tmp = torch.empty(max(tb.value, 1), dtype=torch.uint8, device="cuda")
+    ws = E.FilterWorkspace()
+    stream = E.CudaStream()
+    for op in range(6):
+        assert ref.sparkalog_filter_u32(col.data_ptr(), n, op, 500, flags.data_ptr(), out.data_ptr(),
+                                        count.data_ptr(), tmp.data_ptr(), tb.value, None) == 0
+        torch.cuda.synchronize()
+        want = out[:int(count.item())].cpu().numpy().view(np.uint32)
+        E.filter_cuda(col, U32Predicate(op), 500, ws, stream)
+        assert np.array_equal(ws.selection_host(), want)

@@ -177,3 +177,19 @@ def test_parallel_operators_match_serial():
     j1 = oracle.join(da, db, threads=1)
     j6 = oracle.join(da, db, threads=6)
     assert pairs(j1) == pairs(j6)
+
+
+def test_filter_known_answers(known_answers):
+    # lib.rs:2015-2027, 2403-2445: every predicate, serial == parallel, empty columns.
+    for case in known_answers["filter"]:
+        if "values_mod" in case:
+            n, m = case["values_mod"]
+            values = np.arange(n, dtype=np.uint32) % m
+            a = oracle.filter_serial(values, case["op"], case["operand"])
+            b = oracle.filter_parallel(values, case["op"], case["operand"])
+            assert len(a) == case["expected_count"] and np.array_equal(a, b)
+            continue
+        for op, operand, want in case["cases"]:
+            assert oracle.filter_serial(case["values"], op, operand).tolist() == want, case["source"]
+            assert oracle.filter_parallel(case["values"], op, operand).tolist() == want, case["source"]
+    assert oracle.filter_serial([1, 2, 3], 9, 1).tolist() == []  # unknown operation code: no rows
