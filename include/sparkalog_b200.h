@@ -160,6 +160,7 @@ enum {
     SPARKALOG_E_DEVICE_FAULT = -20,        /* a kernel reported an error bit */
     SPARKALOG_E_INVALID_ARGUMENT = -21,
     SPARKALOG_E_UNSORTED_FULL = -22,       /* FULL must be sorted for anti-join/union */
+    SPARKALOG_E_LOAD = -23,                /* storage::LoadError; details in sparkalog_load_error */
 };
 
 /* JoinInput: 0 = Left (the DELTA side), 1 = Right. */
@@ -319,6 +320,52 @@ SPARKALOG_API int sparkalog_executor_set_fused(sparkalog_executor* executor, int
  * locality that hashing gives up, so the set is opt-in. No counterpart in the
  * reference. */
 SPARKALOG_API int sparkalog_executor_set_member_set(sparkalog_executor* executor, int enable);
+
+/* Device value catalog: ValueCatalog (crates/sparkalog-datalog/src/
+ * catalog.rs:98-127) for u32 values. intern gives every value of the batch
+ * its dense id, new values numbered by first appearance after the catalog's
+ * current size (as interning the values one by one in order would);
+ * decode maps ids back to values (Database::query's decode, database.rs:
+ * 179-213) and fails with SPARKALOG_E_INVALID_ARGUMENT on an id outside the
+ * catalog. `location` applies to both the input and the output array. */
+typedef struct sparkalog_catalog sparkalog_catalog;
+SPARKALOG_API int sparkalog_catalog_create(void* stream, sparkalog_catalog** out);
+SPARKALOG_API void sparkalog_catalog_destroy(sparkalog_catalog* catalog);
+SPARKALOG_API int sparkalog_catalog_intern_u32(sparkalog_catalog* catalog, const uint32_t* values, size_t count,
+                                               int location, uint32_t* ids, size_t* catalog_size);
+SPARKALOG_API int sparkalog_catalog_decode_u32(sparkalog_catalog* catalog, const uint32_t* ids, size_t count,
+                                               int location, uint32_t* values);
+SPARKALOG_API int sparkalog_catalog_size(sparkalog_catalog* catalog, size_t* size);
+
+/* storage::LoadError (crates/sparkalog-storage/src/io.rs:7-20). */
+enum {
+    SPARKALOG_LOAD_OK = 0,
+    SPARKALOG_LOAD_GIT_LFS_POINTER = 1,
+    SPARKALOG_LOAD_INVALID_FIELD_COUNT = 2,
+    SPARKALOG_LOAD_INVALID_U32 = 3
+};
+typedef struct sparkalog_load_error {
+    int32_t kind;           /* SPARKALOG_LOAD_* */
+    uint32_t column;        /* 1 or 2 for SPARKALOG_LOAD_INVALID_U32 */
+    uint64_t line;          /* 1-based line number */
+    uint64_t field_offset;  /* byte offset of the offending field in `text` */
+    uint64_t field_length;  /* its length in bytes */
+} sparkalog_load_error;
+
+/* load_binary_u32 (crates/sparkalog-storage/src/io.rs:72-138) parsed on the
+ * GPU and inserted as relation `id` (static, or recursive with FULL = DELTA
+ * when `recursive` != 0). `text` holds `bytes` bytes of whitespace-separated
+ * u32 pairs, one per line, in host or device memory (`location`); empty
+ * lines and lines starting with '#' or '%' are skipped. On a malformed input
+ * nothing is inserted, the call returns SPARKALOG_E_LOAD and *error (when not
+ * null) names the first failing line as the reference would: a Git LFS
+ * pointer anywhere first, then the lowest line with a wrong field count or a
+ * field that is not a u32. Whitespace is ASCII whitespace. *rows receives the
+ * number of rows read; they are inserted as read (in file order, duplicates
+ * kept), as inserting load_binary_u32's relation would. */
+SPARKALOG_API int sparkalog_store_load_binary_u32(sparkalog_store* store, uint32_t id, const char* text, size_t bytes,
+                                                  int location, int recursive, size_t* rows,
+                                                  sparkalog_load_error* error);
 SPARKALOG_API int sparkalog_executor_stats(sparkalog_executor* executor, sparkalog_kernel_stats* out, int reset);
 
 /* Per-round trace of an executor (the operator cardinalities of each round,

@@ -531,3 +531,64 @@ def filter_parallel(values, op: int, operand: int, workers: int = 8) -> np.ndarr
         out[off:off + counts[c]] = np.nonzero(f)[0].astype(np.uint32) + np.uint32(i)
         off += counts[c]
     return out
+
+
+# ---------------------------------------------------------------------------
+# load_binary_u32 (crates/sparkalog-storage/src/io.rs:72-138): count_rows
+# first (a Git LFS pointer header anywhere is an error), then populate_columns
+# line by line: trim, skip empty / '#' / '%' lines, exactly two whitespace
+# separated fields, each parsed as u32 (optional '+', decimal digits).
+# ---------------------------------------------------------------------------
+class OracleLoadError(Exception):
+    def __init__(self, kind: str, line: int = 0, column: int = 0, value: str | None = None):
+        super().__init__(kind, line, column, value)
+        self.kind, self.line, self.column, self.value = kind, line, column, value
+
+
+_LFS = "version https://git-lfs.github.com/spec/v1"
+_ASCII_SPACE = " \t\n\x0b\x0c\r"
+
+
+def _parse_u32(field: str) -> int | None:
+    digits = field[1:] if field.startswith("+") else field
+    if not digits or any(c not in "0123456789" for c in digits):
+        return None
+    v = int(digits)
+    return v if v <= 0xFFFFFFFF else None
+
+
+def load_binary_u32(data: bytes) -> tuple[np.ndarray, np.ndarray]:
+    lines = data.decode().split("\n")
+    if lines and lines[-1] == "":
+        lines.pop()  # str::lines(): a final '\n' ends the last line
+    for line in lines:  # count_rows
+        t = line.strip(_ASCII_SPACE)
+        if t and t[0] not in "#%" and t == _LFS:
+            raise OracleLoadError("GitLfsPointer")
+    first, second = [], []
+    for index, line in enumerate(lines):  # populate_columns
+        t = line.strip(_ASCII_SPACE)
+        if not t or t[0] in "#%":
+            continue
+        fields = [f for f in t.replace("\t", " ").replace("\x0b", " ").replace("\x0c", " ").replace("\r", " ")
+                  .split(" ") if f]
+        if len(fields) != 2:
+            raise OracleLoadError("InvalidFieldCount", index + 1)
+        for column, f in enumerate(fields, start=1):
+            v = _parse_u32(f)
+            if v is None:
+                raise OracleLoadError("InvalidU32", index + 1, column, f)
+            (first if column == 1 else second).append(v)
+    return np.array(first, dtype=np.uint32), np.array(second, dtype=np.uint32)
+
+
+def intern(values, catalog: dict | None = None) -> tuple[np.ndarray, dict]:
+    """ValueCatalog::intern (crates/sparkalog-datalog/src/catalog.rs:108-117) applied to
+    each value in order: an unseen value gets id len(catalog)."""
+    catalog = {} if catalog is None else catalog
+    out = np.empty(len(values), dtype=np.uint32)
+    for i, v in enumerate(np.asarray(values, dtype=np.uint32).tolist()):
+        if v not in catalog:
+            catalog[v] = len(catalog)
+        out[i] = catalog[v]
+    return out, catalog

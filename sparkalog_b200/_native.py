@@ -44,6 +44,12 @@ TIER_B = [
     "sparkalog_store_rows",
     "sparkalog_store_read",
     "sparkalog_store_anti_join",
+    "sparkalog_store_load_binary_u32",
+    "sparkalog_catalog_create",
+    "sparkalog_catalog_destroy",
+    "sparkalog_catalog_intern_u32",
+    "sparkalog_catalog_decode_u32",
+    "sparkalog_catalog_size",
     "sparkalog_executor_compile",
     "sparkalog_executor_step",
     "sparkalog_store_append",
@@ -110,6 +116,13 @@ class KernelStatsC(ctypes.Structure):
     ]
 
 
+class LoadErrorC(ctypes.Structure):
+    """sparkalog_load_error."""
+
+    _fields_ = [("kind", ctypes.c_int32), ("column", ctypes.c_uint32), ("line", ctypes.c_uint64),
+                ("field_offset", ctypes.c_uint64), ("field_length", ctypes.c_uint64)]
+
+
 class RoundTraceC(ctypes.Structure):
     """sparkalog_round_trace."""
 
@@ -171,6 +184,19 @@ def load() -> ctypes.CDLL:
     L.sparkalog_store_read.restype = i
     L.sparkalog_store_anti_join.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]
     L.sparkalog_store_anti_join.restype = i
+    L.sparkalog_store_load_binary_u32.argtypes = [vp, ctypes.c_uint32, vp, ctypes.c_size_t, i, i, c_sizep,
+                                                   ctypes.POINTER(LoadErrorC)]
+    L.sparkalog_store_load_binary_u32.restype = i
+    L.sparkalog_catalog_create.argtypes = [vp, ctypes.POINTER(vp)]
+    L.sparkalog_catalog_create.restype = i
+    L.sparkalog_catalog_destroy.argtypes = [vp]
+    L.sparkalog_catalog_destroy.restype = None
+    L.sparkalog_catalog_intern_u32.argtypes = [vp, vp, ctypes.c_size_t, i, vp, c_sizep]
+    L.sparkalog_catalog_intern_u32.restype = i
+    L.sparkalog_catalog_decode_u32.argtypes = [vp, vp, ctypes.c_size_t, i, vp]
+    L.sparkalog_catalog_decode_u32.restype = i
+    L.sparkalog_catalog_size.argtypes = [vp, c_sizep]
+    L.sparkalog_catalog_size.restype = i
     L.sparkalog_executor_step.argtypes = [vp, vp, ctypes.c_size_t, ctypes.POINTER(SccSummaryC),
                                           ctypes.POINTER(ctypes.c_int)]
     L.sparkalog_executor_step.restype = i

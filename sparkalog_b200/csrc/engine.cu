@@ -28,6 +28,7 @@
 #include "spk_radix.cuh"
 #include "spk_fused.cuh"
 #include "spk_member.cuh"
+#include "spk_ingest.cuh"
 #include "spk_setops.cuh"
 
 #include <algorithm>
@@ -842,6 +843,171 @@ int sparkalog_reserve_device_memory(size_t bytes, void* stream) {
     return 0;
 }
 
+// ---------------------------------------------------------------------------
+// Value catalog on the device (ValueCatalog, crates/sparkalog-datalog/src/
+// catalog.rs:98-127): see the interning kernels in spk_ingest.cuh.
+// ---------------------------------------------------------------------------
+struct sparkalog_catalog {
+    cudaStream_t stream = nullptr;
+    sparkalog_executor ex;          // radix-sort scratch and look-back epochs (no rules)
+    DevArray keys, keys_spare;      // (value << 32 | id), sorted by value
+    DevArray dict;                  // id -> value
+    DevArray a, b, list_a, list_b;  // sort buffers
+    DevArray staging, ids;          // host input / output staging, ids of a batch
+    DevArray words;                 // u64 new-value count, then the u32 error word
+    DevArray splits;                // merge diagonals
+    u64 size = 0;
+    u64* host = nullptr;            // pinned 64 bytes
+};
+
+namespace {
+
+// Radix-sorts n packed keys held in x (y is the other buffer); returns the one
+// holding the sorted keys.
+int catalog_sort(sparkalog_catalog* c, DevArray& x, DevArray& y, u64 n, u32* err, DevArray** sorted) {
+    cudaStream_t s = c->stream;
+    int rc = radix_sort(x.as<u64>(), y.as<u64>(), nullptr, n, c->ex.index_sort, &c->ex, err, s, nullptr, nullptr);
+    if (rc) return rc;
+    u32* sel = reinterpret_cast<u32*>(c->host + 4);
+    SPK_CUDA(cudaMemcpyAsync(sel, &c->ex.index_sort.plan.as<spk::RadixPlan>()->final_sel, 4, cudaMemcpyDeviceToHost,
+                             s),
+             "cudaMemcpyAsync");
+    SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    *sorted = *sel ? &y : &x;
+    return 0;
+}
+
+}  // namespace
+
+int sparkalog_catalog_create(void* stream, sparkalog_catalog** out) {
+    if (!out) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null output");
+    auto* c = new sparkalog_catalog();
+    c->stream = static_cast<cudaStream_t>(stream);
+    cudaError_t e = c->words.ensure(256, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->words.ptr, 0, 256, c->stream);
+    if (e == cudaSuccess) e = cudaMallocHost(&c->host, 64);
+    if (e != cudaSuccess) {
+        c->words.release(c->stream);
+        delete c;
+        return cuda_fail(e, "sparkalog_catalog_create");
+    }
+    *out = c;
+    return 0;
+}
+
+void sparkalog_catalog_destroy(sparkalog_catalog* c) {
+    if (!c) return;
+    cudaStream_t s = c->stream;
+    for (DevArray* d : {&c->keys, &c->keys_spare, &c->dict, &c->a, &c->b, &c->list_a, &c->list_b, &c->staging,
+                        &c->ids, &c->words, &c->splits, &c->ex.index_sort.plan, &c->ex.index_sort.status})
+        d->release(s);
+    cudaStreamSynchronize(s);
+    if (c->host) cudaFreeHost(c->host);
+    delete c;
+}
+
+int sparkalog_catalog_size(sparkalog_catalog* c, size_t* size) {
+    if (!c || !size) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null argument");
+    *size = c->size;
+    return 0;
+}
+
+int sparkalog_catalog_intern_u32(sparkalog_catalog* c, const u32* values, size_t n, int location, u32* ids,
+                                 size_t* size) {
+    if (!c || (n && (!values || !ids))) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null argument");
+    if (n > kMaxRelationRows) return fail(SPARKALOG_E_TOO_MANY_ROWS, "more than 2^32 - 1 values in one batch");
+    cudaStream_t s = c->stream;
+    if (n) {
+        u32* err = reinterpret_cast<u32*>(c->words.as<u64>() + 1);
+        unsigned long long* new_count = reinterpret_cast<unsigned long long*>(c->words.as<u64>());
+        SPK_CUDA(cudaMemsetAsync(c->words.ptr, 0, 16, s), "cudaMemsetAsync");
+        const u32* dvalues = values;
+        if (location == SPARKALOG_HOST) {
+            SPK_CUDA(c->staging.ensure(n * 4, s), "cudaMallocAsync");
+            SPK_CUDA(cudaMemcpyAsync(c->staging.ptr, values, n * 4, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
+            dvalues = c->staging.as<u32>();
+        }
+        SPK_CUDA(c->a.ensure(n * 8, s), "cudaMallocAsync");
+        SPK_CUDA(c->b.ensure(n * 8, s), "cudaMallocAsync");
+        spk::value_positions_kernel<<<simple_grid(n), 256, 0, s>>>(dvalues, n, c->a.as<u64>());
+        SPK_CUDA(cudaGetLastError(), "value_positions_kernel");
+        DevArray* sorted = nullptr;
+        int rc = catalog_sort(c, c->a, c->b, n, err, &sorted);
+        if (rc) return rc;
+        // Values the catalog lacks, with their first positions.
+        SPK_CUDA(c->list_a.ensure(n * 8, s), "cudaMallocAsync");
+        SPK_CUDA(c->list_b.ensure(n * 8, s), "cudaMallocAsync");
+        spk::new_value_heads_kernel<<<simple_grid(n), 256, 0, s>>>(sorted->as<u64>(), n, c->keys.as<u64>(), c->size,
+                                                                   c->list_a.as<u64>(), new_count);
+        SPK_CUDA(cudaGetLastError(), "new_value_heads_kernel");
+        SPK_CUDA(cudaMemcpyAsync(c->host, new_count, 8, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+        SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+        const u64 m = c->host[0];
+        if (c->size + m > kMaxRelationRows) return fail(SPARKALOG_E_TOO_MANY_ROWS, "more than 2^32 - 1 values");
+        if (m) {
+            DevArray* by_position = nullptr;
+            rc = catalog_sort(c, c->list_a, c->list_b, m, err, &by_position);
+            if (rc) return rc;
+            DevArray& pairs = by_position == &c->list_a ? c->list_b : c->list_a;
+            SPK_CUDA(c->dict.ensure((c->size + m) * 4, s, c->size * 4), "cudaMallocAsync");
+            spk::assign_new_ids_kernel<<<simple_grid(m), 256, 0, s>>>(by_position->as<u64>(), m, c->size,
+                                                                      pairs.as<u64>(), c->dict.as<u32>());
+            SPK_CUDA(cudaGetLastError(), "assign_new_ids_kernel");
+            DevArray& other = &pairs == &c->list_a ? c->list_b : c->list_a;
+            DevArray* sorted_pairs = nullptr;
+            rc = catalog_sort(c, pairs, other, m, err, &sorted_pairs);
+            if (rc) return rc;
+            SPK_CUDA(c->keys_spare.ensure((c->size + m) * 8, s), "cudaMallocAsync");
+            SPK_CUDA(launch_merge(c->keys.as<u64>(), c->size, sorted_pairs->as<u64>(), m, c->keys_spare.as<u64>(),
+                                  c->splits, s),
+                     "merge_disjoint_kernel");
+            swap_arrays(c->keys, c->keys_spare);
+            c->size += m;
+        }
+        u32* dids = ids;
+        if (location == SPARKALOG_HOST) {
+            SPK_CUDA(c->ids.ensure(n * 4, s), "cudaMallocAsync");
+            dids = c->ids.as<u32>();
+        }
+        spk::lookup_ids_kernel<8><<<simple_grid((n + 7) / 8), 256, 0, s>>>(sorted->as<u64>(), n, c->keys.as<u64>(),
+                                                                          c->size, dids, err);
+        SPK_CUDA(cudaGetLastError(), "lookup_ids_kernel");
+        if (location == SPARKALOG_HOST)
+            SPK_CUDA(cudaMemcpyAsync(ids, dids, n * 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+        SPK_CUDA(cudaMemcpyAsync(c->host + 1, err, 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+        SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+        const u32 bits = static_cast<u32>(c->host[1] & 0xffffffffu);
+        if (bits) return fail(SPARKALOG_E_DEVICE_FAULT, "device error bits " + std::to_string(bits));
+    }
+    if (size) *size = c->size;
+    return 0;
+}
+
+int sparkalog_catalog_decode_u32(sparkalog_catalog* c, const u32* ids, size_t n, int location, u32* values) {
+    if (!c || (n && (!values || !ids))) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null argument");
+    if (n == 0) return 0;
+    cudaStream_t s = c->stream;
+    u32* err = reinterpret_cast<u32*>(c->words.as<u64>() + 1);
+    SPK_CUDA(cudaMemsetAsync(err, 0, 4, s), "cudaMemsetAsync");
+    const u32* dids = ids;
+    u32* dvalues = values;
+    if (location == SPARKALOG_HOST) {
+        SPK_CUDA(c->staging.ensure(n * 4, s), "cudaMallocAsync");
+        SPK_CUDA(c->ids.ensure(n * 4, s), "cudaMallocAsync");
+        SPK_CUDA(cudaMemcpyAsync(c->staging.ptr, ids, n * 4, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
+        dids = c->staging.as<u32>();
+        dvalues = c->ids.as<u32>();
+    }
+    spk::decode_ids_kernel<<<simple_grid(n), 256, 0, s>>>(dids, n, c->dict.as<u32>(), c->size, dvalues, err);
+    SPK_CUDA(cudaGetLastError(), "decode_ids_kernel");
+    if (location == SPARKALOG_HOST)
+        SPK_CUDA(cudaMemcpyAsync(values, dvalues, n * 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+    SPK_CUDA(cudaMemcpyAsync(c->host + 1, err, 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+    SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    if (c->host[1] & 0xffffffffu) return fail(SPARKALOG_E_INVALID_ARGUMENT, "value id outside the catalog");
+    return 0;
+}
+
 int sparkalog_store_create(void* stream, sparkalog_store** out) {
     if (!out) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null output pointer");
     auto* st = new sparkalog_store();
@@ -933,6 +1099,164 @@ int sparkalog_store_insert_recursive(sparkalog_store* st, u32 id, const u32* ful
     SPK_CUDA(r.newt.ensure(4096, st->stream), "cudaMallocAsync");
     st->relations[id] = std::move(r);
     return 0;
+}
+
+namespace {
+
+// Host re-parse of the one line the device reported as failing, for the
+// error's details (the same rules as spk::parse_line).
+void describe_load_error(const unsigned char* line, u64 line_offset, u64 len, sparkalog_load_error* e) {
+    auto space = [](unsigned char c) { return c == ' ' || c == '\t' || c == '\n' || c == '\v' || c == '\f' || c == '\r'; };
+    u64 b = 0, end = len;
+    while (b < end && space(line[b])) ++b;
+    while (end > b && space(line[end - 1])) --end;
+    u64 fb[3] = {0, 0, 0}, fe[3] = {0, 0, 0};
+    int fields = 0;
+    for (u64 p = b; p < end;) {
+        while (p < end && space(line[p])) ++p;
+        if (p == end) break;
+        const u64 q = p;
+        while (p < end && !space(line[p])) ++p;
+        if (fields < 3) {
+            fb[fields] = q;
+            fe[fields] = p;
+        }
+        if (++fields > 2) break;
+    }
+    if (fields != 2) {
+        e->kind = SPARKALOG_LOAD_INVALID_FIELD_COUNT;
+        return;
+    }
+    for (int c = 0; c < 2; ++c) {
+        u64 i = fb[c];
+        if (i < fe[c] && line[i] == '+') ++i;
+        bool ok = i < fe[c];
+        u64 v = 0;
+        for (; ok && i < fe[c]; ++i) {
+            ok = line[i] >= '0' && line[i] <= '9';
+            v = v * 10 + (line[i] - '0');
+            ok = ok && v <= 0xffffffffull;
+        }
+        if (!ok) {
+            e->kind = SPARKALOG_LOAD_INVALID_U32;
+            e->column = static_cast<u32>(c + 1);
+            e->field_offset = line_offset + fb[c];
+            e->field_length = fe[c] - fb[c];
+            return;
+        }
+    }
+}
+
+}  // namespace
+
+int sparkalog_store_load_binary_u32(sparkalog_store* st, u32 id, const char* text, size_t bytes, int location,
+                                    int recursive, size_t* rows, sparkalog_load_error* error) {
+    if (!st || !rows || (bytes && !text)) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null argument");
+    if (st->find(id)) return fail(SPARKALOG_E_DUPLICATE, "relation " + std::to_string(id) + " is already registered");
+    if (error) *error = sparkalog_load_error{};
+    *rows = 0;
+    cudaStream_t s = st->stream;
+    StoreOps* ops_ptr = store_ops(st);
+    if (!ops_ptr) return static_cast<int>(cudaErrorMemoryAllocation);
+    StoreOps& ops = *ops_ptr;
+    u32* err = ops.counters.as<u32>() + 32;
+    // The text on the device (ops.b holds it for a host text).
+    const unsigned char* dtext = reinterpret_cast<const unsigned char*>(text);
+    if (location == SPARKALOG_HOST && bytes) {
+        SPK_CUDA(ops.b.ensure(bytes, s), "cudaMallocAsync");
+        SPK_CUDA(cudaMemcpyAsync(ops.b.ptr, text, bytes, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
+        dtext = ops.b.as<unsigned char>();
+    }
+    // Pass 0: count '\n' to size the line ends; pass 1: their positions.
+    unsigned long long* dcount = reinterpret_cast<unsigned long long*>(ops.counts.as<u64>());
+    SPK_CUDA(cudaMemsetAsync(ops.counts.ptr, 0, 64, s), "cudaMemsetAsync");
+    if (bytes) {
+        spk::count_newlines_kernel<<<simple_grid(bytes), 256, 0, s>>>(dtext, bytes, dcount);
+        SPK_CUDA(cudaGetLastError(), "count_newlines_kernel");
+    }
+    SPK_CUDA(cudaMemcpyAsync(ops.host, dcount, 8, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+    SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    const u64 newlines = ops.host[0];
+    unsigned char last = 0;
+    if (bytes) {
+        if (location == SPARKALOG_HOST) {
+            last = static_cast<unsigned char>(text[bytes - 1]);
+        } else {
+            SPK_CUDA(cudaMemcpyAsync(&last, dtext + bytes - 1, 1, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+            SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+        }
+    }
+    const u64 lines = newlines + ((bytes && last != '\n') ? 1 : 0);
+    constexpr int kByteItems = 16, kLineItems = 8;
+    const u64 byte_tiles = (bytes + kThreads * kByteItems - 1) / (kThreads * kByteItems);
+    const u64 line_tiles = (lines + kSetTile - 1) / kSetTile;
+    SPK_CUDA(ops.a.ensure(std::max<u64>(newlines, 1) * 8, s), "cudaMallocAsync");
+    SPK_CUDA(ops.status.ensure_zeroed((std::max(byte_tiles, line_tiles) + 1) * 8, s), "cudaMallocAsync");
+    SPK_CUDA(st->scratch_u32[0].ensure(std::max<u64>(lines, 1) * 4, s), "cudaMallocAsync");
+    SPK_CUDA(st->scratch_u32[1].ensure(std::max<u64>(lines, 1) * 4, s), "cudaMallocAsync");
+    SPK_CUDA(cudaMemsetAsync(ops.counters.ptr, 0, 33 * 4, s), "cudaMemsetAsync");  // tile counters + error word
+    SPK_CUDA(cudaMemsetAsync(ops.counts.as<u64>() + 2, 0xff, 16, s), "cudaMemsetAsync");
+    u64* ends_n = ops.counts.as<u64>() + 1;
+    unsigned long long* first_error = reinterpret_cast<unsigned long long*>(ops.counts.as<u64>() + 2);
+    u64* out_n = ops.counts.as<u64>() + 4;
+    {
+        auto kernel = spk::line_ends_kernel<kThreads, kByteItems>;
+        kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, std::max<u64>(byte_tiles, 1)), kThreads, 0,
+                 s>>>(dtext, bytes, ops.a.as<u64>(), ends_n, ops.status.as<u64>(), ops.counters.as<u32>(),
+                      ops.ex.epoch++, err);
+        SPK_CUDA(cudaGetLastError(), "line_ends_kernel");
+    }
+    {
+        auto kernel = spk::parse_lines_kernel<kThreads, kLineItems>;
+        kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, std::max<u64>(line_tiles, 1)), kThreads, 0,
+                 s>>>(dtext, bytes, ops.a.as<u64>(), ends_n, lines, st->scratch_u32[0].as<u32>(),
+                      st->scratch_u32[1].as<u32>(), out_n, first_error, ops.status.as<u64>(),
+                      ops.counters.as<u32>() + 1, ops.ex.epoch++, err);
+        SPK_CUDA(cudaGetLastError(), "parse_lines_kernel");
+    }
+    SPK_CUDA(cudaMemcpyAsync(ops.host, ops.counts.as<u64>() + 2, 24, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+    SPK_CUDA(cudaMemcpyAsync(ops.host + 3, err, 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+    SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    const u64 field_error = ops.host[0], lfs_line = ops.host[1], parsed = ops.host[2];
+    const u32 bits = static_cast<u32>(ops.host[3] & 0xffffffffu);
+    if (bits) return fail(SPARKALOG_E_DEVICE_FAULT, "device error bits " + std::to_string(bits));
+    if (lfs_line != spk::kNoLine || field_error != spk::kNoLine) {
+        sparkalog_load_error e{};
+        if (lfs_line != spk::kNoLine) {
+            // count_rows (io.rs:92-105) meets the pointer header before any field is parsed.
+            e.kind = SPARKALOG_LOAD_GIT_LFS_POINTER;
+            e.line = lfs_line + 1;
+        } else {
+            // The failing line's bytes, re-read on the host for the details.
+            u64 bounds[2] = {0, bytes};
+            if (field_error > 0)
+                SPK_CUDA(cudaMemcpyAsync(&bounds[0], ops.a.as<u64>() + field_error - 1, 8, cudaMemcpyDeviceToHost, s),
+                         "cudaMemcpyAsync");
+            if (field_error < newlines)
+                SPK_CUDA(cudaMemcpyAsync(&bounds[1], ops.a.as<u64>() + field_error, 8, cudaMemcpyDeviceToHost, s),
+                         "cudaMemcpyAsync");
+            SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+            if (field_error > 0) bounds[0] += 1;
+            std::vector<unsigned char> line(bounds[1] - bounds[0]);
+            if (!line.empty())
+                SPK_CUDA(cudaMemcpy(line.data(), dtext + bounds[0], line.size(), cudaMemcpyDefault), "cudaMemcpy");
+            e.line = field_error + 1;
+            describe_load_error(line.data(), bounds[0], line.size(), &e);
+        }
+        if (error) *error = e;
+        return fail(SPARKALOG_E_LOAD, e.kind == SPARKALOG_LOAD_GIT_LFS_POINTER
+                                          ? "the text is a Git LFS pointer, not materialized graph data"
+                                          : "line " + std::to_string(e.line) +
+                                                (e.kind == SPARKALOG_LOAD_INVALID_FIELD_COUNT
+                                                     ? " does not contain exactly two fields"
+                                                     : ", column " + std::to_string(e.column) + " is not a u32"));
+    }
+    if (parsed > kMaxRelationRows) return fail(SPARKALOG_E_TOO_MANY_ROWS, "too many rows for u32 row ids");
+    *rows = parsed;
+    const u32* c0 = st->scratch_u32[0].as<u32>();
+    const u32* c1 = st->scratch_u32[1].as<u32>();
+    return recursive ? sparkalog_store_insert_recursive(st, id, c0, c1, parsed, c0, c1, parsed, SPARKALOG_DEVICE)
+                     : sparkalog_store_insert_static(st, id, c0, c1, parsed, SPARKALOG_DEVICE);
 }
 
 int sparkalog_store_rows(sparkalog_store* st, u32 id, int version, size_t* rows) {

@@ -74,6 +74,79 @@ class GeneralSccSummary:
     new_rows: int
 
 
+class ValueCatalog:
+    """ValueCatalog (crates/sparkalog-datalog/src/catalog.rs:98-127) for u32 values, kept on
+    the GPU: ``intern`` numbers unseen values by first appearance after the current size,
+    ``decode`` maps ids back (Database::query's decode). Arrays may be NumPy (host) or
+    CUDA tensors; results come back in the same kind."""
+
+    def __init__(self, stream=None):
+        import ctypes
+
+        import torch
+
+        from . import _native
+
+        self._torch, self._ctypes, self._native = torch, ctypes, _native
+        self._stream = stream if stream is not None else torch.cuda.current_stream()
+        h = ctypes.c_void_p()
+        self._check(_native.load().sparkalog_catalog_create(self._stream.cuda_stream, ctypes.byref(h)))
+        self._h = h
+
+    def _check(self, code: int) -> None:
+        if code != 0:
+            from .recursion import GenericExecutionError
+
+            raise GenericExecutionError(code, self._native.last_error())
+
+    def _call(self, fn, array):
+        torch, ctypes = self._torch, self._ctypes
+        if isinstance(array, torch.Tensor):
+            out = torch.empty_like(array)
+            fn(array.data_ptr(), array.numel(), 1, out.data_ptr())
+            return out
+        a = np.ascontiguousarray(np.asarray(array, dtype=np.uint32))
+        out = np.empty_like(a)
+        fn(a.ctypes.data if len(a) else None, len(a), 0, out.ctypes.data if len(a) else None)
+        return out
+
+    def intern(self, values):
+        L, size = self._native.load(), self._ctypes.c_size_t(0)
+        return self._call(lambda p, n, loc, o: self._check(
+            L.sparkalog_catalog_intern_u32(self._h, p, n, loc, o, self._ctypes.byref(size))), values)
+
+    def intern_rows(self, first, second):
+        """Interns a binary relation row by row (Database::insert order: row[0], row[1], next row)."""
+        torch = self._torch
+        if isinstance(first, torch.Tensor):
+            ids = self.intern(torch.stack([first, second], dim=1).reshape(-1))
+            return ids[0::2].contiguous(), ids[1::2].contiguous()
+        both = np.stack([np.asarray(first, dtype=np.uint32), np.asarray(second, dtype=np.uint32)], axis=1)
+        ids = self.intern(both.reshape(-1))
+        return ids[0::2].copy(), ids[1::2].copy()
+
+    def decode(self, ids):
+        L = self._native.load()
+        return self._call(lambda p, n, loc, o: self._check(L.sparkalog_catalog_decode_u32(self._h, p, n, loc, o)),
+                          ids)
+
+    def __len__(self) -> int:
+        size = self._ctypes.c_size_t(0)
+        self._check(self._native.load().sparkalog_catalog_size(self._h, self._ctypes.byref(size)))
+        return int(size.value)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._native.load().sparkalog_catalog_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def _pack(pairs: np.ndarray) -> np.ndarray:
     return (pairs[:, 0].astype(np.uint64) << np.uint64(32)) | pairs[:, 1].astype(np.uint64)
 

@@ -30,7 +30,7 @@ class GenericExecutionError(RuntimeError):
         -1: "Missing", -2: "Duplicate", -3: "NotRecursive", -4: "EmptyScc", -5: "DuplicateSccRelation",
         -6: "DeltaOutsideScc", -7: "TargetOutsideScc", -8: "IncompatibleTargetPlans", -9: "MissingRuleTarget",
         -10: "IterationLimit", -11: "TooManyRows", -12: "MissingPlanColumn", -20: "DeviceFault",
-        -21: "InvalidArgument", -22: "UnsortedFull",
+        -21: "InvalidArgument", -22: "UnsortedFull", -23: "Load",
     }
 
     def __init__(self, code: int, message: str):
@@ -40,6 +40,19 @@ class GenericExecutionError(RuntimeError):
 
 
 RelationStoreError = GenericExecutionError
+
+
+class LoadError(GenericExecutionError):
+    """storage::LoadError (crates/sparkalog-storage/src/io.rs:7-20): ``kind`` is
+    GitLfsPointer, InvalidFieldCount or InvalidU32, with the 1-based ``line`` and,
+    for InvalidU32, the ``column`` and the field's text ``value``."""
+
+    LOAD_KINDS = {1: "GitLfsPointer", 2: "InvalidFieldCount", 3: "InvalidU32"}
+
+    def __init__(self, code: int, message: str, kind: int, line: int, column: int, value: str | None):
+        super().__init__(code, message)
+        self.kind = self.LOAD_KINDS.get(kind, "Load")
+        self.line, self.column, self.value = line, column, value
 
 
 def _check(code: int) -> None:
@@ -141,6 +154,31 @@ class RelationStore:
         ids = [int(getattr(r, "value", r)) for r in (left, right, out)]
         _check(_native.load().sparkalog_store_anti_join(self._h, *ids))
         return self.rows(ids[2])
+
+    def load_binary_u32(self, rid: RelationId | int, text, recursive: bool = False) -> int:
+        """Parses whitespace-separated u32 pairs on the GPU and inserts them as relation
+        ``rid`` (load_binary_u32, crates/sparkalog-storage/src/io.rs:72-141); ``text``
+        is bytes, str, or a uint8 CUDA tensor. Returns the number of rows read."""
+        L = _native.load()
+        if isinstance(text, str):
+            text = text.encode()
+        if isinstance(text, torch.Tensor):
+            ptr, nbytes, loc, host = text.data_ptr(), int(text.numel()), DEVICE, None
+        else:
+            host = np.frombuffer(bytes(text), dtype=np.uint8)
+            ptr, nbytes, loc = host.ctypes.data if len(host) else None, len(host), HOST
+        rows = ctypes.c_size_t(0)
+        err = _native.LoadErrorC()
+        code = L.sparkalog_store_load_binary_u32(self._h, int(getattr(rid, "value", rid)), ptr, nbytes, loc,
+                                                 1 if recursive else 0, ctypes.byref(rows), ctypes.byref(err))
+        if code == -23:
+            value = None
+            if err.kind == 3:
+                raw = host if host is not None else text.cpu().numpy()
+                value = bytes(raw[err.field_offset:err.field_offset + err.field_length]).decode(errors="replace")
+            raise LoadError(code, _native.last_error(), err.kind, int(err.line), int(err.column), value)
+        _check(code)
+        return int(rows.value)
 
     def append(self, rid: RelationId | int, relation) -> None:
         """FULL u= rows (and DELTA u= the genuinely new rows of a recursive relation),

@@ -193,3 +193,23 @@ def test_filter_known_answers(known_answers):
             assert oracle.filter_serial(case["values"], op, operand).tolist() == want, case["source"]
             assert oracle.filter_parallel(case["values"], op, operand).tolist() == want, case["source"]
     assert oracle.filter_serial([1, 2, 3], 9, 1).tolist() == []  # unknown operation code: no rows
+
+
+def test_load_binary_u32_known_answers(known_answers):
+    # io.rs:145-174, plus the u32 syntax of str::parse and the line rules.
+    for case in known_answers["load_binary_u32"]:
+        if "error" in case:
+            with pytest.raises(oracle.OracleLoadError) as e:
+                oracle.load_binary_u32(case["text"].encode())
+            assert e.value.kind == case["error"] and e.value.line == case.get("line", 0)
+        else:
+            f, s = oracle.load_binary_u32(case["text"].encode())
+            assert f.tolist() == case["first"] and s.tolist() == case["second"]
+    f, s = oracle.load_binary_u32(b"+7 007\r\n  \t8\t9  \n4294967295 0")
+    assert f.tolist() == [7, 8, 4294967295] and s.tolist() == [7, 9, 0]
+    for text, kind, line, column in [(b"1 2\n1 -2\n", "InvalidU32", 2, 2), (b"1 4294967296\n", "InvalidU32", 1, 2),
+                                      (b"x 1\n", "InvalidU32", 1, 1), (b"1\n", "InvalidFieldCount", 1, 0),
+                                      (b"1 2\n3 + \n", "InvalidU32", 2, 2)]:
+        with pytest.raises(oracle.OracleLoadError) as e:
+            oracle.load_binary_u32(text)
+        assert (e.value.kind, e.value.line, e.value.column) == (kind, line, column)
