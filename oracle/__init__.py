@@ -74,6 +74,12 @@ def lib() -> ctypes.CDLL:
         if not LIB_PATH.exists():
             build()
         L = ctypes.CDLL(str(LIB_PATH))
+        L.oracle_load_binary_u32.restype = ctypes.c_int
+        L.oracle_load_binary_u32.argtypes = [ctypes.c_char_p, ctypes.c_uint64, _u32p, _u32p, ctypes.c_uint64,
+                                             ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
+                                             ctypes.POINTER(ctypes.c_int)]
+        L.oracle_intern_u32.restype = None
+        L.oracle_intern_u32.argtypes = [_u32p, ctypes.c_uint64, _u32p]
         L.oracle_splitmix64.restype = ctypes.c_uint64
         L.oracle_splitmix64.argtypes = [ctypes.c_uint64, ctypes.c_uint64]
         L.oracle_er_edges.restype = ctypes.c_uint64
@@ -592,3 +598,25 @@ def intern(values, catalog: dict | None = None) -> tuple[np.ndarray, dict]:
             catalog[v] = len(catalog)
         out[i] = catalog[v]
     return out, catalog
+
+
+def load_binary_u32_c(data: bytes) -> tuple[np.ndarray, np.ndarray]:
+    """The C restatement of load_binary_u32 (oracle.cpp), for large texts and timing."""
+    cap = data.count(b"\n") + 1
+    first = np.empty(cap, dtype=np.uint32)
+    second = np.empty(cap, dtype=np.uint32)
+    rows, line, column = ctypes.c_uint64(0), ctypes.c_uint64(0), ctypes.c_int(0)
+    rc = lib().oracle_load_binary_u32(data, len(data), _p32(first), _p32(second), cap, ctypes.byref(rows),
+                                      ctypes.byref(line), ctypes.byref(column))
+    if rc:
+        raise OracleLoadError({1: "GitLfsPointer", 2: "InvalidFieldCount", 3: "InvalidU32"}[rc], int(line.value),
+                              int(column.value) if rc == 3 else 0)
+    return first[:rows.value].copy(), second[:rows.value].copy()
+
+
+def intern_c(values) -> np.ndarray:
+    """The C restatement of ValueCatalog::intern over one batch (oracle.cpp)."""
+    v = np.ascontiguousarray(np.asarray(values, dtype=np.uint32))
+    out = np.empty_like(v)
+    lib().oracle_intern_u32(_p32(v), len(v), _p32(out))
+    return out

@@ -23,6 +23,7 @@
 #include <string>
 #include <thread>
 #include <vector>
+#include <unordered_map>
 
 namespace {
 
@@ -700,6 +701,98 @@ int oracle_run_scc(void* s, const u32* relations, u64 n_relations, const oracle_
     *iterations_out = iterations;
     *total_new_out = total_new;
     return 0;
+}
+
+// load_binary_u32 (crates/sparkalog-storage/src/io.rs:72-138) on one thread,
+// the way the reference reads a graph: count_rows (a Git LFS pointer header
+// anywhere is an error), then populate_columns line by line. Returns 0, or
+// 1 (Git LFS pointer), 2 (field count), 3 (invalid u32) with *line (1-based)
+// and *column. The columns must hold `capacity` rows.
+int oracle_load_binary_u32(const char* text, u64 bytes, uint32_t* first, uint32_t* second, u64 capacity, u64* rows,
+                           u64* line_out, int* column_out) {
+    auto space = [](char c) { return c == ' ' || c == '\t' || c == '\n' || c == '\v' || c == '\f' || c == '\r'; };
+    static const char kLfs[] = "version https://git-lfs.github.com/spec/v1";
+    auto for_lines = [&](auto&& visit) -> int {
+        u64 b = 0, index = 0;
+        while (b < bytes) {
+            u64 e = b;
+            while (e < bytes && text[e] != '\n') ++e;
+            int rc = visit(b, e, index);
+            if (rc) return rc;
+            ++index;
+            b = e + 1;
+        }
+        return 0;
+    };
+    auto trim = [&](u64& b, u64& e) {
+        while (b < e && space(text[b])) ++b;
+        while (e > b && space(text[e - 1])) --e;
+    };
+    int rc = for_lines([&](u64 b, u64 e, u64) {
+        trim(b, e);
+        if (b == e || text[b] == '#' || text[b] == '%') return 0;
+        if (e - b == sizeof(kLfs) - 1 && std::memcmp(text + b, kLfs, e - b) == 0) return 1;
+        return 0;
+    });
+    if (rc) {
+        *line_out = 0;
+        return rc;
+    }
+    u64 n = 0;
+    return for_lines([&](u64 b, u64 e, u64 index) {
+        trim(b, e);
+        if (b == e || text[b] == '#' || text[b] == '%') return 0;
+        u64 fb[2] = {0, 0}, fe[2] = {0, 0};
+        int fields = 0;
+        for (u64 p = b; p < e;) {
+            while (p < e && space(text[p])) ++p;
+            if (p == e) break;
+            const u64 q = p;
+            while (p < e && !space(text[p])) ++p;
+            if (fields < 2) {
+                fb[fields] = q;
+                fe[fields] = p;
+            }
+            if (++fields > 2) break;
+        }
+        *line_out = index + 1;
+        if (fields != 2) return 2;
+        uint32_t v[2];
+        for (int c = 0; c < 2; ++c) {
+            u64 i = fb[c];
+            if (i < fe[c] && text[i] == '+') ++i;
+            bool ok = i < fe[c];
+            u64 x = 0;
+            for (; ok && i < fe[c]; ++i) {
+                ok = text[i] >= '0' && text[i] <= '9';
+                x = x * 10 + static_cast<u64>(text[i] - '0');
+                ok = ok && x <= 0xffffffffull;
+            }
+            if (!ok) {
+                *column_out = c + 1;
+                return 3;
+            }
+            v[c] = static_cast<uint32_t>(x);
+        }
+        if (n < capacity) {
+            first[n] = v[0];
+            second[n] = v[1];
+        }
+        *rows = ++n;
+        return 0;
+    });
+}
+
+// ValueCatalog::intern (crates/sparkalog-datalog/src/catalog.rs:108-117) for
+// each value in order, with a hash map as the reference's HashMap.
+void oracle_intern_u32(const uint32_t* values, u64 n, uint32_t* ids) {
+    std::unordered_map<uint32_t, uint32_t> by_value;
+    by_value.reserve(n);
+    for (u64 i = 0; i < n; ++i) {
+        auto it = by_value.find(values[i]);
+        if (it == by_value.end()) it = by_value.emplace(values[i], static_cast<uint32_t>(by_value.size())).first;
+        ids[i] = it->second;
+    }
 }
 
 }  // extern "C"

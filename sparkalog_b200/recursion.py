@@ -165,7 +165,9 @@ class RelationStore:
         if isinstance(text, torch.Tensor):
             ptr, nbytes, loc, host = text.data_ptr(), int(text.numel()), DEVICE, None
         else:
-            host = np.frombuffer(bytes(text), dtype=np.uint8)
+            # bytes-like or a uint8 NumPy array (e.g. a pinned buffer): read in place.
+            host = text if isinstance(text, np.ndarray) else np.frombuffer(text, dtype=np.uint8)
+            host = np.ascontiguousarray(host.view(np.uint8).reshape(-1))
             ptr, nbytes, loc = host.ctypes.data if len(host) else None, len(host), HOST
         rows = ctypes.c_size_t(0)
         err = _native.LoadErrorC()

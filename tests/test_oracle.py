@@ -213,3 +213,22 @@ def test_load_binary_u32_known_answers(known_answers):
         with pytest.raises(oracle.OracleLoadError) as e:
             oracle.load_binary_u32(text)
         assert (e.value.kind, e.value.line, e.value.column) == (kind, line, column)
+
+
+def test_load_and_intern_c_restatements_agree():
+    # The C restatements (used for timing) equal the line-by-line Python ones.
+    rng = np.random.default_rng(9)
+    rows = rng.integers(0, 1 << 32, size=(20_000, 2), dtype=np.uint64)
+    lines = [("# c" if i % 13 == 0 else f"{a}\t+{b}\r" if i % 7 == 0 else f"{a} {b}") for i, (a, b) in enumerate(rows)]
+    text = "\n".join(lines).encode()
+    a = oracle.load_binary_u32(text)
+    b = oracle.load_binary_u32_c(text)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    for bad in (b"1 2\n3 x\n", b"1 2 3\n", b"version https://git-lfs.github.com/spec/v1\n"):
+        with pytest.raises(oracle.OracleLoadError) as e1:
+            oracle.load_binary_u32(bad)
+        with pytest.raises(oracle.OracleLoadError) as e2:
+            oracle.load_binary_u32_c(bad)
+        assert (e1.value.kind, e1.value.line, e1.value.column) == (e2.value.kind, e2.value.line, e2.value.column)
+    v = rng.integers(0, 5000, size=50_000).astype(np.uint32)
+    assert np.array_equal(oracle.intern(v)[0], oracle.intern_c(v))
