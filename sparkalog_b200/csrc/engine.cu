@@ -299,6 +299,17 @@ int refresh_directories(sparkalog_store* st, RelState& r, cudaStream_t s, u64* l
     return 0;
 }
 
+// Grows r.spare and level l's directory for a merged level of n rows (done
+// before the merge so that allocation stays out of its timing).
+int merge_buffers(sparkalog_store* st, RelState& r, int l, u64 n, cudaStream_t s) {
+    u32 shift;
+    u64 buckets;
+    directory_shape(st, n, &shift, &buckets);
+    SPK_CUDA(r.spare.ensure(n * 8, s), "cudaMallocAsync");
+    SPK_CUDA(r.dir[l].ensure((buckets + 1) * 4, s), "cudaMallocAsync");
+    return 0;
+}
+
 // Merges two disjoint sorted runs into level l of r (through r.spare) and
 // writes the merged level's directory on the way when the merge runs a kernel.
 int merge_into_level(sparkalog_store* st, RelState& r, int l, const u64* a, u64 na, const u64* b, u64 nb,
@@ -2135,9 +2146,11 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                 const u64 tn = tr.level_n[tail] + newt_n;
                 {
                     u64 launched = 0;
+                    int rc = merge_buffers(st, tr, tail, tn, s);
+                    if (rc) return rc;
                     const int tm = ex->begin(SPARKALOG_K_MERGE, s);
-                    int rc = merge_into_level(st, tr, tail, tr.level[tail].as<u64>(), tr.level_n[tail],
-                                              tr.newt.as<u64>(), newt_n, s, &launched);
+                    rc = merge_into_level(st, tr, tail, tr.level[tail].as<u64>(), tr.level_n[tail],
+                                          tr.newt.as<u64>(), newt_n, s, &launched);
                     if (rc) return rc;
                     ex->end(tm, s, 16.0 * static_cast<double>(tn), launched);
                     ex->stats.total_launches += launched;
@@ -2157,8 +2170,10 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                     }
                     const u64 mn = tr.level_n[l - 1] + tr.level_n[l];
                     u64 launched = 0;
+                    int rc = merge_buffers(st, tr, l - 1, mn, s);
+                    if (rc) return rc;
                     const int tm = ex->begin(SPARKALOG_K_MERGE, s);
-                    int rc = merge_into_level(st, tr, l - 1, tr.level[l - 1].as<u64>(), tr.level_n[l - 1],
+                    rc = merge_into_level(st, tr, l - 1, tr.level[l - 1].as<u64>(), tr.level_n[l - 1],
                                               tr.level[l].as<u64>(), tr.level_n[l], s, &launched);
                     if (rc) return rc;
                     ex->end(tm, s, 16.0 * static_cast<double>(mn), launched);
