@@ -74,7 +74,7 @@ constexpr int kLevelStage = 2048;  // level rows per shared-memory chunk of the 
 constexpr int kSparseThreads = 128;  // anti-join of small candidate sets
 constexpr int kSparseItems = 4;
 constexpr int kSparseTile = kSparseThreads * kSparseItems;
-constexpr u64 kSparseCandidates = 1ull << 22;
+constexpr u64 kSparseCandidates = 1ull << 26;
 constexpr int kMergeItems = 8;
 constexpr int kMergeTile = kThreads * kMergeItems;
 constexpr int kSortThreads = spk::RadixSortConfig::kThreads;

@@ -480,11 +480,21 @@ struct MergeDirectory {
 // every output row that starts a bucket (or a run of empty buckets) writes
 // the directory entries up to its bucket, so the merged level needs no
 // separate directory pass.
+// Shared-memory rows of a merge tile are padded by one slot every 8 rows: a
+// thread's merge walk starts ITEMS = 8 rows after its neighbour's, which
+// without padding puts the 32 lanes of a warp on 2 of the 32 banks.
+struct PaddedKeys {
+    const u64* keys;
+    u32 base;
+    __device__ __forceinline__ static u32 slot(u32 i) { return i + (i >> 3); }
+    __device__ __forceinline__ u64 operator()(u64 i) const { return keys[slot(base + static_cast<u32>(i))]; }
+};
+
 template <int THREADS, int ITEMS>
 __global__ void __launch_bounds__(THREADS) merge_disjoint_kernel(const u64* a, u64 na, const u64* b, u64 nb,
                                                                  const u64* splits, u64* out, MergeDirectory md) {
     constexpr int kTile = THREADS * ITEMS;
-    __shared__ __align__(16) u64 sm[kTile];
+    __shared__ __align__(16) u64 sm[kTile + kTile / 8];
     __shared__ u64 before_tile;  // the output row just before the tile
     const u64 total = na + nb;
     const u64 num_tiles = (total + kTile - 1) / kTile;
@@ -494,8 +504,8 @@ __global__ void __launch_bounds__(THREADS) merge_disjoint_kernel(const u64* a, u
         const u64 i0 = splits[tile], i1 = splits[tile + 1];
         const u64 j0 = d0 - i0, j1 = d1 - i1;
         const u32 sa_n = static_cast<u32>(i1 - i0), sb_n = static_cast<u32>(j1 - j0);
-        for (u32 t = threadIdx.x; t < sa_n; t += THREADS) cp_async_8(sm + t, a + i0 + t);
-        for (u32 t = threadIdx.x; t < sb_n; t += THREADS) cp_async_8(sm + sa_n + t, b + j0 + t);
+        for (u32 t = threadIdx.x; t < sa_n; t += THREADS) cp_async_8(sm + PaddedKeys::slot(t), a + i0 + t);
+        for (u32 t = threadIdx.x; t < sb_n; t += THREADS) cp_async_8(sm + PaddedKeys::slot(sa_n + t), b + j0 + t);
         cp_async_commit();
         if (md.dir && threadIdx.x == 0 && d0 > 0) {
             const u64 pa = i0 > 0 ? a[i0 - 1] : 0, pb = j0 > 0 ? b[j0 - 1] : 0;
@@ -503,7 +513,7 @@ __global__ void __launch_bounds__(THREADS) merge_disjoint_kernel(const u64* a, u
         }
         cp_async_wait<0>();
         __syncthreads();
-        const SmemKeys sa{sm}, sb{sm + sa_n};
+        const PaddedKeys sa{sm, 0}, sb{sm, sa_n};
         const u32 diag = threadIdx.x * ITEMS;
         const u32 len = static_cast<u32>(d1 - d0);
         u64 v[ITEMS];
@@ -521,15 +531,15 @@ __global__ void __launch_bounds__(THREADS) merge_disjoint_kernel(const u64* a, u
         __syncthreads();
 #pragma unroll
         for (int i = 0; i < ITEMS; ++i)
-            if (diag + i < len) sm[diag + i] = v[i];
+            if (diag + i < len) sm[PaddedKeys::slot(diag + i)] = v[i];
         __syncthreads();
-        for (u32 j = threadIdx.x; j < len; j += THREADS) out[d0 + j] = sm[j];
+        for (u32 j = threadIdx.x; j < len; j += THREADS) out[d0 + j] = sm[PaddedKeys::slot(j)];
         if (md.dir) {
             for (u32 j = threadIdx.x; j < len; j += THREADS) {
                 const u64 o = d0 + j;
-                const u64 bucket = sm[j] >> md.shift;
+                const u64 bucket = sm[PaddedKeys::slot(j)] >> md.shift;
                 u64 from = 0;
-                if (o > 0) from = ((j > 0 ? sm[j - 1] : before_tile) >> md.shift) + 1;
+                if (o > 0) from = ((j > 0 ? sm[PaddedKeys::slot(j - 1)] : before_tile) >> md.shift) + 1;
                 for (u64 e = from; e <= bucket && e <= md.buckets; ++e) md.dir[e] = static_cast<u32>(o);
                 if (o == total - 1)
                     for (u64 e = bucket + 1; e <= md.buckets; ++e) md.dir[e] = static_cast<u32>(total);
