@@ -156,6 +156,14 @@ class ClockSampler:
                  "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
         except (FileNotFoundError, OSError):
             self.proc = None
+        # nvidia-smi's start-up (NVML initialisation) can stall the GPU's work
+        # for tens of ms: wait for its first sample before the timed region.
+        deadline = time.time() + 5.0
+        while self.proc is not None and time.time() < deadline and self.proc.poll() is None:
+            self.file.flush()
+            if Path(self.file.name).read_text().count("\n") >= 1:
+                break
+            time.sleep(0.02)
         return self
 
     def __exit__(self, *exc):

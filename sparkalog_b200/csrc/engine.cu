@@ -32,6 +32,7 @@
 #include "spk_setops.cuh"
 
 #include <algorithm>
+#include <mutex>
 #include <atomic>
 #include <cstdio>
 #include <cstring>
@@ -55,6 +56,39 @@ int cuda_fail(cudaError_t st, const char* what) {
     g_last_error = std::string(what) + " failed with CUDA error " + std::to_string(static_cast<int>(st)) + " (" +
                    cudaGetErrorString(st) + ")";
     return static_cast<int>(st);
+}
+
+// Small pinned host buffers (counts, error words) are recycled per size class
+// instead of freed: cudaFreeHost synchronises the whole device and unpins
+// pages, which would make every store or executor teardown a device-wide
+// barrier.
+std::mutex g_pinned_mu;
+std::map<size_t, std::vector<void*>> g_pinned_free;
+
+size_t pinned_class(size_t bytes) {
+    size_t c = 256;
+    while (c < bytes) c <<= 1;
+    return c;
+}
+
+cudaError_t pinned_get(void** p, size_t bytes) {
+    const size_t c = pinned_class(bytes);
+    {
+        std::lock_guard<std::mutex> lock(g_pinned_mu);
+        auto& list = g_pinned_free[c];
+        if (!list.empty()) {
+            *p = list.back();
+            list.pop_back();
+            return cudaSuccess;
+        }
+    }
+    return cudaMallocHost(p, c);
+}
+
+void pinned_put(void* p, size_t bytes) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(g_pinned_mu);
+    g_pinned_free[pinned_class(bytes)].push_back(p);
 }
 
 #define SPK_CUDA(expr, what)                         \
@@ -626,7 +660,7 @@ StoreOps* store_ops(sparkalog_store* st) {
         cudaError_t e = ops->counts.ensure(256, s);
         if (e == cudaSuccess) e = ops->counters.ensure(256, s);
         if (e == cudaSuccess) e = cudaMemsetAsync(ops->counters.ptr, 0, 256, s);
-        if (e == cudaSuccess) e = cudaMallocHost(&ops->host, 256);
+        if (e == cudaSuccess) e = pinned_get(reinterpret_cast<void**>(&ops->host), 256);
         if (e != cudaSuccess) {
             ops->counts.release(s);
             ops->counters.release(s);
@@ -654,7 +688,7 @@ void release_store_ops(sparkalog_store* st) {
                         &o.ex.index_sort.status})
         d->release(s);
     cudaStreamSynchronize(s);
-    if (o.host) cudaFreeHost(o.host);
+    pinned_put(o.host, 256);
     delete st->ops;
     st->ops = nullptr;
 }
@@ -896,7 +930,7 @@ int sparkalog_catalog_create(void* stream, sparkalog_catalog** out) {
     c->stream = static_cast<cudaStream_t>(stream);
     cudaError_t e = c->words.ensure(256, c->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(c->words.ptr, 0, 256, c->stream);
-    if (e == cudaSuccess) e = cudaMallocHost(&c->host, 64);
+    if (e == cudaSuccess) e = pinned_get(reinterpret_cast<void**>(&c->host), 64);
     if (e != cudaSuccess) {
         c->words.release(c->stream);
         delete c;
@@ -913,7 +947,7 @@ void sparkalog_catalog_destroy(sparkalog_catalog* c) {
                         &c->ids, &c->words, &c->splits, &c->ex.index_sort.plan, &c->ex.index_sort.status})
         d->release(s);
     cudaStreamSynchronize(s);
-    if (c->host) cudaFreeHost(c->host);
+    pinned_put(c->host, 64);
     delete c;
 }
 
@@ -1035,7 +1069,7 @@ int sparkalog_store_create(void* stream, sparkalog_store** out) {
         }
     }
     cudaError_t e = st->flags.ensure(256, st->stream);
-    if (e == cudaSuccess) e = cudaMallocHost(&st->pinned, 256);
+    if (e == cudaSuccess) e = pinned_get(reinterpret_cast<void**>(&st->pinned), 256);
     if (e != cudaSuccess) {
         delete st;
         return cuda_fail(e, "sparkalog_store_create");
@@ -1062,7 +1096,7 @@ void sparkalog_store_destroy(sparkalog_store* st) {
     st->merge_splits.release(s);
     release_store_ops(st);
     cudaStreamSynchronize(s);
-    if (st->pinned) cudaFreeHost(st->pinned);
+    pinned_put(st->pinned, 256);
     delete st;
 }
 
@@ -1604,10 +1638,10 @@ int sparkalog_executor_compile(sparkalog_store* st, const u32* relations, size_t
     const size_t counter_bytes = (kCounterWords + 2 * ex->counts_words + 64) * 4;
     cudaError_t e = ex->counters.ensure(counter_bytes, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(ex->counters.ptr, 0, counter_bytes, s);
-    if (e == cudaSuccess) e = cudaMallocHost(&ex->host_counts, ex->counts_words * 8 + 512);
+    if (e == cudaSuccess) e = pinned_get(reinterpret_cast<void**>(&ex->host_counts), ex->counts_words * 8 + 512);
     if (e == cudaSuccess) e = ex->rule_delta.ensure(std::max<size_t>(rule_count, 1) * 8, s);
-    if (e == cudaSuccess) e = cudaMallocHost(&ex->host_rule_delta, std::max<size_t>(rule_count, 1) * 8);
-    if (e == cudaSuccess) e = cudaMallocHost(&ex->host_active, relation_count * spk::kMaxPasses * 4 + 64);
+    if (e == cudaSuccess) e = pinned_get(reinterpret_cast<void**>(&ex->host_rule_delta), std::max<size_t>(rule_count, 1) * 8);
+    if (e == cudaSuccess) e = pinned_get(reinterpret_cast<void**>(&ex->host_active), relation_count * spk::kMaxPasses * 4 + 64);
     if (e != cudaSuccess) {
         delete ex;
         return cuda_fail(e, "sparkalog_executor_compile");
@@ -1641,9 +1675,9 @@ void sparkalog_executor_destroy(sparkalog_executor* ex) {
     ex->index_pairs[0].release(s);
     ex->index_pairs[1].release(s);
     cudaDeviceSynchronize();
-    if (ex->host_counts) cudaFreeHost(ex->host_counts);
-    if (ex->host_rule_delta) cudaFreeHost(ex->host_rule_delta);
-    if (ex->host_active) cudaFreeHost(ex->host_active);
+    pinned_put(ex->host_counts, ex->counts_words * 8 + 512);
+    pinned_put(ex->host_rule_delta, std::max<size_t>(ex->rules.size(), 1) * 8);
+    pinned_put(ex->host_active, ex->relations.size() * spk::kMaxPasses * 4 + 64);
     for (auto& t : ex->timings) {
         cudaEventDestroy(t.a);
         cudaEventDestroy(t.b);
