@@ -105,7 +105,7 @@ constexpr int kJoinTile = kThreads * kJoinItems;
 constexpr u64 kMaxRelationRows = 0xffffffffull;  // row ids are u32
 constexpr size_t kCounterWords = 1024;  // per-round tile counters
 constexpr int kLevelStage = 2048;  // level rows per shared-memory chunk of the anti-join (two buffers)
-constexpr int kSparseThreads = 128;  // anti-join of small candidate sets
+constexpr int kSparseThreads = 256;  // anti-join of small candidate sets
 constexpr int kSparseItems = 4;
 constexpr int kSparseTile = kSparseThreads * kSparseItems;
 constexpr u64 kSparseCandidates = 1ull << 26;
