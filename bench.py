@@ -460,12 +460,16 @@ def run_batched(args):
     edges = (dev(t0), dev(t1))
     for _ in range(args.warmup):
         batch.run(edges=edges)
-    times = []
+    times, e2e_times = [], []
     for _ in range(args.steps):
-        ms, (results, summary) = timed(lambda: batch.run(edges=edges), stream)
+        ms, (store, summary, seen, per_new) = timed(lambda: batch.run_device(edges=edges), stream)
+        store.close()
         times.append(ms)
+        ms, (results, summary) = timed(lambda: batch.run(edges=edges), stream)
+        e2e_times.append(ms)
     new_rows = sum(r.new_rows for r in results)
     ms = statistics.median(times)
+    e2e_ms = statistics.median(e2e_times)
     serial_ms, serial = timed(batch.run_serial, stream)
     assert all(s.iterations == r.iterations and s.new_rows == r.new_rows for s, r in zip(serial, results))
     line = {
@@ -474,10 +478,14 @@ def run_batched(args):
         "dtype": "u32", "data": "synthetic (seeded ER instances)",
         "config": {"workload": "batched_4096", "instances": len(inst), "edges": int(len(t0)),
                    "derived_tuples": new_rows, "max_iterations": summary.iterations,
-                   "note": "timed step includes reading FULL back to the host and splitting it per instance"},
+                   "note": "value: the device fixpoint from device-resident tagged edges; e2e adds reading "
+                           "every instance's FULL back to the host"},
+        "e2e": {"value": new_rows / (e2e_ms / 1e3), "unit": "tuples/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 8 * (new_rows + int(len(t0))), "ms_per_step": e2e_ms},
         "serial": {"value": new_rows / (serial_ms / 1e3), "ms": serial_ms,
-                   "what": "same instances one at a time through the same engine, same outputs checked equal"},
-        "batched_speedup": serial_ms / ms,
+                   "what": "same instances one at a time through the same engine (upload, run, read back), "
+                           "same outputs checked equal"},
+        "batched_speedup": serial_ms / e2e_ms,
     }
     print(json.dumps(line), flush=True)
 

@@ -69,6 +69,16 @@ class BatchedTransitiveClosure:
 
         ``edges`` may pass the tagged EDB already resident on the device
         (a pair of int32 CUDA tensors) to skip the upload."""
+        store, summary, seen, new_rows = self.run_device(max_iterations, edges)
+        try:
+            return self.collect(store, seen, new_rows), summary
+        finally:
+            store.close()
+
+    def run_device(self, max_iterations: int = 10_000, edges=None):
+        """The device part of run(): the fixpoint, leaving the union's FULL in the
+        returned store (the caller closes it); also returns the SccSummary and the
+        per-instance (last active round, new rows)."""
         first, second = edges if edges is not None else self.tagged_edges()
         store = RelationStore(self.stream)
         store.insert_static(0, (first, second))
@@ -78,19 +88,43 @@ class BatchedTransitiveClosure:
         summary = executor.run(store, max_iterations)
         seen, new_rows = executor.segment_stats()
         executor.close()
-        f0, f1 = store.full(1)
-        store.close()
-        return self.split(f0, f1, seen, new_rows), summary
+        return store, summary, seen, new_rows
+
+    def collect(self, store: RelationStore, seen, new_rows) -> list[InstanceResult]:
+        """Per-instance results from the union's FULL: the instance tags are cleared on the
+        device, the columns come back once, and each instance is a slice of them (its
+        FULL holds its seed plus its new rows, and instances are contiguous)."""
+        import torch
+
+        n = store.rows(1)
+        d0 = torch.empty(max(n, 1), dtype=torch.int32, device="cuda")
+        d1 = torch.empty_like(d0)
+        store.read_into(1, 0, d0, d1)
+        mask = (1 << self.id_bits) - 1
+        h0 = torch.empty(max(n, 1), dtype=torch.int32, pin_memory=True)
+        h1 = torch.empty_like(h0, pin_memory=True)
+        h0.copy_(torch.bitwise_and(d0, mask), non_blocking=True)
+        h1.copy_(torch.bitwise_and(d1, mask), non_blocking=True)
+        torch.cuda.synchronize()
+        return self._slices(h0.numpy()[:n].view(np.uint32), h1.numpy()[:n].view(np.uint32), seen, new_rows)
 
     def split(self, f0, f1, seen, new_rows) -> list[InstanceResult]:
+        """Per-instance results from the union's FULL read to the host with its tags."""
         mask = np.uint32((1 << self.id_bits) - 1)
-        tags = f0 >> np.uint32(self.id_bits)
-        bounds = np.searchsorted(tags, np.arange(len(self.edges) + 1, dtype=np.uint32), side="left")
+        return self._slices(np.asarray(f0, dtype=np.uint32) & mask, np.asarray(f1, dtype=np.uint32) & mask, seen,
+                            new_rows)
+
+    def _slices(self, f0, f1, seen, new_rows) -> list[InstanceResult]:
+        n = len(f0)
+        sizes = np.array([len(e[0]) for e in self.edges], dtype=np.int64) + np.asarray(new_rows, dtype=np.int64)
+        bounds = np.concatenate([[0], np.cumsum(sizes)])
+        if bounds[-1] != n:
+            raise RuntimeError(f"per-instance sizes sum to {bounds[-1]}, FULL holds {n} rows")
         out = []
         for k in range(len(self.edges)):
             a, b = bounds[k], bounds[k + 1]
             iterations = int(seen[k]) + 1 if len(self.edges[k][0]) else 0
-            out.append(InstanceResult((f0[a:b] & mask, f1[a:b] & mask), iterations, int(new_rows[k])))
+            out.append(InstanceResult((f0[a:b], f1[a:b]), iterations, int(new_rows[k])))
         return out
 
     def run_serial(self, max_iterations: int = 10_000) -> list[InstanceResult]:
