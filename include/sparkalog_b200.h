@@ -263,6 +263,14 @@ SPARKALOG_API int sparkalog_store_extract_segment(sparkalog_store* store, uint32
                                                   uint32_t segment, uint32_t* first, uint32_t* second,
                                                   int location, size_t* rows);
 
+/* As sparkalog_store_extract_segment, with the segment tag (the bits at and
+ * above `shift`) cleared on the device from the first column and, when
+ * clear_second is non-zero, from the second column too: a tagged request's
+ * rows come back in its own node ids without a host pass over them. */
+SPARKALOG_API int sparkalog_store_extract_segment_untagged(sparkalog_store* store, uint32_t id, uint32_t shift,
+                                                           uint32_t segment, int clear_second, uint32_t* first,
+                                                           uint32_t* second, int location, size_t* rows);
+
 /* Removes every row whose first >> shift is one of `segments` from FULL and
  * DELTA of relation id (a completed request's rows, freeing its tag). */
 SPARKALOG_API int sparkalog_store_remove_segments(sparkalog_store* store, uint32_t id, uint32_t shift,

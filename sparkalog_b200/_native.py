@@ -54,6 +54,7 @@ TIER_B = [
     "sparkalog_executor_step",
     "sparkalog_store_append",
     "sparkalog_store_extract_segment",
+    "sparkalog_store_extract_segment_untagged",
     "sparkalog_store_remove_segments",
     "sparkalog_executor_destroy",
     "sparkalog_executor_run",
@@ -205,6 +206,9 @@ def load() -> ctypes.CDLL:
     L.sparkalog_store_extract_segment.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, vp, vp, i,
                                                   c_sizep]
     L.sparkalog_store_extract_segment.restype = i
+    L.sparkalog_store_extract_segment_untagged.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, i,
+                                                           vp, vp, i, c_sizep]
+    L.sparkalog_store_extract_segment_untagged.restype = i
     L.sparkalog_store_remove_segments.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, c_u32p, ctypes.c_size_t]
     L.sparkalog_store_remove_segments.restype = i
     L.sparkalog_executor_compile.argtypes = [vp, c_u32p, ctypes.c_size_t, ctypes.POINTER(RulePlanC), ctypes.c_size_t,

@@ -38,6 +38,8 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <system_error>
+#include <thread>
 #include <vector>
 
 using spk::u32;
@@ -89,6 +91,77 @@ void pinned_put(void* p, size_t bytes) {
     if (!p) return;
     std::lock_guard<std::mutex> lock(g_pinned_mu);
     g_pinned_free[pinned_class(bytes)].push_back(p);
+}
+
+// Device columns into caller host memory. A page-locked destination, or a
+// small copy, takes one DMA per column. For a large pageable destination the
+// driver would stage every byte through its own page-locked buffer on one
+// thread, page faults included (a few GB/s); instead the columns are cut into
+// chunks that several host threads each DMA into a page-locked chunk of their
+// own and copy out while the other threads' chunks are in flight.
+constexpr size_t kHostChunk = 8u << 20;
+constexpr size_t kStagedMin = 32u << 20;
+
+cudaError_t columns_to_host(u32* first, u32* second, const u32* d0, const u32* d1, u64 n, cudaStream_t s) {
+    const size_t bytes = n * 4;
+    cudaPointerAttributes attr{};
+    cudaError_t e = cudaPointerGetAttributes(&attr, first);
+    if (e != cudaSuccess) return e;
+    const bool pageable = attr.type == cudaMemoryTypeUnregistered;
+    if (!pageable || bytes < kStagedMin) {
+        e = cudaMemcpyAsync(first, d0, bytes, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(second, d1, bytes, cudaMemcpyDeviceToHost, s);
+        return e;
+    }
+    struct Job {
+        char* dst;
+        const char* src;
+        size_t len;
+    };
+    std::vector<Job> jobs;
+    for (int c = 0; c < 2; ++c) {
+        char* dst = reinterpret_cast<char*>(c ? second : first);
+        const char* src = reinterpret_cast<const char*>(c ? d1 : d0);
+        for (size_t off = 0; off < bytes; off += kHostChunk)
+            jobs.push_back({dst + off, src + off, std::min(kHostChunk, bytes - off)});
+    }
+    int device = 0;
+    e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return e;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t workers = std::min<size_t>({16, std::max(1u, hw / 2), jobs.size()});
+    std::atomic<int> status{cudaSuccess};
+    auto work = [&](size_t t) {
+        cudaError_t w = cudaSetDevice(device);
+        void* buf = nullptr;
+        cudaEvent_t ev = nullptr;
+        if (w == cudaSuccess) w = pinned_get(&buf, kHostChunk);
+        if (w == cudaSuccess) w = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        for (size_t j = t; w == cudaSuccess && j < jobs.size(); j += workers) {
+            if (status.load(std::memory_order_relaxed) != cudaSuccess) break;
+            w = cudaMemcpyAsync(buf, jobs[j].src, jobs[j].len, cudaMemcpyDeviceToHost, s);
+            if (w == cudaSuccess) w = cudaEventRecord(ev, s);
+            if (w == cudaSuccess) w = cudaEventSynchronize(ev);
+            if (w == cudaSuccess) std::memcpy(jobs[j].dst, buf, jobs[j].len);
+        }
+        if (ev) cudaEventDestroy(ev);
+        if (buf) pinned_put(buf, kHostChunk);
+        if (w != cudaSuccess) {
+            int expect = cudaSuccess;
+            status.compare_exchange_strong(expect, static_cast<int>(w));
+        }
+    };
+    std::vector<std::thread> pool;
+    size_t started = 0;
+    try {
+        for (; started + 1 < workers; ++started) pool.emplace_back(work, started + 1);
+    } catch (const std::system_error&) {
+        // Fewer threads than planned: the jobs of the missing ones run below.
+    }
+    work(0);
+    for (auto& th : pool) th.join();
+    for (size_t t = started + 1; t < workers; ++t) work(t);
+    return static_cast<cudaError_t>(status.load());
 }
 
 #define SPK_CUDA(expr, what)                         \
@@ -1348,10 +1421,7 @@ int sparkalog_store_read(sparkalog_store* st, u32 id, int version, u32* first, u
     }
     spk::unpack_rows_kernel<<<simple_grid(n), 256, 0, s>>>(src, n, d0, d1);
     SPK_CUDA(cudaGetLastError(), "unpack_rows_kernel");
-    if (location == SPARKALOG_HOST) {
-        SPK_CUDA(cudaMemcpyAsync(first, d0, n * 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
-        SPK_CUDA(cudaMemcpyAsync(second, d1, n * 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
-    }
+    if (location == SPARKALOG_HOST) SPK_CUDA(columns_to_host(first, second, d0, d1, n, s), "cudaMemcpyAsync");
     SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
     return 0;
 }
@@ -1455,8 +1525,10 @@ int sparkalog_store_append(sparkalog_store* st, u32 id, const u32* first, const 
     return 0;
 }
 
-int sparkalog_store_extract_segment(sparkalog_store* st, u32 id, u32 shift, u32 segment, u32* first, u32* second,
-                                    int location, size_t* rows) {
+namespace {
+
+int extract_segment(sparkalog_store* st, u32 id, u32 shift, u32 segment, u32* first, u32* second, int location,
+                    size_t* rows, u32 mask0, u32 mask1) {
     if (!st || !rows || shift > 31) return fail(SPARKALOG_E_INVALID_ARGUMENT, "invalid argument");
     RelState* r = st->find(id);
     if (!r) return fail(SPARKALOG_E_MISSING, "relation " + std::to_string(id) + " is not registered");
@@ -1512,14 +1584,26 @@ int sparkalog_store_extract_segment(sparkalog_store* st, u32 id, u32 shift, u32 
         d0 = st->scratch_u32[0].as<u32>();
         d1 = st->scratch_u32[1].as<u32>();
     }
-    spk::unpack_rows_kernel<<<simple_grid(total), 256, 0, s>>>(ops.a.as<u64>(), total, d0, d1);
+    spk::unpack_rows_kernel<<<simple_grid(total), 256, 0, s>>>(ops.a.as<u64>(), total, d0, d1, mask0, mask1);
     SPK_CUDA(cudaGetLastError(), "unpack_rows_kernel");
-    if (location == SPARKALOG_HOST) {
-        SPK_CUDA(cudaMemcpyAsync(first, d0, total * 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
-        SPK_CUDA(cudaMemcpyAsync(second, d1, total * 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
-    }
+    if (location == SPARKALOG_HOST) SPK_CUDA(columns_to_host(first, second, d0, d1, total, s), "cudaMemcpyAsync");
     SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
     return 0;
+}
+
+}  // namespace
+
+int sparkalog_store_extract_segment(sparkalog_store* st, u32 id, u32 shift, u32 segment, u32* first, u32* second,
+                                    int location, size_t* rows) {
+    return extract_segment(st, id, shift, segment, first, second, location, rows, ~0u, ~0u);
+}
+
+int sparkalog_store_extract_segment_untagged(sparkalog_store* st, u32 id, u32 shift, u32 segment,
+                                             int clear_second, u32* first, u32* second, int location,
+                                             size_t* rows) {
+    if (shift > 31) return fail(SPARKALOG_E_INVALID_ARGUMENT, "invalid argument");
+    const u32 low = shift == 0 ? 0u : (~0u >> (32 - shift));
+    return extract_segment(st, id, shift, segment, first, second, location, rows, low, clear_second ? low : ~0u);
 }
 
 int sparkalog_store_remove_segments(sparkalog_store* st, u32 id, u32 shift, const u32* segments, size_t count) {

@@ -573,12 +573,15 @@ static __global__ void pack_rows_kernel(const u32* c0, const u32* c1, u64 n, u64
     if (lane_id() == 0) atomicMax(flags + 1, max_value);
 }
 
-static __global__ void unpack_rows_kernel(const u64* in, u64 n, u32* c0, u32* c1) {
+// Packed rows back to two columns; mask0/mask1 keep the given bits of each
+// column (all ones for a plain read, the low bits to drop a segment tag).
+static __global__ void unpack_rows_kernel(const u64* in, u64 n, u32* c0, u32* c1, u32 mask0 = ~0u,
+                                          u32 mask1 = ~0u) {
     const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
     for (u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
         const u64 k = in[i];
-        c0[i] = static_cast<u32>(k >> 32);
-        c1[i] = static_cast<u32>(k);
+        c0[i] = static_cast<u32>(k >> 32) & mask0;
+        c1[i] = static_cast<u32>(k) & mask1;
     }
 }
 

@@ -189,16 +189,23 @@ class RelationStore:
         _check(_native.load().sparkalog_store_append(self._h, int(getattr(rid, "value", rid)), p0, p1, n, loc))
         del keep
 
-    def extract_segment(self, rid: RelationId | int, shift: int, segment: int) -> tuple[np.ndarray, np.ndarray]:
-        """Sorted rows of FULL whose first column >> shift == segment."""
+    def extract_segment(self, rid: RelationId | int, shift: int, segment: int,
+                        untag: bool = False) -> tuple[np.ndarray, np.ndarray]:
+        """Sorted rows of FULL whose first column >> shift == segment; with
+        ``untag`` the segment bits of both columns are cleared on the device."""
         L = _native.load()
         rid = int(getattr(rid, "value", rid))
         n = ctypes.c_size_t(0)
-        _check(L.sparkalog_store_extract_segment(self._h, rid, shift, segment, None, None, HOST, ctypes.byref(n)))
+        if untag:
+            call = lambda a, b: L.sparkalog_store_extract_segment_untagged(self._h, rid, shift, segment, 1, a, b, HOST,
+                                                                            ctypes.byref(n))
+        else:
+            call = lambda a, b: L.sparkalog_store_extract_segment(self._h, rid, shift, segment, a, b, HOST,
+                                                                  ctypes.byref(n))
+        _check(call(None, None))
         a = np.empty(max(n.value, 1), dtype=np.uint32)
         b = np.empty(max(n.value, 1), dtype=np.uint32)
-        _check(L.sparkalog_store_extract_segment(self._h, rid, shift, segment, a.ctypes.data, b.ctypes.data, HOST,
-                                                 ctypes.byref(n)))
+        _check(call(a.ctypes.data, b.ctypes.data))
         return a[: n.value], b[: n.value]
 
     def remove_segments(self, rid: RelationId | int, shift: int, segments) -> None:

@@ -30,6 +30,7 @@ import time
 from dataclasses import dataclass, field
 
 import numpy as np
+import torch
 
 from .recursion import RecursiveExecutor, RelationStore, transitive_closure_scc
 from .relational import RelationId
@@ -92,6 +93,7 @@ class FixpointServer:
         self.retired_bytes = 0.0
         self.active: dict[int, _Active] = {}
         self.rounds = 0
+        self._stage: tuple = ()  # (page-locked tensors, their u32 views)
         self.completions: list[Completion] = []
 
     # ------------------------------------------------------------ admission
@@ -117,34 +119,49 @@ class FixpointServer:
             self.purge()
         return self.resident_bytes() + reserved + need <= self.budget or (not self.active and not batch)
 
+    def _staging(self, rows: int) -> tuple[np.ndarray, np.ndarray]:
+        """Two page-locked u32 columns of at least `rows` entries, kept across
+        admissions: tagged edges are written there once and copied to the
+        device at full link speed."""
+        if not self._stage or len(self._stage[1][0]) < rows:
+            cap = max(rows, 2 * len(self._stage[1][0]) if self._stage else 1 << 20)
+            pin = torch.cuda.is_available()
+            t = [torch.empty(cap, dtype=torch.int32, pin_memory=pin) for _ in range(2)]
+            self._stage = (t, [x.numpy().view(np.uint32) for x in t])
+        return self._stage[1][0], self._stage[1][1]
+
     def admit(self, requests: list[ServeRequest]) -> None:
         """Appends the requests' tagged edges to the EDB and, as seed, to FULL/DELTA of path."""
         if not requests:
             return
         now = self.clock()
         _, new_rows = self.executor.segment_stats()
-        firsts, seconds = [], []
-        for req in requests:
-            slot = self.free.pop()
-            # Raw edge lists: the device append sorts and deduplicates them.
-            s = np.asarray(req.src, dtype=np.uint32)
-            d = np.asarray(req.dst, dtype=np.uint32)
+        cols = [(np.asarray(r.src, dtype=np.uint32), np.asarray(r.dst, dtype=np.uint32)) for r in requests]
+        first, second = self._staging(sum(len(s) for s, _ in cols))
+        off = 0
+        for req, (s, d) in zip(requests, cols):
+            if len(s) != len(d):
+                raise ValueError(f"request {req.request_id} has columns of different lengths")
             if len(s) and max(int(s.max()), int(d.max())) >= (1 << self.shift):
                 raise ValueError(f"request {req.request_id} has node ids >= 2^{self.shift}")
-            tag = np.uint32(slot << self.shift)
-            firsts.append(s | tag)
-            seconds.append(d | tag)
+            slot = self.free.pop()
             if len(s) == 0:
                 # No seed: the fixpoint runs zero rounds.
                 self.completions.append(Completion(req.request_id, (s, d), 0, 0, req.arrival_s, now, now))
                 self.free.append(slot)
                 continue
+            # Raw edge lists, tagged in the staging columns: the device append
+            # sorts and deduplicates them.
+            tag = np.uint32(slot << self.shift)
+            np.bitwise_or(s, tag, out=first[off:off + len(s)])
+            np.bitwise_or(d, tag, out=second[off:off + len(s)])
+            off += len(s)
             self.active[slot] = _Active(req, slot, self.rounds, now, int(new_rows[slot]),
                                         self.estimate_bytes(len(s)))
-        first, second = np.concatenate(firsts), np.concatenate(seconds)
-        if len(first):
-            self.store.append(EDB, (first, second))
-            self.store.append(PATH, (first, second))
+        if off:
+            # Each append has finished reading the staging columns when it returns.
+            self.store.append(EDB, (first[:off], second[:off]))
+            self.store.append(PATH, (first[:off], second[:off]))
 
     # ------------------------------------------------------------ rounds
 
@@ -160,11 +177,10 @@ class FixpointServer:
         now = None
         for slot in done:
             a = self.active.pop(slot)
-            f0, f1 = self.store.extract_segment(PATH, self.shift, slot)
-            mask = np.uint32((1 << self.shift) - 1)
+            f0, f1 = self.store.extract_segment(PATH, self.shift, slot, untag=True)
             iterations = int(seen[slot]) - a.admit_round + 1 if int(seen[slot]) > a.admit_round else 1
             now = self.clock()
-            c = Completion(a.request.request_id, (f0 & mask, f1 & mask), iterations,
+            c = Completion(a.request.request_id, (f0, f1), iterations,
                            int(new_rows[slot]) - a.base_new_rows, a.request.arrival_s, a.admitted_s, now)
             finished.append(c)
             edges = max(len(a.request.src), 1)

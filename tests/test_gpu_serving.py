@@ -81,3 +81,56 @@ def test_realtime_stream_latencies(cuda):
     assert s["requests"] == 20
     assert all(c.finished_s >= c.arrival_s for c in report.completions)
     assert s["p99_ms"] >= s["p50_ms"] > 0
+
+
+def test_extract_segment_untagged_equals_masked_read(cuda):
+    from sparkalog_b200.recursion import RelationStore
+
+    rng = np.random.default_rng(17)
+    shift = 20
+    segs = rng.integers(0, 1 << (32 - shift), 5000).astype(np.uint32)
+    first = (segs << np.uint32(shift)) | rng.integers(0, 1 << shift, 5000).astype(np.uint32)
+    second = (segs << np.uint32(shift)) | rng.integers(0, 1 << shift, 5000).astype(np.uint32)
+    store = RelationStore()
+    empty = np.zeros(0, dtype=np.uint32)
+    store.insert_static(0, (empty, empty))
+    store.append(0, (first, second))  # sorted and deduplicated on the device
+    mask = np.uint32((1 << shift) - 1)
+    for seg in [int(segs[0]), int(segs[1]), (1 << (32 - shift)) - 1, 0]:
+        t0, t1 = store.extract_segment(0, shift, seg)
+        u0, u1 = store.extract_segment(0, shift, seg, untag=True)
+        assert np.all((t0 >> np.uint32(shift)) == seg)
+        assert np.array_equal(u0, t0 & mask) and np.array_equal(u1, t1 & mask)
+    store.close()
+
+
+def test_large_pageable_reads_equal_pinned_reads(cuda):
+    """Reads above the staged-copy threshold (32 MiB per column) into pageable
+    NumPy arrays equal a read into page-locked buffers."""
+    import torch
+
+    from sparkalog_b200.recursion import FULL, RelationStore
+
+    rng = np.random.default_rng(23)
+    n = 20_000_000
+    first = rng.integers(0, 1 << 12, n).astype(np.uint32) << np.uint32(20)
+    first |= rng.integers(0, 1 << 20, n).astype(np.uint32)
+    second = rng.integers(0, 1 << 32, n, dtype=np.uint64).astype(np.uint32)
+    store = RelationStore()
+    empty = np.zeros(0, dtype=np.uint32)
+    store.insert_static(0, (empty, empty))
+    store.append(0, (first, second))
+    rows = store.rows(0)
+    p0 = torch.empty(rows, dtype=torch.int32, pin_memory=True)
+    p1 = torch.empty(rows, dtype=torch.int32, pin_memory=True)
+    store.read_into(0, FULL, p0, p1)
+    f0, f1 = store.full(0)
+    assert len(f0) == rows
+    assert np.array_equal(f0, p0.numpy().view(np.uint32)) and np.array_equal(f1, p1.numpy().view(np.uint32))
+    # Segment 0 under shift 31 (first < 2^31) holds about half of the rows
+    # (10M, 40 MB a column): the staged path with the tag cleared.
+    u0, u1 = store.extract_segment(0, 31, 0, untag=True)
+    t0, t1 = store.extract_segment(0, 31, 0)
+    assert len(u0) * 4 >= 32 << 20
+    assert np.array_equal(u0, t0 & np.uint32(0x7FFFFFFF)) and np.array_equal(u1, t1 & np.uint32(0x7FFFFFFF))
+    store.close()
