@@ -134,17 +134,9 @@ class RoundTraceC(ctypes.Structure):
 _lib = None
 
 
-def load() -> ctypes.CDLL:
-    """Loads the CUDA library; raises if it has not been built."""
-    global _lib
-    if _lib is not None:
-        return _lib
-    if not LIB_PATH.exists():
-        raise ImportError(
-            f"{LIB_PATH} is missing: build it with `python -m sparkalog_b200.build` "
-            "(sparkalog_b200 has no CPU fallback)")
-    L = ctypes.CDLL(str(LIB_PATH))
-    i = ctypes.c_int
+def declare_operator_abi(L: ctypes.CDLL) -> None:
+    """Argument types of the operator ABI that this library shares with the
+    reference's column_ops.cu (crates/sparkalog-execution/native/column_ops.cu:231-775)."""
     L.sparkalog_stream_synchronize.argtypes = [vp]
     L.sparkalog_join_u32_temporary_bytes.argtypes = [vp, vp, ctypes.c_size_t, c_sizep, vp]
     L.sparkalog_join_u32_count.argtypes = [vp, ctypes.c_size_t, vp, vp, ctypes.c_size_t, vp, vp, vp, vp,
@@ -165,6 +157,20 @@ def load() -> ctypes.CDLL:
                                                       vp]
     L.sparkalog_union_u32.argtypes = [vp, vp, ctypes.c_size_t, vp, vp, ctypes.c_size_t, vp, vp, vp, vp, vp, vp, vp,
                                       vp, ctypes.c_size_t, vp]
+
+
+def load() -> ctypes.CDLL:
+    """Loads the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -m sparkalog_b200.build` "
+            "(sparkalog_b200 has no CPU fallback)")
+    L = ctypes.CDLL(str(LIB_PATH))
+    i = ctypes.c_int
+    declare_operator_abi(L)
     L.sparkalog_anti_join_u32_no_alloc.argtypes = [vp, vp, ctypes.c_size_t, vp, vp, ctypes.c_size_t, vp, vp, vp,
                                                    vp, vp, vp]
     L.sparkalog_b200_device_error.argtypes = [c_u32p, i]
