@@ -122,6 +122,18 @@ def parse_args():
     return p.parse_args()
 
 
+def grow_device_pool(nbytes: int) -> int:
+    """Grows the device's stream-ordered memory pool once, before warm-up, as a
+    long-running process would: relation buffers are allocated and freed every
+    round, and a pool that has to map new memory in the middle of a round
+    stalls it (a few ms per fixpoint, up to 0.5 s on a fresh box). Returns the
+    size in GB for the config line."""
+    from sparkalog_b200.recursion import reserve_device_memory
+
+    reserve_device_memory(int(nbytes))
+    return int(nbytes) >> 30
+
+
 def measured_peaks():
     f = ROOT / "MEASURED_PEAKS.json"
     if f.exists():
@@ -267,6 +279,7 @@ def run_ours(args):
     src, dst = generators.er_edges(nodes, edges, seed)
     ps, pd = partition(src, dst, nodes, rank, world)
     stream = torch.cuda.current_stream()
+    pool_gb = grow_device_pool(min(48 << 30, max(2 << 30, 1600 * edges)))
     dev = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).cuda()
     e0, e1, s0, s1 = dev(src), dev(dst), dev(ps), dev(pd)
     path, edge = RelationId(1), RelationId(0)
@@ -398,7 +411,7 @@ def run_ours(args):
             "dtype": "u32",
             "data": "synthetic (seeded ER, splitmix64)",
             "config": {"workload": args.workload, "nodes": nodes, "edges": edges, "seed": seed,
-                       "derived_tuples": new_rows, "iterations": iterations,
+                       "derived_tuples": new_rows, "iterations": iterations, "device_pool_gb": pool_gb,
                        "parallelism": f"x-range partition x{world}" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (FULL ~1 GB, candidates ~100 MB per round)"},
             "e2e": {"value": e2e_value, "unit": "tuples/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -455,6 +468,7 @@ def run_batched(args):
     inst = [generators.er_edges(p.nodes, p.edges, p.seed) for p in params]
     batch = BatchedTransitiveClosure(inst)
     stream = torch.cuda.current_stream()
+    pool_gb = grow_device_pool(48 << 30)
     t0, t1 = batch.tagged_edges()
     dev = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).cuda()
     edges = (dev(t0), dev(t1))
@@ -476,7 +490,7 @@ def run_batched(args):
         "metric": "TC derived tuples/s (batched)", "value": new_rows / (ms / 1e3), "unit": "tuples/s",
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "dtype": "u32", "data": "synthetic (seeded ER instances)",
-        "config": {"workload": "batched_4096", "instances": len(inst), "edges": int(len(t0)),
+        "config": {"workload": "batched_4096", "instances": len(inst), "edges": int(len(t0)), "device_pool_gb": pool_gb,
                    "derived_tuples": new_rows, "max_iterations": summary.iterations,
                    "note": "value: the device fixpoint from device-resident tagged edges; e2e adds reading "
                            "every instance's FULL back to the host"},
@@ -510,6 +524,7 @@ def run_negation(args):
     c1 = generators._bounded(generators.splitmix64(55, 2 * j + np.uint64(1)), 8_388_608).astype(np.uint32)
     del j
     stream = torch.cuda.current_stream()
+    pool_gb = grow_device_pool(24 << 30)
     dev = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).cuda()
     e0, e1, d0, d1 = dev(src), dev(dst), dev(c0), dev(c1)
     plan = transitive_closure_scc(R(1), R(0))
@@ -547,6 +562,7 @@ def run_negation(args):
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "dtype": "u32", "data": "synthetic (seeded ER + uniform candidates)",
         "config": {"workload": "negation_8m", "nodes": 8_388_608, "edges": 7_340_032, "cand": int(len(c0)),
+                   "device_pool_gb": pool_gb,
                    "path_rows": store.rows(1), "iterations": summary.iterations,
                    "unreached_rows": unreached,
                    "note": "timed step = both strata from device-resident raw facts (the anti-join sorts and "
@@ -573,6 +589,7 @@ def run_ingest(args):
     host = torch.from_numpy(np.frombuffer(text, dtype=np.uint8).copy()).pin_memory()
     dev_text = host.cuda()
     stream = torch.cuda.current_stream()
+    pool_gb = grow_device_pool(8 << 30)
 
     def parse(t):
         store = RelationStore(stream)
@@ -619,7 +636,7 @@ def run_ingest(args):
         "metric": "ingested rows/s", "value": rows / (ms_dev / 1e3), "unit": "rows/s", "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_dev, "higher_is_better": True,
         "dtype": "u8 text -> u32", "data": "synthetic (seeded ER edge list as text)",
-        "config": {"workload": "ingest_16m", "bytes": len(text), "rows": rows},
+        "config": {"workload": "ingest_16m", "bytes": len(text), "rows": rows, "device_pool_gb": pool_gb},
         "e2e": {"value": rows / (ms_host / 1e3), "unit": "rows/s", "h2d_bytes_per_step": len(text),
                 "d2h_bytes_per_step": 0, "ms_per_step": ms_host},
         "roofline": {"bound": "hbm", "kernel": "line_ends + parse_lines (+ insert)",
@@ -645,14 +662,12 @@ def run_served(args):
     from sparkalog_b200 import generators
     from sparkalog_b200.serving import FixpointServer, ServeRequest, serve, serve_one_at_a_time
 
-    from sparkalog_b200.recursion import reserve_device_memory
-
     count = args.requests
     params = generators.served_requests(count, 1.0, 4)
     edges = [generators.er_edges(p.nodes, p.edges, p.seed) for p in params]
     rates = [float(r) for r in args.rates.split(",")]
     # A serving process keeps its memory pool; grow it once up front.
-    reserve_device_memory(48 << 30)
+    pool_gb = grow_device_pool(48 << 30)
     results = []
     for rate in rates:
         reqs = [ServeRequest(k, p.arrival_s / rate, *edges[k]) for k, p in enumerate(params)]
@@ -674,6 +689,7 @@ def run_served(args):
         "unit": "tuples/s", "n_gpus": 1, "higher_is_better": True, "dtype": "u32",
         "data": "synthetic (seeded Poisson stream of ER requests)",
         "config": {"workload": "served", "requests": count, "rates_per_s": rates, "budget_gb": 120,
+                   "device_pool_gb": pool_gb,
                    "edges_total": int(sum(len(e[0]) for e in edges))},
         "per_rate": results,
     }

@@ -181,6 +181,12 @@ constexpr int kLevelStage = 2048;  // level rows per shared-memory chunk of the 
 constexpr int kSparseThreads = 256;  // anti-join of small candidate sets
 constexpr int kSparseItems = 4;
 constexpr int kSparseTile = kSparseThreads * kSparseItems;
+// Candidate bounds up to this use the group-searched anti-join (8 lanes per
+// candidate): latency-bound rounds with a few thousand candidates at most.
+constexpr u64 kWideCandidates = 1ull << 15;
+constexpr int kWideThreads = 256;
+constexpr int kWideGroup = 8;
+constexpr int kWideTile = kWideThreads / kWideGroup;
 constexpr u64 kSparseCandidates = 1ull << 26;
 constexpr int kMergeItems = 8;
 constexpr int kMergeTile = kThreads * kMergeItems;
@@ -1973,6 +1979,9 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                 // One status word per anti-join tile (the sparse kernel's
                 // tiles are the smallest)...
                 max_status_words = std::max<size_t>(max_status_words, (t.j_cap + kSparseTile - 1) / kSparseTile + 1);
+                // ...or the group-searched kernel's, over at most kWideCandidates.
+                const u64 wide = std::min<u64>(t.j_cap, kWideCandidates);
+                max_status_words = std::max<size_t>(max_status_words, (wide + kWideTile - 1) / kWideTile + 1);
                 // ...and per fused tile, which are DELTA-row tiles.
                 u64 delta_rows = 0;
                 for (size_t k : t.rules) delta_rows += ex->host_rule_delta[k];
@@ -2147,6 +2156,16 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                                                tr.newt.as<u64>(), tc + t.rules.size() + 1, ex->status.as<u64>(),
                                                counters + counter_slot++, ex->epoch++, err, unique_word);
                     SPK_CUDA(cudaGetLastError(), "anti_join_member_kernel");
+                } else if (cand_bound <= kWideCandidates) {
+                    // A few candidates: lookup latency dominates, so 8 lanes
+                    // search each one together.
+                    auto kernel = spk::anti_join_levels_wide_kernel<kWideThreads, kWideGroup>;
+                    const size_t tiles = (cand_bound + kWideTile - 1) / kWideTile;
+                    kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kWideThreads, std::max<size_t>(tiles, 1)),
+                             kWideThreads, 0, s>>>(cand, t.j_b.as<u64>(), cand_sel, jn, lv, tr.newt.as<u64>(),
+                                                   tc + t.rules.size() + 1, ex->status.as<u64>(),
+                                                   counters + counter_slot++, ex->epoch++, err, unique_word);
+                    SPK_CUDA(cudaGetLastError(), "anti_join_levels_wide_kernel");
                 } else if (cand_bound <= kSparseCandidates) {
                     // Few candidates, far apart in every level: look each up
                     // in all levels at once.

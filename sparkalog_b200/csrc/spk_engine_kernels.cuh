@@ -329,6 +329,104 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_sparse_kernel(const 
     }
 }
 
+// The same anti-join for a handful of candidates (the last rounds of a
+// fixpoint), where a lookup's latency, not the loads' bandwidth, sets the
+// time: G lanes search one candidate together. Each step loads G pivots of
+// the candidate's bucket in every level at once and keeps the gap between the
+// two pivots that bracket the key, so a bucket of S rows takes
+// log_{G+1}(S) steps instead of log_2(S) dependent loads. A tile is
+// THREADS / G candidates, one per group.
+template <int THREADS, int G>
+__global__ void __launch_bounds__(THREADS) anti_join_levels_wide_kernel(const u64* buf_a, const u64* buf_b,
+                                                                        const u32* final_sel, const u64* n_ptr,
+                                                                        Levels levels, u64* out, u64* out_count,
+                                                                        u64* status, u32* tile_counter, u32 epoch,
+                                                                        u32* err, unsigned long long* unique_count) {
+    static_assert(G >= 2 && G <= 32 && 32 % G == 0 && THREADS % 32 == 0, "groups tile the warp");
+    constexpr int kTile = THREADS / G;
+    // Each step shrinks a window of S > G rows to at most S / (G + 1) + 1;
+    // 64 steps cover any u32 row range.
+    constexpr int kMaxSteps = 64;
+    __shared__ CompactShared<THREADS> cs;
+    __shared__ u64 stage[kTile];
+    const u64* keys = (final_sel && *final_sel) ? buf_b : buf_a;
+    const u64 n = *n_ptr;
+    const u64 num_tiles = (n + kTile - 1) / kTile;
+    if (num_tiles == 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) *out_count = 0;
+        return;
+    }
+    const u32 lane = threadIdx.x % G;
+    const u32 group_mask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << (lane_id() / G * G);
+    for (;;) {
+        if (threadIdx.x == 0) cs.tile = atomicAdd(tile_counter, 1u);
+        __syncthreads();
+        const u64 tile = cs.tile;
+        if (tile >= num_tiles) break;
+        const u64 idx = tile * kTile + threadIdx.x / G;
+        u64 v = 0;
+        bool keep = false;
+        if (idx < n) {
+            v = keys[idx];
+            keep = idx == 0 || keys[idx - 1] != v;
+        }
+        count_unique(lane == 0 && keep ? 1u : 0u, unique_count);
+        // [lo, hi): the rows of v's bucket in each level; a row equal to v
+        // can only lie there.
+        u64 lo[kMaxLevels], hi[kMaxLevels];
+#pragma unroll
+        for (int l = 0; l < kMaxLevels; ++l) {
+            lo[l] = hi[l] = 0;
+            if (keep && l < levels.n) dir_range(levels, l, v, &lo[l], &hi[l]);
+        }
+        bool wide = false;
+#pragma unroll
+        for (int l = 0; l < kMaxLevels; ++l) wide |= hi[l] - lo[l] > static_cast<u64>(G);
+        for (int step = 0; step < kMaxSteps && __any_sync(0xffffffffu, wide); ++step) {
+            u64 pivot[kMaxLevels];
+            bool below[kMaxLevels];
+#pragma unroll
+            for (int l = 0; l < kMaxLevels; ++l) {
+                const u64 span = hi[l] - lo[l];
+                below[l] = false;
+                pivot[l] = lo[l] + (span * (lane + 1)) / (G + 1);
+                if (span > static_cast<u64>(G)) below[l] = levels.keys[l][pivot[l]] < v;
+            }
+            wide = false;
+#pragma unroll
+            for (int l = 0; l < kMaxLevels; ++l) {
+                const u64 span = hi[l] - lo[l];
+                // Pivots ascend with the lane, so the lanes below v form a prefix.
+                const u32 c = __popc(__ballot_sync(0xffffffffu, below[l]) & group_mask);
+                if (span > static_cast<u64>(G)) {
+                    const u64 p_lo = lo[l] + (span * c) / (G + 1);          // pivot c - 1
+                    const u64 p_hi = lo[l] + (span * (c + 1)) / (G + 1);    // pivot c
+                    const u64 nlo = c > 0 ? p_lo + 1 : lo[l];
+                    const u64 nhi = c < static_cast<u32>(G) ? p_hi + 1 : hi[l];
+                    lo[l] = nlo;
+                    hi[l] = nhi;
+                }
+                wide |= hi[l] - lo[l] > static_cast<u64>(G);
+            }
+        }
+        if (wide) atomicOr(err, kErrIndexRange);  // cannot happen: the windows shrink every step
+        bool found = false;
+#pragma unroll
+        for (int l = 0; l < kMaxLevels; ++l)
+            if (lane < hi[l] - lo[l] && levels.keys[l][lo[l] + lane] == v) found = true;
+        found = (__ballot_sync(0xffffffffu, found) & group_mask) != 0;
+        keep = keep && !found;
+        u32 excl, total;
+        const u64 off =
+            compact_offsets<THREADS>(lane == 0 && keep ? 1u : 0u, &excl, &total, tile, status, epoch, err, cs);
+        if (lane == 0 && keep) stage[excl] = v;
+        __syncthreads();
+        for (u32 j = threadIdx.x; j < total; j += THREADS) out[off + j] = stage[j];
+        if (tile == num_tiles - 1 && threadIdx.x == 0) *out_count = off + total;
+        __syncthreads();
+    }
+}
+
 // Per-segment activity of one round's NEWT rows (sorted, so a segment's rows
 // are contiguous): seen[seg] = max(seen[seg], round1), new_rows[seg] += rows.
 // Lanes holding the same segment are grouped with match.any and one lane per
