@@ -536,7 +536,8 @@ struct TargetRT {
     DevArray j_a, j_b;     // candidate buffers (sort ping-pong)
     u64 j_cap = 0;         // elements
     SortScratch sort;
-    u32 fused_rows = 896;  // nominal DELTA rows per fused tile (halved when tiles overflow)
+    u32 fused_rows = 672;      // DELTA rows per fused tile in the next round
+    u32 fused_rows_cap = 672;  // its ceiling, halved whenever a tile overflows
     bool force_generic = false;  // redo the current round with the general kernels
     bool fused_last = false;     // the round just applied ran the fused kernel
 };
@@ -675,8 +676,12 @@ size_t target_count_base(const sparkalog_executor* ex, size_t t) {
 }
 
 constexpr int kFusedThreads = 256;
-constexpr int kFusedCap = 1920;     // join output rows per fused tile (shared memory)
-constexpr int kFusedRowCap = 1024;  // DELTA rows per fused tile
+// 40 KB of shared memory per tile: five CTAs fit an SM (the kernel waits on
+// its barriers and shared-memory dependencies, so resident tiles are what
+// hides that latency; tiles of 1920 / 1024, four per SM, took 7.0 ms of the
+// fixpoint over the 16.7M-node ER graph against 4.5 ms).
+constexpr int kFusedCap = 1280;    // join output rows per fused tile (shared memory)
+constexpr int kFusedRowCap = 768;  // DELTA rows per fused tile
 constexpr size_t kFusedFlagBase = 8;      // fallback flags live at err + 8 + target
 constexpr size_t kFusedMaxTargets = 48;
 constexpr size_t kMaxTraceRounds = 1u << 20;
@@ -2239,6 +2244,7 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                 TargetRT& t = ex->targets[ti];
                 t.force_generic = true;
                 if (t.fused_rows > 64) t.fused_rows /= 2;
+                t.fused_rows_cap = std::min(t.fused_rows_cap, t.fused_rows);
                 redo_generic = true;
             }
             if (redo_generic) {
@@ -2358,6 +2364,20 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                 rec.full_rows += st->find(t.id)->full_rows();
             }
             if (ex->trace.size() < kMaxTraceRounds) ex->trace.push_back(rec);
+        }
+        // Rows per fused tile for the next round: a tile holds kFusedCap join
+        // rows, so aim at two thirds of that with this round's join rows per
+        // DELTA row (dense graphs get short tiles instead of overflowing).
+        for (size_t ti = 0; ti < ex->targets.size(); ++ti) {
+            TargetRT& t = ex->targets[ti];
+            u64 delta_rows = 0;
+            for (size_t k : t.rules) delta_rows += ex->host_rule_delta[k];
+            if (delta_rows == 0) continue;
+            const u64* c = ex->host_counts + target_count_base(ex, ti);
+            const double per_row = static_cast<double>(t.fused_last ? c[0] : c[t.rules.size()]) /
+                                   static_cast<double>(delta_rows);
+            const double rows = kFusedCap / (1.5 * std::max(per_row, 1e-3));
+            t.fused_rows = static_cast<u32>(std::max(64.0, std::min<double>(t.fused_rows_cap, rows)));
         }
     }
     u32* member_err_host = reinterpret_cast<u32*>(ex->host_counts + ex->counts_words + 30);
