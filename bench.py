@@ -225,6 +225,29 @@ def cpu_baseline(workload, edges_cols=None, threads=None):
                       f"restatement of the reference's *_cpu_parallel operators inside RecursiveExecutor::run"}
 
 
+def general_cpu_baseline(cols, delta_rows_total, new_rows, time_cap_s=10.0):
+    """GeneralCpu, the reference's single-threaded nested-loop evaluator, on the
+    same edges: a sample bounded by time_cap_s, extrapolated when it does not
+    converge by the nested loop's tuple tests, (|edge| + 1) per DELTA tuple
+    over every round of the fixpoint (sum|DELTA| from the GPU run's trace)."""
+    import oracle
+
+    src, dst = cols
+    r = oracle.general_tc_c(src, dst, time_cap_s=time_cap_s)
+    edges = len(np.unique((np.asarray(src, dtype=np.uint64) << np.uint64(32)) | np.asarray(dst, dtype=np.uint64)))
+    total_tests = (edges + 1) * int(delta_rows_total)
+    if r["converged"]:
+        seconds, status = r["seconds"], "run to the fixpoint"
+    else:
+        seconds, status = total_tests * r["seconds"] / max(r["tests"], 1), "not run (extrapolated)"
+    return {"value": new_rows / seconds if seconds > 0 else None, "unit": "tuples/s", "cores": 1, "kind": "port",
+            "seconds": seconds, "status": status,
+            "sample": f"{r['tests']:.3g} tuple tests in {r['seconds']:.1f} s ({r['rounds']} whole rounds); the "
+                      f"fixpoint makes (|edge| + 1) x sum|DELTA| = {total_tests:.3g}; restatement of general.rs "
+                      f"execute_scc/evaluate_clause with a plain compare per test (the reference clones a "
+                      f"binding per test), so a lower bound on its time"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -396,6 +419,8 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.workload, (src, dst))
+        cpu["general_cpu"] = general_cpu_baseline((src, dst), sum(r["delta_rows"] for r in pstats["trace"]),
+                                                  new_rows)
     if rank == 0:
         line = {
             "metric": "TC derived tuples/s",

@@ -80,6 +80,11 @@ def lib() -> ctypes.CDLL:
                                              ctypes.POINTER(ctypes.c_int)]
         L.oracle_intern_u32.restype = None
         L.oracle_intern_u32.argtypes = [_u32p, ctypes.c_uint64, _u32p]
+        L.oracle_general_tc.restype = ctypes.c_int
+        L.oracle_general_tc.argtypes = [_u32p, _u32p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_double,
+                                        ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
+                                        ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_double),
+                                        ctypes.POINTER(ctypes.c_int)]
         L.oracle_splitmix64.restype = ctypes.c_uint64
         L.oracle_splitmix64.argtypes = [ctypes.c_uint64, ctypes.c_uint64]
         L.oracle_er_edges.restype = ctypes.c_uint64
@@ -598,6 +603,20 @@ def intern(values, catalog: dict | None = None) -> tuple[np.ndarray, dict]:
             catalog[v] = len(catalog)
         out[i] = catalog[v]
     return out, catalog
+
+
+def general_tc_c(src, dst, max_rounds: int = 10_000, time_cap_s: float = 1e30) -> dict:
+    """GeneralCpu's nested-loop evaluation of transitive closure (oracle.cpp,
+    general.rs:393-536), bounded by rounds and a time cap: completed rounds,
+    their new tuples, the tuple tests made, seconds, and whether it converged."""
+    s = np.ascontiguousarray(src, dtype=np.uint32)
+    d = np.ascontiguousarray(dst, dtype=np.uint32)
+    rounds, new, tests = ctypes.c_uint64(0), ctypes.c_uint64(0), ctypes.c_uint64(0)
+    seconds, converged = ctypes.c_double(0.0), ctypes.c_int(0)
+    lib().oracle_general_tc(_p32(s), _p32(d), len(s), max_rounds, time_cap_s, ctypes.byref(rounds),
+                            ctypes.byref(new), ctypes.byref(tests), ctypes.byref(seconds), ctypes.byref(converged))
+    return {"rounds": rounds.value, "new_rows": new.value, "tests": tests.value, "seconds": seconds.value,
+            "converged": bool(converged.value)}
 
 
 def load_binary_u32_c(data: bytes) -> tuple[np.ndarray, np.ndarray]:

@@ -16,6 +16,8 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
+#include <set>
 #include <cstdint>
 #include <cstring>
 #include <map>
@@ -793,6 +795,68 @@ void oracle_intern_u32(const uint32_t* values, u64 n, uint32_t* ids) {
         if (it == by_value.end()) it = by_value.emplace(values[i], static_cast<uint32_t>(by_value.size())).first;
         ids[i] = it->second;
     }
+}
+
+// GeneralCpu on the transitive-closure program (execute_scc and
+// evaluate_clause, crates/sparkalog-datalog/src/general.rs:393-447 and
+// :478-536): FULL is an ordered set seeded with the edges, DELTA = FULL; a
+// round binds path(x, y) from every DELTA tuple (|DELTA| tests), then tests
+// every edge tuple against y (|DELTA| x |edge| tests: the nested loop),
+// collects (x, z), and keeps the tuples absent from FULL as the next DELTA.
+// Single-threaded, as GeneralCpu is. Stops after max_rounds rounds, or once
+// time_cap_s has passed (checked every 64 DELTA tuples, so a sample can end
+// inside a round). Reports completed rounds, new tuples of those rounds, the
+// tuple tests made and the seconds spent; *converged = 1 if DELTA emptied.
+// A test here is a plain compare, where the reference clones a binding per
+// tested pair, so times measured here bound GeneralCpu's from below.
+int oracle_general_tc(const uint32_t* src, const uint32_t* dst, u64 n, u64 max_rounds, double time_cap_s,
+                      u64* rounds_out, u64* new_out, u64* tests_out, double* seconds_out, int* converged_out) {
+    const auto start = std::chrono::steady_clock::now();
+    auto elapsed = [&] { return std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count(); };
+    std::vector<u64> edges(n);
+    for (u64 i = 0; i < n; ++i) edges[i] = (static_cast<u64>(src[i]) << 32) | dst[i];
+    std::sort(edges.begin(), edges.end());
+    edges.erase(std::unique(edges.begin(), edges.end()), edges.end());
+    std::vector<uint32_t> edge_first(edges.size()), edge_second(edges.size());
+    for (size_t i = 0; i < edges.size(); ++i) {
+        edge_first[i] = static_cast<uint32_t>(edges[i] >> 32);
+        edge_second[i] = static_cast<uint32_t>(edges[i]);
+    }
+    std::set<u64> full(edges.begin(), edges.end());
+    std::vector<u64> delta(edges.begin(), edges.end());
+    u64 rounds = 0, total_new = 0, tests = 0;
+    bool capped = false;
+    const size_t m = edges.size();
+    while (!delta.empty() && rounds < max_rounds && !capped) {
+        std::vector<u64> joined;
+        for (size_t d = 0; d < delta.size(); ++d) {
+            if ((d & 63) == 0 && elapsed() > time_cap_s) {
+                capped = true;
+                break;
+            }
+            const u64 x = delta[d] >> 32;
+            const uint32_t y = static_cast<uint32_t>(delta[d]);
+            tests += 1 + m;
+            for (size_t i = 0; i < m; ++i)
+                if (edge_first[i] == y) joined.push_back((x << 32) | edge_second[i]);
+        }
+        if (capped) break;
+        std::sort(joined.begin(), joined.end());
+        joined.erase(std::unique(joined.begin(), joined.end()), joined.end());
+        std::vector<u64> next;
+        for (u64 t : joined)
+            if (!full.count(t)) next.push_back(t);
+        full.insert(next.begin(), next.end());
+        total_new += next.size();
+        delta.swap(next);
+        ++rounds;
+    }
+    *rounds_out = rounds;
+    *new_out = total_new;
+    *tests_out = tests;
+    *seconds_out = elapsed();
+    *converged_out = delta.empty() ? 1 : 0;
+    return 0;
 }
 
 }  // extern "C"

@@ -232,3 +232,21 @@ def test_load_and_intern_c_restatements_agree():
         assert (e1.value.kind, e1.value.line, e1.value.column) == (e2.value.kind, e2.value.line, e2.value.column)
     v = rng.integers(0, 5000, size=50_000).astype(np.uint32)
     assert np.array_equal(oracle.intern(v)[0], oracle.intern_c(v))
+
+
+def test_general_tc_c_restatement(known_answers):
+    # GeneralCpu's nested loop (general.rs:393-536) in C: the chain of
+    # generic.rs:716-746 and small ER graphs against the operator pipeline.
+    r = oracle.general_tc_c(np.array([1, 2, 3, 4], np.uint32), np.array([2, 3, 4, 5], np.uint32))
+    assert r["converged"] and r["rounds"] == 4 and r["new_rows"] == 6
+    for nodes, edges, seed in [(300, 280, 5), (500, 900, 6)]:
+        s, d = generators.er_edges(nodes, edges, seed)
+        (_, _), it, new = oracle.transitive_closure(s, d)
+        e0, _ = oracle.btree_pairs(s, d)
+        r = oracle.general_tc_c(s, d)
+        assert r["converged"] and r["rounds"] == it and r["new_rows"] == new
+        # Every round tests (|edge| + 1) tuples per DELTA tuple: the figure the
+        # bench extrapolates a capped sample by.
+        assert r["tests"] == (len(e0) + 1) * (len(e0) + new)
+    capped = oracle.general_tc_c(*generators.er_edges(2000, 8000, 1), time_cap_s=0.0)
+    assert not capped["converged"] and capped["rounds"] == 0
