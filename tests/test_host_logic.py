@@ -71,3 +71,23 @@ def test_bench_partition_covers_every_row():
     for r, (s, _) in enumerate(parts):
         if len(s):
             assert s.min() >= 1000 * r // 3 and s.max() < 1000 * (r + 1) // 3
+
+
+def test_bench_baseline_helpers_on_cpu():
+    # The bench's CPU-side helpers (no GPU): the GeneralCpu baseline, converged
+    # and extrapolated, the pipeline-byte formula and the profiled traffic.
+    import bench
+    import oracle
+
+    src, dst = generators.er_edges(300, 280, 5)
+    e0, _ = oracle.btree_pairs(src, dst)
+    (_, _), it, new = oracle.transitive_closure(src, dst)
+    g = bench.general_cpu_baseline((src, dst), len(e0) + new, new, time_cap_s=5.0)
+    assert g["status"] == "run to the fixpoint" and g["cores"] == 1 and g["value"] > 0
+    src, dst = generators.er_edges(2000, 8000, 1)
+    g = bench.general_cpu_baseline((src, dst), 3_837_620, 3_829_620, time_cap_s=0.2)
+    assert g["status"] == "not run (extrapolated)" and g["seconds"] > 0.2
+    trace = [{"delta_rows": 10, "join_rows": 8, "unique_rows": 8, "new_rows": 7, "full_rows": 17}]
+    assert bench.pipeline_bytes(trace) > 0
+    traffic, source = bench.profiled_traffic("anti_join", 26_045_821)
+    assert traffic is None or traffic > 0
