@@ -605,6 +605,136 @@ def intern(values, catalog: dict | None = None) -> tuple[np.ndarray, dict]:
     return out, catalog
 
 
+# ---------------------------------------------------------------------------
+# load_delimited (crates/sparkalog-datalog/src/database.rs:165-177) over
+# parse_delimited_parallel (crates/sparkalog-datalog/src/ingest.rs:20-120):
+# str::lines (split at '\n', a '\r' before it dropped, no piece after a
+# final '\n'), the header line skipped, lines that trim to nothing dropped,
+# then each record split at the delimiter byte: a field starting with '"' is
+# a quoted String ('""' is a quote) that must be followed by the delimiter or
+# the end; any other field is trimmed and is a U32 when it parses as one,
+# else a Symbol. Errors carry the 1-based line and byte column. Values are
+# then interned row by row (ValueCatalog, catalog.rs:98-127), String, Symbol
+# and U32 being distinct keys.
+# ---------------------------------------------------------------------------
+class OracleDelimitedError(Exception):
+    def __init__(self, line: int, column: int, message: str):
+        super().__init__(line, column, message)
+        self.line, self.column, self.message = line, column, message
+
+
+class OracleArityError(Exception):
+    """DatabaseError::Arity (database.rs:98-104): a row with the wrong number of values."""
+
+    def __init__(self, expected: int, actual: int):
+        super().__init__(expected, actual)
+        self.expected, self.actual = expected, actual
+
+
+# char::is_whitespace (the Unicode White_Space property), used by str::trim.
+_RUST_WHITESPACE = set("\t\n\x0b\x0c\r \x85\xa0\u1680\u2028\u2029\u202f\u205f\u3000") | {
+    chr(c) for c in range(0x2000, 0x200B)}
+
+
+def _rust_trim(s: str) -> str:
+    a, b = 0, len(s)
+    while a < b and s[a] in _RUST_WHITESPACE:
+        a += 1
+    while b > a and s[b - 1] in _RUST_WHITESPACE:
+        b -= 1
+    return s[a:b]
+
+
+def _rust_lines(text: str) -> list[str]:
+    # A '\r' is dropped only before a '\n' (str::lines strips "\n", then "\r").
+    pieces = text.split("\n")
+    out = [p[:-1] if p.endswith("\r") else p for p in pieces[:-1]]
+    if pieces[-1]:
+        out.append(pieces[-1])
+    return out
+
+
+def _utf8_len(lead: int) -> int:
+    return 1 if lead < 0x80 else 2 if lead < 0xE0 else 3 if lead < 0xF0 else 4
+
+
+def _parse_record(record: str, line: int, delimiter: int) -> list[tuple]:
+    b = record.encode()
+    n, pos, fields = len(b), 0, []
+    while True:
+        column = pos + 1
+        if pos < n and b[pos] == 0x22:
+            pos += 1
+            value, closed = bytearray(), False
+            while pos < n:
+                if b[pos] == 0x22:
+                    if pos + 1 < n and b[pos + 1] == 0x22:
+                        value += b'"'
+                        pos += 2
+                    else:
+                        pos += 1
+                        closed = True
+                        break
+                else:
+                    step = _utf8_len(b[pos])
+                    value += b[pos:pos + step]
+                    pos += step
+            if not closed:
+                raise OracleDelimitedError(line, column, "unterminated quoted field")
+            fields.append(("string", value.decode()))
+            if pos < n and b[pos] != delimiter:
+                raise OracleDelimitedError(line, pos + 1, "expected delimiter after quoted field")
+        else:
+            start = pos
+            while pos < n and b[pos] != delimiter:
+                pos += 1
+            value = _rust_trim(b[start:pos].decode())
+            if not value:
+                raise OracleDelimitedError(line, column, "empty fields are not values")
+            number = _parse_u32(value)
+            fields.append(("u32", number) if number is not None else ("symbol", value))
+        if pos == n:
+            break
+        pos += 1
+        if pos == n:
+            raise OracleDelimitedError(line, pos, "record ends with an empty field")
+    return fields
+
+
+def parse_delimited(source: str, delimiter: str = ",", has_header: bool = False) -> list[list[tuple]]:
+    """parse_delimited_parallel (ingest.rs:20-41): rows of ("u32", n) /
+    ("string", s) / ("symbol", s) values in input order."""
+    d = ord(delimiter)
+    if chr(d) in " \t\n\x0c\r" and chr(d) != "\t":
+        raise OracleDelimitedError(0, 0, "delimiter must be a visible ASCII byte or tab")
+    rows = []
+    for index, record in enumerate(_rust_lines(source)):
+        if has_header and index == 0:
+            continue
+        if not _rust_trim(record):
+            continue
+        rows.append(_parse_record(record, index + 1, d))
+    return rows
+
+
+def load_delimited(source: str, arity: int, delimiter: str = ",", has_header: bool = False,
+                   catalog: dict | None = None) -> tuple[np.ndarray, dict]:
+    """Database::load_delimited (database.rs:165-177): every row must have
+    `arity` values (Database::insert, :80-110); values are interned in row
+    order. Returns the rows as value ids, shape (rows, arity), and the catalog."""
+    catalog = {} if catalog is None else catalog
+    rows = parse_delimited(source, delimiter, has_header)
+    out = np.empty((len(rows), arity), dtype=np.uint32)
+    for r, row in enumerate(rows):
+        if len(row) != arity:
+            raise OracleArityError(arity, len(row))
+        for c, value in enumerate(row):
+            if value not in catalog:
+                catalog[value] = len(catalog)
+            out[r, c] = catalog[value]
+    return out, catalog
+
+
 def general_tc_c(src, dst, max_rounds: int = 10_000, time_cap_s: float = 1e30) -> dict:
     """GeneralCpu's nested-loop evaluation of transitive closure (oracle.cpp,
     general.rs:393-536), bounded by rounds and a time cap: completed rounds,

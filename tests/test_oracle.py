@@ -250,3 +250,56 @@ def test_general_tc_c_restatement(known_answers):
         assert r["tests"] == (len(e0) + 1) * (len(e0) + new)
     capped = oracle.general_tc_c(*generators.er_edges(2000, 8000, 1), time_cap_s=0.0)
     assert not capped["converged"] and capped["rounds"] == 0
+
+
+def _value(v):
+    return (v[0], v[1])
+
+
+def test_load_delimited_known_answers(known_answers):
+    # parse_delimited_parallel / Database::load_delimited vectors
+    # (ingest.rs:143-181, database.rs:441-457).
+    for case in known_answers["load_delimited"]:
+        text = case.get("text")
+        if text is None:
+            text = "\n".join(case["format"].format(v=v) for v in range(case["generated_rows"]))
+        rows = oracle.parse_delimited(text, case["delimiter"], case["has_header"])
+        if "rows" in case:
+            assert len(rows) == case["rows"], case["source"]
+        for r, length in enumerate(case.get("row_lengths", [])):
+            assert len(rows[r]) == length, case["source"]
+        for r, c, want in case.get("checks", []):
+            got = rows[r] if c is None else rows[r][c]
+            want = [_value(v) for v in want] if c is None else _value(want)
+            assert got == want, case["source"]
+        if "arity" in case:
+            ids, catalog = oracle.load_delimited(text, case["arity"], case["delimiter"], case["has_header"])
+            # path(x, y) :- edge(x, y): the copy has the loaded rows.
+            assert len({tuple(r) for r in ids.tolist()}) == case["path_rows"]
+
+
+def test_load_delimited_errors_and_u32_subset():
+    # Error positions follow parse_record (ingest.rs:43-120): 1-based line,
+    # byte column; a whitespace delimiter other than tab is refused.
+    cases = [("1,", (1, 2, "record ends with an empty field")), ('"ab', (1, 1, "unterminated quoted field")),
+             ('"a"b,1', (1, 4, "expected delimiter after quoted field")),
+             ("1,,2", (1, 3, "empty fields are not values")), ("x\n\n 1 , ", (3, 5, "empty fields are not values"))]
+    for text, (line, column, message) in cases:
+        with pytest.raises(oracle.OracleDelimitedError) as e:
+            oracle.parse_delimited(text)
+        assert (e.value.line, e.value.column, e.value.message) == (line, column, message), text
+    with pytest.raises(oracle.OracleDelimitedError):
+        oracle.parse_delimited("1 2", " ")
+    # Quotes, trimming, CRLF, symbols that only look numeric, u32 overflow.
+    rows = oracle.parse_delimited('"a ""q"" b", x \r\n+7,4294967296\r\n-1,007\n')
+    assert rows == [[("string", 'a "q" b'), ("symbol", "x")], [("u32", 7), ("symbol", "4294967296")],
+                    [("symbol", "-1"), ("u32", 7)]]
+    with pytest.raises(oracle.OracleArityError):
+        oracle.load_delimited("1,2,3\n", 2)
+    # A u32-only file: the same rows and ids as load_binary_u32 + interning.
+    src, dst = generators.er_edges(500, 700, 9)
+    text = "".join(f"{a},{b}\n" for a, b in zip(src.tolist(), dst.tolist()))
+    ids, _ = oracle.load_delimited(text, 2)
+    f, s = oracle.load_binary_u32(text.replace(",", "\t").encode())
+    want, _ = oracle.intern(np.stack([f, s], axis=1).reshape(-1))
+    assert np.array_equal(ids.reshape(-1), want)
