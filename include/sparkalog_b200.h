@@ -350,11 +350,20 @@ enum {
     SPARKALOG_LOAD_OK = 0,
     SPARKALOG_LOAD_GIT_LFS_POINTER = 1,
     SPARKALOG_LOAD_INVALID_FIELD_COUNT = 2,
-    SPARKALOG_LOAD_INVALID_U32 = 3
+    SPARKALOG_LOAD_INVALID_U32 = 3,
+    /* DelimitedError (crates/sparkalog-datalog/src/ingest.rs:43-120), by message */
+    SPARKALOG_LOAD_UNTERMINATED_QUOTE = 4,   /* "unterminated quoted field" */
+    SPARKALOG_LOAD_EXPECTED_DELIMITER = 5,   /* "expected delimiter after quoted field" */
+    SPARKALOG_LOAD_EMPTY_FIELD = 6,          /* "empty fields are not values" */
+    SPARKALOG_LOAD_TRAILING_DELIMITER = 7,   /* "record ends with an empty field" */
+    /* DatabaseError::Arity (crates/sparkalog-datalog/src/database.rs:98-104); column = values in the row */
+    SPARKALOG_LOAD_ARITY = 8,
+    /* a String or Symbol value where this entry point loads u32 relations */
+    SPARKALOG_LOAD_NOT_U32 = 9
 };
 typedef struct sparkalog_load_error {
     int32_t kind;           /* SPARKALOG_LOAD_* */
-    uint32_t column;        /* 1 or 2 for SPARKALOG_LOAD_INVALID_U32 */
+    uint32_t column;        /* 1 or 2 for SPARKALOG_LOAD_INVALID_U32; the 1-based byte column for 4-7 and 9 */
     uint64_t line;          /* 1-based line number */
     uint64_t field_offset;  /* byte offset of the offending field in `text` */
     uint64_t field_length;  /* its length in bytes */
@@ -374,6 +383,26 @@ typedef struct sparkalog_load_error {
 SPARKALOG_API int sparkalog_store_load_binary_u32(sparkalog_store* store, uint32_t id, const char* text, size_t bytes,
                                                   int location, int recursive, size_t* rows,
                                                   sparkalog_load_error* error);
+
+/* Database::load_delimited (crates/sparkalog-datalog/src/database.rs:165-177,
+ * parse_delimited_parallel in crates/sparkalog-datalog/src/ingest.rs:20-120)
+ * for a binary relation of u32 values, parsed on the GPU and inserted as
+ * relation `id` like sparkalog_store_load_binary_u32. Lines are split at
+ * '\n' (a '\r' before it dropped); with has_header the first line is
+ * skipped; lines that trim to nothing are skipped; every other line is a
+ * record split at `delimiter`: a field starting with '"' is a quoted string,
+ * any other is trimmed (Unicode whitespace) and must parse as a u32. A
+ * whitespace delimiter other than tab is SPARKALOG_E_INVALID_ARGUMENT. On a
+ * syntax error anywhere (kinds 4-7, the first failing line) nothing is
+ * inserted and the call returns SPARKALOG_E_LOAD; otherwise the first line
+ * whose record is not two u32 values reports SPARKALOG_LOAD_ARITY or
+ * SPARKALOG_LOAD_NOT_U32 (the reference would intern strings and symbols;
+ * this entry point loads u32 relations only). Values are not interned here:
+ * sparkalog_catalog_intern_u32 over the rows gives Database's value ids. */
+SPARKALOG_API int sparkalog_store_load_delimited_u32(sparkalog_store* store, uint32_t id, const char* text,
+                                                     size_t bytes, int location, unsigned char delimiter,
+                                                     int has_header, int recursive, size_t* rows,
+                                                     sparkalog_load_error* error);
 SPARKALOG_API int sparkalog_executor_stats(sparkalog_executor* executor, sparkalog_kernel_stats* out, int reset);
 
 /* Per-round trace of an executor (the operator cardinalities of each round,

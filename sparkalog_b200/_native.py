@@ -45,6 +45,7 @@ TIER_B = [
     "sparkalog_store_read",
     "sparkalog_store_anti_join",
     "sparkalog_store_load_binary_u32",
+    "sparkalog_store_load_delimited_u32",
     "sparkalog_catalog_create",
     "sparkalog_catalog_destroy",
     "sparkalog_catalog_intern_u32",
@@ -194,6 +195,9 @@ def load() -> ctypes.CDLL:
     L.sparkalog_store_load_binary_u32.argtypes = [vp, ctypes.c_uint32, vp, ctypes.c_size_t, i, i, c_sizep,
                                                    ctypes.POINTER(LoadErrorC)]
     L.sparkalog_store_load_binary_u32.restype = i
+    L.sparkalog_store_load_delimited_u32.argtypes = [vp, ctypes.c_uint32, vp, ctypes.c_size_t, i, ctypes.c_ubyte, i,
+                                                     i, c_sizep, ctypes.POINTER(LoadErrorC)]
+    L.sparkalog_store_load_delimited_u32.restype = i
     L.sparkalog_catalog_create.argtypes = [vp, ctypes.POINTER(vp)]
     L.sparkalog_catalog_create.restype = i
     L.sparkalog_catalog_destroy.argtypes = [vp]

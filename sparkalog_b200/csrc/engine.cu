@@ -1276,10 +1276,137 @@ void describe_load_error(const unsigned char* line, u64 line_offset, u64 len, sp
     }
 }
 
+// parse_record (crates/sparkalog-datalog/src/ingest.rs:43-120) on the one
+// failing line of a delimited text (without the '\r' before its '\n'), for
+// the details: the first syntax error with its 1-based byte column, else a
+// row that does not hold two values, else its first value that is not a u32.
+void describe_delimited_error(const unsigned char* t, u64 offset, u64 len, unsigned char delim,
+                              sparkalog_load_error* e) {
+    u64 pos = 0;
+    u32 fields = 0;
+    bool bad = false;
+    u32 bad_column = 0;
+    u64 bad_begin = 0, bad_len = 0;
+    for (;;) {
+        const u32 column = static_cast<u32>(pos + 1);
+        if (pos < len && t[pos] == '"') {
+            ++pos;
+            bool closed = false;
+            while (pos < len) {
+                if (t[pos] == '"') {
+                    if (pos + 1 < len && t[pos + 1] == '"') {
+                        pos += 2;
+                    } else {
+                        ++pos;
+                        closed = true;
+                        break;
+                    }
+                } else {
+                    ++pos;
+                }
+            }
+            if (!closed) {
+                e->kind = SPARKALOG_LOAD_UNTERMINATED_QUOTE;
+                e->column = column;
+                return;
+            }
+            if (!bad) {
+                bad = true;
+                bad_column = column;
+                bad_begin = column - 1;
+                bad_len = pos - bad_begin;
+            }
+            if (pos < len && t[pos] != delim) {
+                e->kind = SPARKALOG_LOAD_EXPECTED_DELIMITER;
+                e->column = static_cast<u32>(pos + 1);
+                return;
+            }
+        } else {
+            const u64 start = pos;
+            while (pos < len && t[pos] != delim) ++pos;
+            u64 fb = start, fe = pos;
+            spk::unicode_trim(t, &fb, &fe);
+            if (fb == fe) {
+                e->kind = SPARKALOG_LOAD_EMPTY_FIELD;
+                e->column = column;
+                return;
+            }
+            u32 v = 0;
+            if (!bad && !spk::parse_u32_field(t + fb, fe - fb, &v)) {
+                bad = true;
+                bad_column = column;
+                bad_begin = fb;
+                bad_len = fe - fb;
+            }
+        }
+        ++fields;
+        if (pos == len) break;
+        ++pos;
+        if (pos == len) {
+            e->kind = SPARKALOG_LOAD_TRAILING_DELIMITER;
+            e->column = static_cast<u32>(pos);
+            return;
+        }
+    }
+    if (fields != 2) {
+        e->kind = SPARKALOG_LOAD_ARITY;
+        e->column = fields;
+        return;
+    }
+    if (bad) {
+        e->kind = SPARKALOG_LOAD_NOT_U32;
+        e->column = bad_column;
+        e->field_offset = offset + bad_begin;
+        e->field_length = bad_len;
+    }
+}
+
+const char* delimited_message(int kind) {
+    switch (kind) {
+    case SPARKALOG_LOAD_UNTERMINATED_QUOTE: return "unterminated quoted field";
+    case SPARKALOG_LOAD_EXPECTED_DELIMITER: return "expected delimiter after quoted field";
+    case SPARKALOG_LOAD_EMPTY_FIELD: return "empty fields are not values";
+    case SPARKALOG_LOAD_TRAILING_DELIMITER: return "record ends with an empty field";
+    case SPARKALOG_LOAD_ARITY: return "the row does not hold two values";
+    default: return "a value is not a u32 (this entry point loads u32 relations)";
+    }
+}
+
+// A text format for load_text_u32: load_binary_u32's whitespace-separated
+// pairs, or a delimited text (load_delimited) whose values are all u32.
+struct TextFormat {
+    bool delimited = false;
+    unsigned char delim = ',';
+    bool header = false;
+};
+
+int load_text_u32(sparkalog_store* st, u32 id, const char* text, size_t bytes, int location, int recursive,
+                  size_t* rows, sparkalog_load_error* error, const TextFormat& fmt);
+
 }  // namespace
 
 int sparkalog_store_load_binary_u32(sparkalog_store* st, u32 id, const char* text, size_t bytes, int location,
                                     int recursive, size_t* rows, sparkalog_load_error* error) {
+    return load_text_u32(st, id, text, bytes, location, recursive, rows, error, TextFormat{});
+}
+
+int sparkalog_store_load_delimited_u32(sparkalog_store* st, u32 id, const char* text, size_t bytes, int location,
+                                       unsigned char delimiter, int has_header, int recursive, size_t* rows,
+                                       sparkalog_load_error* error) {
+    // parse_delimited_parallel refuses whitespace delimiters other than tab (ingest.rs:24-30).
+    if (delimiter == ' ' || delimiter == '\n' || delimiter == '\f' || delimiter == '\r')
+        return fail(SPARKALOG_E_INVALID_ARGUMENT, "delimiter must be a visible ASCII byte or tab");
+    TextFormat fmt;
+    fmt.delimited = true;
+    fmt.delim = delimiter;
+    fmt.header = has_header != 0;
+    return load_text_u32(st, id, text, bytes, location, recursive, rows, error, fmt);
+}
+
+namespace {
+
+int load_text_u32(sparkalog_store* st, u32 id, const char* text, size_t bytes, int location, int recursive,
+                  size_t* rows, sparkalog_load_error* error, const TextFormat& fmt) {
     if (!st || !rows || (bytes && !text)) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null argument");
     if (st->find(id)) return fail(SPARKALOG_E_DUPLICATE, "relation " + std::to_string(id) + " is already registered");
     if (error) *error = sparkalog_load_error{};
@@ -1335,13 +1462,19 @@ int sparkalog_store_load_binary_u32(sparkalog_store* st, u32 id, const char* tex
                       ops.ex.epoch++, err);
         SPK_CUDA(cudaGetLastError(), "line_ends_kernel");
     }
-    {
-        auto kernel = spk::parse_lines_kernel<kThreads, kLineItems>;
+    auto parse = [&](auto parser) -> int {
+        auto kernel = spk::parse_lines_kernel<kThreads, kLineItems, decltype(parser)>;
         kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, std::max<u64>(line_tiles, 1)), kThreads, 0,
-                 s>>>(dtext, bytes, ops.a.as<u64>(), ends_n, lines, st->scratch_u32[0].as<u32>(),
+                 s>>>(dtext, bytes, ops.a.as<u64>(), ends_n, lines, parser, st->scratch_u32[0].as<u32>(),
                       st->scratch_u32[1].as<u32>(), out_n, first_error, ops.status.as<u64>(),
                       ops.counters.as<u32>() + 1, ops.ex.epoch++, err);
         SPK_CUDA(cudaGetLastError(), "parse_lines_kernel");
+        return 0;
+    };
+    {
+        const int rc = fmt.delimited ? parse(spk::DelimitedLineParser{fmt.delim, fmt.header})
+                                     : parse(spk::BinaryLineParser{});
+        if (rc) return rc;
     }
     SPK_CUDA(cudaMemcpyAsync(ops.host, ops.counts.as<u64>() + 2, 24, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
     SPK_CUDA(cudaMemcpyAsync(ops.host + 3, err, 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
@@ -1349,6 +1482,40 @@ int sparkalog_store_load_binary_u32(sparkalog_store* st, u32 id, const char* tex
     const u64 field_error = ops.host[0], lfs_line = ops.host[1], parsed = ops.host[2];
     const u32 bits = static_cast<u32>(ops.host[3] & 0xffffffffu);
     if (bits) return fail(SPARKALOG_E_DEVICE_FAULT, "device error bits " + std::to_string(bits));
+    // The bytes of line `index` (without its '\n'), copied to the host.
+    auto line_bytes = [&](u64 index, u64* offset, std::vector<unsigned char>* out) -> int {
+        u64 bounds[2] = {0, bytes};
+        if (index > 0)
+            SPK_CUDA(cudaMemcpyAsync(&bounds[0], ops.a.as<u64>() + index - 1, 8, cudaMemcpyDeviceToHost, s),
+                     "cudaMemcpyAsync");
+        if (index < newlines)
+            SPK_CUDA(cudaMemcpyAsync(&bounds[1], ops.a.as<u64>() + index, 8, cudaMemcpyDeviceToHost, s),
+                     "cudaMemcpyAsync");
+        SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+        if (index > 0) bounds[0] += 1;
+        out->resize(bounds[1] - bounds[0]);
+        if (!out->empty())
+            SPK_CUDA(cudaMemcpy(out->data(), dtext + bounds[0], out->size(), cudaMemcpyDefault), "cudaMemcpy");
+        *offset = bounds[0];
+        return 0;
+    };
+    if (fmt.delimited && (field_error != spk::kNoLine || lfs_line != spk::kNoLine)) {
+        // A syntax error anywhere comes first (parse_delimited_parallel
+        // fails before any row is inserted); then the first row that is not
+        // two u32 values.
+        const u64 index = field_error != spk::kNoLine ? field_error : lfs_line;
+        u64 offset = 0;
+        std::vector<unsigned char> line;
+        int rc = line_bytes(index, &offset, &line);
+        if (rc) return rc;
+        if (index < newlines && !line.empty() && line.back() == '\r') line.pop_back();
+        sparkalog_load_error e{};
+        e.line = index + 1;
+        describe_delimited_error(line.data(), offset, line.size(), fmt.delim, &e);
+        if (error) *error = e;
+        return fail(SPARKALOG_E_LOAD, "line " + std::to_string(e.line) + ", column " + std::to_string(e.column) +
+                                          ": " + delimited_message(e.kind));
+    }
     if (lfs_line != spk::kNoLine || field_error != spk::kNoLine) {
         sparkalog_load_error e{};
         if (lfs_line != spk::kNoLine) {
@@ -1357,20 +1524,12 @@ int sparkalog_store_load_binary_u32(sparkalog_store* st, u32 id, const char* tex
             e.line = lfs_line + 1;
         } else {
             // The failing line's bytes, re-read on the host for the details.
-            u64 bounds[2] = {0, bytes};
-            if (field_error > 0)
-                SPK_CUDA(cudaMemcpyAsync(&bounds[0], ops.a.as<u64>() + field_error - 1, 8, cudaMemcpyDeviceToHost, s),
-                         "cudaMemcpyAsync");
-            if (field_error < newlines)
-                SPK_CUDA(cudaMemcpyAsync(&bounds[1], ops.a.as<u64>() + field_error, 8, cudaMemcpyDeviceToHost, s),
-                         "cudaMemcpyAsync");
-            SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
-            if (field_error > 0) bounds[0] += 1;
-            std::vector<unsigned char> line(bounds[1] - bounds[0]);
-            if (!line.empty())
-                SPK_CUDA(cudaMemcpy(line.data(), dtext + bounds[0], line.size(), cudaMemcpyDefault), "cudaMemcpy");
+            u64 offset = 0;
+            std::vector<unsigned char> line;
+            int rc = line_bytes(field_error, &offset, &line);
+            if (rc) return rc;
             e.line = field_error + 1;
-            describe_load_error(line.data(), bounds[0], line.size(), &e);
+            describe_load_error(line.data(), offset, line.size(), &e);
         }
         if (error) *error = e;
         return fail(SPARKALOG_E_LOAD, e.kind == SPARKALOG_LOAD_GIT_LFS_POINTER
@@ -1387,6 +1546,8 @@ int sparkalog_store_load_binary_u32(sparkalog_store* st, u32 id, const char* tex
     return recursive ? sparkalog_store_insert_recursive(st, id, c0, c1, parsed, c0, c1, parsed, SPARKALOG_DEVICE)
                      : sparkalog_store_insert_static(st, id, c0, c1, parsed, SPARKALOG_DEVICE);
 }
+
+}  // namespace
 
 int sparkalog_store_rows(sparkalog_store* st, u32 id, int version, size_t* rows) {
     if (!st || !rows) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null argument");

@@ -14,6 +14,14 @@
 // order (look-back again) into the two output columns. Errors are reduced to
 // the smallest failing line index with atomicMin; the host re-reads that one
 // line to report its details.
+//
+// The same two passes read delimited text for load_delimited
+// (crates/sparkalog-datalog/src/database.rs:165-177 over
+// parse_delimited_parallel, ingest.rs:20-120) when every value is a u32: a
+// line (a '\r' before its '\n' dropped) after the optional header that is
+// not blank is a record, split at the delimiter byte; a field starting with
+// '"' is a quoted string, any other field is trimmed of Unicode whitespace
+// and is a u32 when it parses as one (a symbol otherwise).
 #pragma once
 
 #include "spk_common.cuh"
@@ -25,6 +33,37 @@ constexpr u64 kNoLine = ~0ull;
 
 __device__ __forceinline__ bool ascii_space(unsigned char c) {
     return c == ' ' || c == '\t' || c == '\n' || c == '\v' || c == '\f' || c == '\r';
+}
+
+// Length in bytes of the White_Space character (char::is_whitespace, which
+// str::trim strips) that starts at t[p], reading below `end`; 0 if none.
+__host__ __device__ __forceinline__ int ws_at(const unsigned char* t, u64 p, u64 end) {
+    const unsigned c = t[p];
+    if (c == ' ' || (c >= '\t' && c <= '\r')) return 1;
+    if (c == 0xC2 && p + 1 < end && (t[p + 1] == 0x85 || t[p + 1] == 0xA0)) return 2;  // U+0085, U+00A0
+    if (p + 2 >= end) return 0;
+    const unsigned b1 = t[p + 1], b2 = t[p + 2];
+    if (c == 0xE1 && b1 == 0x9A && b2 == 0x80) return 3;  // U+1680
+    if (c == 0xE2 && b1 == 0x80 && ((b2 >= 0x80 && b2 <= 0x8A) || b2 == 0xA8 || b2 == 0xA9 || b2 == 0xAF))
+        return 3;  // U+2000..U+200A, U+2028, U+2029, U+202F
+    if (c == 0xE2 && b1 == 0x81 && b2 == 0x9F) return 3;  // U+205F
+    if (c == 0xE3 && b1 == 0x80 && b2 == 0x80) return 3;  // U+3000
+    return 0;
+}
+
+// Length of the White_Space character that ends just before t[p], reading at
+// or above `begin`; 0 if none.
+__host__ __device__ __forceinline__ int ws_before(const unsigned char* t, u64 begin, u64 p) {
+    if (p > begin && ws_at(t, p - 1, p) == 1) return 1;
+    if (p >= begin + 2 && ws_at(t, p - 2, p) == 2) return 2;
+    if (p >= begin + 3 && ws_at(t, p - 3, p) == 3) return 3;
+    return 0;
+}
+
+// [*b, *e) trimmed of White_Space at both ends.
+__host__ __device__ __forceinline__ void unicode_trim(const unsigned char* t, u64* b, u64* e) {
+    for (int k; *b < *e && (k = ws_at(t, *b, *e)) > 0;) *b += k;
+    for (int k; *e > *b && (k = ws_before(t, *b, *e)) > 0;) *e -= k;
 }
 
 // *count += number of '\n' bytes (sizes the line-end array).
@@ -73,7 +112,7 @@ __global__ void __launch_bounds__(THREADS) line_ends_kernel(const unsigned char*
 }
 
 // u32 per Rust's from_str: optional '+', at least one decimal digit, no overflow.
-__device__ __forceinline__ bool parse_u32_field(const unsigned char* p, u64 len, u32* out) {
+__host__ __device__ __forceinline__ bool parse_u32_field(const unsigned char* p, u64 len, u32* out) {
     u64 i = 0;
     if (len > 0 && p[0] == '+') i = 1;
     if (i == len) return false;
@@ -123,13 +162,92 @@ __device__ __forceinline__ int parse_line(const unsigned char* text, u64 begin, 
     return 1;
 }
 
+// A line parser returns 0 (skipped line), 1 (a row in *first, *second),
+// 2 (an error of the first class) or 3 (an error of the second class).
+
+// load_binary_u32: class 2 a field-count or u32 error, class 3 the LFS header.
+struct BinaryLineParser {
+    __device__ __forceinline__ int operator()(const unsigned char* text, u64, u64 b, u64 e, bool, u32* first,
+                                              u32* second) const {
+        const int kind = parse_line(text, b, e, first, second);
+        return kind == 4 ? 3 : (kind == 3 ? 2 : kind);
+    }
+};
+
+// One record of parse_record (ingest.rs:43-120) restricted to two u32
+// values: 2 for a syntax error (unterminated quote, no delimiter after a
+// quoted field, an empty field, a trailing delimiter), 3 for a record that
+// parses but is not two u32 values (arity, or a string or symbol value).
+__device__ __forceinline__ int parse_delimited_record(const unsigned char* t, u64 b, u64 e, unsigned char delim,
+                                                      u32* first, u32* second) {
+    u64 pos = b;
+    int fields = 0;
+    bool not_u32 = false;
+    for (;;) {
+        if (pos < e && t[pos] == '"') {
+            ++pos;
+            bool closed = false;
+            while (pos < e) {
+                if (t[pos] == '"') {
+                    if (pos + 1 < e && t[pos + 1] == '"') {
+                        pos += 2;
+                    } else {
+                        ++pos;
+                        closed = true;
+                        break;
+                    }
+                } else {
+                    ++pos;  // UTF-8 continuation bytes are never '"'
+                }
+            }
+            if (!closed) return 2;
+            not_u32 = true;
+            if (pos < e && t[pos] != delim) return 2;
+        } else {
+            const u64 start = pos;
+            while (pos < e && t[pos] != delim) ++pos;
+            u64 fb = start, fe = pos;
+            unicode_trim(t, &fb, &fe);
+            if (fb == fe) return 2;
+            u32 v = 0;
+            if (parse_u32_field(t + fb, fe - fb, &v)) {
+                if (fields == 0) *first = v;
+                if (fields == 1) *second = v;
+            } else {
+                not_u32 = true;
+            }
+        }
+        ++fields;
+        if (pos == e) break;
+        ++pos;
+        if (pos == e) return 2;
+    }
+    return (fields != 2 || not_u32) ? 3 : 1;
+}
+
+// load_delimited: the header line skipped, a '\r' before the '\n' dropped,
+// blank lines skipped, every other line one record.
+struct DelimitedLineParser {
+    unsigned char delim;
+    bool header;
+    __device__ __forceinline__ int operator()(const unsigned char* text, u64 line, u64 b, u64 e, bool newline,
+                                              u32* first, u32* second) const {
+        if (header && line == 0) return 0;
+        if (newline && e > b && text[e - 1] == '\r') --e;
+        u64 tb = b, te = e;
+        unicode_trim(text, &tb, &te);
+        if (tb == te) return 0;
+        return parse_delimited_record(text, b, e, delim, first, second);
+    }
+};
+
 // Line i spans [i == 0 ? 0 : ends[i - 1] + 1, i < ends_n ? ends[i] : bytes).
-// first_error[0] = smallest line index with a field or u32 error,
-// first_error[1] = smallest line index holding the LFS header.
-template <int THREADS, int ITEMS>
+// first_error[0] = smallest line index whose parser returned 2,
+// first_error[1] = smallest line index whose parser returned 3.
+template <int THREADS, int ITEMS, class Parser>
 __global__ void __launch_bounds__(THREADS) parse_lines_kernel(const unsigned char* text, u64 bytes, const u64* ends,
-                                                              const u64* ends_n_ptr, u64 lines, u32* out_first,
-                                                              u32* out_second, u64* out_count,
+                                                              const u64* ends_n_ptr, u64 lines, Parser parser,
+                                                              u32* out_first, u32* out_second, u64* out_count,
                                                               unsigned long long* first_error, u64* status,
                                                               u32* tile_counter, u32 epoch, u32* err) {
     constexpr int kTile = THREADS * ITEMS;
@@ -157,13 +275,13 @@ __global__ void __launch_bounds__(THREADS) parse_lines_kernel(const unsigned cha
             const u64 b = line == 0 ? 0 : ends[line - 1] + 1;
             const u64 e = line < ends_n ? ends[line] : bytes;
             u32 f = 0, s = 0;
-            const int kind = parse_line(text, b, e, &f, &s);
+            const int kind = parser(text, line, b, e, line < ends_n, &f, &s);
             if (kind == 1) {
                 keep |= 1u << i;
                 row[i] = (static_cast<u64>(f) << 32) | s;
-            } else if (kind == 2 || kind == 3) {
+            } else if (kind == 2) {
                 atomicMin(first_error, static_cast<unsigned long long>(line));
-            } else if (kind == 4) {
+            } else if (kind == 3) {
                 atomicMin(first_error + 1, static_cast<unsigned long long>(line));
             }
         }

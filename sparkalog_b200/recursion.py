@@ -47,7 +47,10 @@ class LoadError(GenericExecutionError):
     GitLfsPointer, InvalidFieldCount or InvalidU32, with the 1-based ``line`` and,
     for InvalidU32, the ``column`` and the field's text ``value``."""
 
-    LOAD_KINDS = {1: "GitLfsPointer", 2: "InvalidFieldCount", 3: "InvalidU32"}
+    LOAD_KINDS = {1: "GitLfsPointer", 2: "InvalidFieldCount", 3: "InvalidU32",
+                  # DelimitedError messages (ingest.rs:43-120), DatabaseError::Arity, a non-u32 value
+                  4: "unterminated quoted field", 5: "expected delimiter after quoted field",
+                  6: "empty fields are not values", 7: "record ends with an empty field", 8: "Arity", 9: "NotU32"}
 
     def __init__(self, code: int, message: str, kind: int, line: int, column: int, value: str | None):
         super().__init__(code, message)
@@ -176,6 +179,38 @@ class RelationStore:
         if code == -23:
             value = None
             if err.kind == 3:
+                raw = host if host is not None else text.cpu().numpy()
+                value = bytes(raw[err.field_offset:err.field_offset + err.field_length]).decode(errors="replace")
+            raise LoadError(code, _native.last_error(), err.kind, int(err.line), int(err.column), value)
+        _check(code)
+        return int(rows.value)
+
+    def load_delimited_u32(self, rid: RelationId | int, text, delimiter: str = ",", has_header: bool = False,
+                           recursive: bool = False) -> int:
+        """Database::load_delimited (database.rs:165-177) for a binary relation of u32
+        values, parsed on the GPU; ``text`` is bytes, str, or a uint8 CUDA tensor.
+        Returns the number of rows read. Errors raise LoadError with the reference's
+        line, byte column and message (``kind``)."""
+        L = _native.load()
+        if isinstance(text, str):
+            text = text.encode()
+        if isinstance(text, torch.Tensor):
+            ptr, nbytes, loc, host = text.data_ptr(), int(text.numel()), DEVICE, None
+        else:
+            host = text if isinstance(text, np.ndarray) else np.frombuffer(text, dtype=np.uint8)
+            host = np.ascontiguousarray(host.view(np.uint8).reshape(-1))
+            ptr, nbytes, loc = host.ctypes.data if len(host) else None, len(host), HOST
+        d = delimiter.encode()
+        if len(d) != 1:
+            raise ValueError("the delimiter is one byte")
+        rows = ctypes.c_size_t(0)
+        err = _native.LoadErrorC()
+        code = L.sparkalog_store_load_delimited_u32(self._h, int(getattr(rid, "value", rid)), ptr, nbytes, loc, d[0],
+                                                    1 if has_header else 0, 1 if recursive else 0,
+                                                    ctypes.byref(rows), ctypes.byref(err))
+        if code == -23:
+            value = None
+            if err.kind == 9:
                 raw = host if host is not None else text.cpu().numpy()
                 value = bytes(raw[err.field_offset:err.field_offset + err.field_length]).decode(errors="replace")
             raise LoadError(code, _native.last_error(), err.kind, int(err.line), int(err.column), value)
