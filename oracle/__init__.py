@@ -1,6 +1,6 @@
 """CPU oracle for the sparkalog binary recursive operator pipeline.
 
-TEST INFRASTRUCTURE ONLY: the checker the CUDA path is compared against. Only
+TEST INFRASTRUCTURE ONLY: the reference the CUDA path is compared against. Only
 ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
 ``bench.py`` import this package; the product package never does.
 

@@ -1,7 +1,7 @@
 // CPU oracle for the sparkalog binary recursive operator pipeline.
 //
-// TEST INFRASTRUCTURE ONLY. This library is the checker that the CUDA path is
-// compared against (tests/, __graft_entry__.smoke() and bench.py's CPU
+// TEST INFRASTRUCTURE ONLY. This library is what the CUDA path is compared
+// against (tests/, __graft_entry__.smoke() and bench.py's CPU
 // baseline arm). Nothing in the product package links, loads or calls it.
 //
 // Every function restates the reference's CPU semantics and cites the file and
@@ -419,7 +419,7 @@ u64 oracle_er_edges(u32 n, u64 edges, u64 seed, u32* src, u32* dst) {
     std::vector<u64> accepted;
     accepted.reserve(edges);
     std::vector<u64> seen;  // sorted set of accepted keys
-    // A hash set keeps this O(E); unordered_set of u64 is fine for a checker.
+    // A hash set keeps this O(E); unordered_set of u64 is fine for test code.
     std::vector<u64> table(1, 0);
     size_t mask = 0;
     size_t count = 0;

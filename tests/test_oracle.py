@@ -1,6 +1,6 @@
 """CPU tests: the oracle pinned against the reference's own known answers.
 
-The oracle is only trusted as a checker once it reproduces every known-answer
+The oracle is only trusted for parity once it reproduces every known-answer
 vector of the reference's tests (tests/golden/known_answers.json) and the
 serial/parallel equalities the reference asserts for each operator.
 """
