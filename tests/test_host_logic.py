@@ -91,3 +91,23 @@ def test_bench_baseline_helpers_on_cpu():
     assert bench.pipeline_bytes(trace) > 0
     traffic, source = bench.profiled_traffic("anti_join", 26_045_821)
     assert traffic is None or traffic > 0
+
+
+def test_bench_reference_arm_line():
+    # `bench.py --impl reference` needs no GPU: one JSON line with the keys the
+    # bench contract names, on the small workload.
+    import json
+    import subprocess
+    import sys
+    from pathlib import Path
+
+    root = Path(__file__).resolve().parents[1]
+    out = subprocess.run([sys.executable, str(root / "bench.py"), "--impl", "reference", "--workload", "er_2000_8000",
+                          "--steps", "1", "--warmup", "0"], capture_output=True, text=True, timeout=600, cwd=root)
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = json.loads(out.stdout.strip().splitlines()[-1])
+    for key in ("impl", "metric", "value", "unit", "n_gpus", "steps", "warmup", "higher_is_better", "config",
+                "cpu_baseline", "e2e"):
+        assert key in line, key
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["cpu_baseline"]["cores"] >= 1
