@@ -135,9 +135,20 @@ SPARKALOG_API int sparkalog_anti_join_u32_no_alloc(const uint32_t* left_first, c
                                                    uint32_t* selected, uint32_t* selected_rows,
                                                    uint32_t* output_first, uint32_t* output_second, void* stream);
 
-/* Asynchronous error bits of this device's Tier A kernels (a decoupled
- * look-back that hit its spin cap). No counterpart in the reference, whose
- * CUB kernels have no such wait. reset != 0 clears the bits. */
+/* Error bits of sparkalog_anti_join_u32_no_alloc on the current device (a
+ * look-back wait that hit its spin cap), accumulated over every call since
+ * the last reset; reset != 0 clears them. The bits live in a static device
+ * word that the entry point's per-call clearing never touches, and this
+ * getter reads it with a synchronous symbol copy, so it allocates nothing.
+ * Call it after the stream of the calls it covers has finished. No
+ * counterpart in the reference. */
+SPARKALOG_API int sparkalog_anti_join_u32_no_alloc_error(uint32_t* bits, int reset);
+
+/* Asynchronous error bits of this device's allocating Tier A kernels (a
+ * decoupled look-back that hit its spin cap); the no-alloc anti-join reports
+ * through sparkalog_anti_join_u32_no_alloc_error instead. No counterpart in
+ * the reference, whose CUB kernels have no such wait. reset != 0 clears the
+ * bits. */
 SPARKALOG_API int sparkalog_b200_device_error(uint32_t* bits, int reset);
 
 /* ------------------------------------------------------------------------ */

@@ -34,6 +34,7 @@ TIER_A = [
     "sparkalog_union_u32_temporary_bytes",
     "sparkalog_union_u32",
     "sparkalog_anti_join_u32_no_alloc",
+    "sparkalog_anti_join_u32_no_alloc_error",
     "sparkalog_b200_device_error",
 ]
 TIER_B = [
@@ -174,6 +175,7 @@ def load() -> ctypes.CDLL:
     declare_operator_abi(L)
     L.sparkalog_anti_join_u32_no_alloc.argtypes = [vp, vp, ctypes.c_size_t, vp, vp, ctypes.c_size_t, vp, vp, vp,
                                                    vp, vp, vp]
+    L.sparkalog_anti_join_u32_no_alloc_error.argtypes = [c_u32p, i]
     L.sparkalog_b200_device_error.argtypes = [c_u32p, i]
     for name in TIER_A:
         getattr(L, name).restype = i
