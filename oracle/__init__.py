@@ -25,6 +25,7 @@ of the operator ABI when it is present.
 from __future__ import annotations
 
 import ctypes
+import os
 import subprocess
 from dataclasses import dataclass, field
 from pathlib import Path
@@ -58,11 +59,19 @@ class OracleRulePlan(ctypes.Structure):
     ]
 
 
+def reference_root() -> Path:
+    """The reference checkout: $SPARKALOG_REFERENCE, else a directory named
+    ``reference`` beside this repository's root (the Makefile's default)."""
+    env = os.environ.get("SPARKALOG_REFERENCE")
+    return Path(env) if env else ORACLE_DIR.parent.parent / "reference"
+
+
 def build() -> None:
     """Compiles liboracle.so (and the reference CUDA library when the reference tree exists)."""
     subprocess.run(["make", "-s", "-C", str(ORACLE_DIR), "liboracle.so"], check=True)
-    if Path("/root/reference/crates/sparkalog-execution/native/column_ops.cu").exists():
-        subprocess.run(["make", "-s", "-C", str(ORACLE_DIR), "reference"], check=True)
+    ref = reference_root()
+    if (ref / "crates/sparkalog-execution/native/column_ops.cu").exists():
+        subprocess.run(["make", "-s", "-C", str(ORACLE_DIR), "reference", f"REFERENCE={ref}"], check=True)
 
 
 _lib = None
