@@ -340,6 +340,29 @@ SPARKALOG_API int sparkalog_executor_set_fused(sparkalog_executor* executor, int
  * reference. */
 SPARKALOG_API int sparkalog_executor_set_member_set(sparkalog_executor* executor, int enable);
 
+/* Launch shapes and thresholds of the executor's kernels, chosen per device
+ * by the autotuner (sparkalog_b200/autotune.py) on a short calibration
+ * fixpoint. Every value gives identical results; only speed changes. The
+ * reference fixes its analogue at compile time for one GPU
+ * (crates/sparkalog-execution/src/placement.rs:34-38). */
+typedef struct sparkalog_tuning {
+    uint32_t dir_rows_log2;       /* 2^k rows per bucket of a FULL level's directory (0-10) */
+    uint32_t group_lanes;         /* lanes that search one candidate together: 4, 8 or 16 */
+    uint64_t group_candidates;    /* candidate bound up to which the group search runs */
+    uint64_t sparse_candidates;   /* ... up to which the per-thread search runs; above: staged slices */
+    uint32_t fused_rows_cap;      /* DELTA rows per fused join tile, at most (64-768) */
+    uint32_t merge_items;         /* rows per thread of a merge tile: 7, 11 or 15 */
+    uint32_t level_ratio;         /* a FULL level merges down past 1/ratio of the next (2-64) */
+    uint32_t levels;              /* sorted runs that hold a recursive FULL (2-4) */
+} sparkalog_tuning;
+
+/* The built-in defaults (measured on a B200). */
+SPARKALOG_API int sparkalog_tuning_defaults(sparkalog_tuning* out);
+/* Replaces the executor's tuning; SPARKALOG_E_INVALID_ARGUMENT for a value
+ * outside the ranges above. Takes effect at the next run or step. */
+SPARKALOG_API int sparkalog_executor_set_tuning(sparkalog_executor* executor, const sparkalog_tuning* tuning);
+SPARKALOG_API int sparkalog_executor_get_tuning(sparkalog_executor* executor, sparkalog_tuning* out);
+
 /* Device value catalog: ValueCatalog (crates/sparkalog-datalog/src/
  * catalog.rs:98-127) for u32 values. intern gives every value of the batch
  * its dense id, new values numbered by first appearance after the catalog's

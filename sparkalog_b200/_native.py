@@ -65,6 +65,9 @@ TIER_B = [
     "sparkalog_executor_set_profiling",
     "sparkalog_executor_set_fused",
     "sparkalog_executor_set_member_set",
+    "sparkalog_tuning_defaults",
+    "sparkalog_executor_set_tuning",
+    "sparkalog_executor_get_tuning",
     "sparkalog_executor_stats",
     "sparkalog_executor_trace",
     "sparkalog_reserve_device_memory",
@@ -102,6 +105,24 @@ class SccSummaryC(ctypes.Structure):
         ("relation_ids", c_u32p),
         ("relation_rows", c_u64p),
     ]
+
+
+class TuningC(ctypes.Structure):
+    """sparkalog_tuning."""
+
+    _fields_ = [
+        ("dir_rows_log2", ctypes.c_uint32),
+        ("group_lanes", ctypes.c_uint32),
+        ("group_candidates", ctypes.c_uint64),
+        ("sparse_candidates", ctypes.c_uint64),
+        ("fused_rows_cap", ctypes.c_uint32),
+        ("merge_items", ctypes.c_uint32),
+        ("level_ratio", ctypes.c_uint32),
+        ("levels", ctypes.c_uint32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: int(getattr(self, name)) for name, _ in self._fields_}
 
 
 KERNEL_CLASSES = ["join", "sort_histogram", "sort_pass", "anti_join", "merge", "index", "join_distinct"]
@@ -240,6 +261,12 @@ def load() -> ctypes.CDLL:
     L.sparkalog_executor_set_fused.restype = i
     L.sparkalog_executor_set_member_set.argtypes = [vp, i]
     L.sparkalog_executor_set_member_set.restype = i
+    L.sparkalog_tuning_defaults.argtypes = [ctypes.POINTER(TuningC)]
+    L.sparkalog_tuning_defaults.restype = i
+    L.sparkalog_executor_set_tuning.argtypes = [vp, ctypes.POINTER(TuningC)]
+    L.sparkalog_executor_set_tuning.restype = i
+    L.sparkalog_executor_get_tuning.argtypes = [vp, ctypes.POINTER(TuningC)]
+    L.sparkalog_executor_get_tuning.restype = i
     L.sparkalog_executor_stats.argtypes = [vp, ctypes.POINTER(KernelStatsC), i]
     L.sparkalog_executor_stats.restype = i
     L.sparkalog_executor_trace.argtypes = [vp, ctypes.POINTER(RoundTraceC), ctypes.c_size_t, c_sizep, i]

@@ -181,22 +181,36 @@ constexpr int kLevelStage = 2048;  // level rows per shared-memory chunk of the 
 constexpr int kSparseThreads = 256;  // anti-join of small candidate sets
 constexpr int kSparseItems = 4;
 constexpr int kSparseTile = kSparseThreads * kSparseItems;
-// Candidate bounds up to this use the group-searched anti-join (8 lanes per
-// candidate): latency-bound rounds (on the 16.7M-node ER fixpoint, 2^17
-// took 18.75 ms against 18.86 ms for 2^15 and 18.77 ms for 2^19).
-constexpr u64 kWideCandidates = 1ull << 17;
-constexpr int kWideThreads = 256;
-constexpr int kWideGroup = 8;
-constexpr int kWideTile = kWideThreads / kWideGroup;
-constexpr u64 kSparseCandidates = 1ull << 26;
+constexpr int kWideThreads = 256;    // group-searched anti-join (lanes per candidate: tuning.group_lanes)
 constexpr int kMergeItems = 8;
 constexpr int kMergeTile = kThreads * kMergeItems;
 constexpr int kSortThreads = spk::RadixSortConfig::kThreads;
 constexpr int kSortItems = spk::RadixSortConfig::kItems;
 constexpr int kSortTile = spk::RadixSortConfig::kTile;
-// A level is merged into the next larger one once it holds more than
-// 1/kLevelRatio of that level's rows.
-constexpr u64 kLevelRatio = 4;
+
+// Built-in tuning (sparkalog_tuning in the header). Candidate bounds up to
+// group_candidates use the group-searched anti-join, whose rounds are
+// latency-bound; on the 16.7M-node ER fixpoint 2^17 took 18.75 ms against
+// 18.86 ms for 2^15 and 18.77 ms for 2^19 with 64-row directory buckets.
+sparkalog_tuning default_tuning() {
+    sparkalog_tuning t{};
+    t.dir_rows_log2 = 6;
+    t.group_lanes = 8;
+    t.group_candidates = 1ull << 17;
+    t.sparse_candidates = 1ull << 26;
+    t.fused_rows_cap = 672;
+    t.merge_items = 8;
+    t.level_ratio = 4;
+    t.levels = 3;
+    return t;
+}
+
+bool tuning_valid(const sparkalog_tuning& t) {
+    const bool lanes = t.group_lanes == 4 || t.group_lanes == 8 || t.group_lanes == 16;
+    return t.dir_rows_log2 <= 10 && lanes && t.fused_rows_cap >= 64 && t.fused_rows_cap <= 768 &&
+           t.merge_items == 8 && t.level_ratio >= 2 && t.level_ratio <= 64 && t.levels >= 2 &&
+           t.levels <= static_cast<u32>(spk::kMaxLevels) && t.group_candidates <= t.sparse_candidates;
+}
 
 // A stream-ordered device allocation that only grows.
 struct DevArray {
@@ -254,13 +268,13 @@ struct RelState {
     bool sorted = true;     // level[0] as inserted is non-decreasing
     bool has_dups = false;  // level[0] as inserted has adjacent duplicates
     DevArray level[spk::kMaxLevels];
-    u64 level_n[spk::kMaxLevels] = {0, 0, 0};
+    u64 level_n[spk::kMaxLevels] = {};
     // Bucket directories of the levels (see spk::Levels), rebuilt lazily
     // after a level changes.
     DevArray dir[spk::kMaxLevels];
-    bool dir_valid[spk::kMaxLevels] = {false, false, false};
-    u32 dir_shift[spk::kMaxLevels] = {0, 0, 0};
-    u64 dir_buckets[spk::kMaxLevels] = {0, 0, 0};
+    bool dir_valid[spk::kMaxLevels] = {};
+    u32 dir_shift[spk::kMaxLevels] = {};
+    u64 dir_buckets[spk::kMaxLevels] = {};
     DevArray spare;         // merge destination, swapped with a level after a merge
     DevArray delta, newt;
     u64 delta_n = 0;
@@ -292,6 +306,8 @@ struct sparkalog_store {
     DevArray flags;            // device flag words
     DevArray merge_splits;     // diagonal splits of the merge pre-pass
     u32 max_value = 0;         // largest value stored in any column
+    u32 dir_rows_log2 = 6;     // ~2^k rows per level-directory bucket
+    u32 levels = 3;            // sorted runs of a recursive FULL (the last executor run's tuning)
     StoreOps* ops = nullptr;   // scratch of store-level operations (anti-join, append, segments)
     u32* pinned = nullptr;     // small pinned host buffer
 
@@ -386,11 +402,11 @@ int pack_columns(sparkalog_store* st, const u32* c0, const u32* c1, size_t rows,
 
 // Rebuilds the bucket directory of every non-empty level whose rows changed.
 // The bucket width comes from the store's largest value, which bounds every
-// key: ~64 rows per bucket.
+// key: ~2^dir_rows_log2 rows per bucket.
 void directory_shape(const sparkalog_store* st, u64 rows, u32* shift, u64* buckets) {
     const u64 key_max = (static_cast<u64>(st->max_value) << 32) | st->max_value;
     const int key_bits = 64 - __builtin_clzll(key_max | 1);
-    const int target_bits = 64 - __builtin_clzll(std::max<u64>(rows / 64, 1));
+    const int target_bits = 64 - __builtin_clzll(std::max<u64>(rows >> st->dir_rows_log2, 1));
     *shift = static_cast<u32>(std::max(0, key_bits - target_bits));
     *buckets = (key_max >> *shift) + 1;
 }
@@ -576,6 +592,7 @@ struct sparkalog_executor {
     };
     bool profiling = false;
     bool fused_enabled = true;
+    sparkalog_tuning tuning = default_tuning();
     // `counters` holds, in this order: the per-round tile counters
     // (kCounterWords u32), the per-target counts (counts_words u64), the error
     // word and the fused kernels' fallback flags, then a few words that the
@@ -950,6 +967,39 @@ int build_index_impl(sparkalog_executor* ex, sparkalog_store* st, IndexCache& ic
 }
 
 bool valid_cols(const u32 c[2]) { return c[0] <= 1 && c[1] <= 1; }
+
+// Cascade after TAIL grew: a level merges down once it outgrows
+// 1/level_ratio of the next (an empty next level just takes it).
+int cascade_levels(sparkalog_executor* ex, sparkalog_store* st, RelState& tr) {
+    cudaStream_t s = st->stream;
+    const int tail = static_cast<int>(ex->tuning.levels) - 1;
+    for (int l = tail; l > 0; --l) {
+        if (tr.level_n[l] == 0 || tr.level_n[l] * ex->tuning.level_ratio <= tr.level_n[l - 1]) continue;
+        if (tr.level_n[l - 1] == 0) {
+            swap_arrays(tr.level[l - 1], tr.level[l]);
+            swap_arrays(tr.dir[l - 1], tr.dir[l]);
+            std::swap(tr.dir_valid[l - 1], tr.dir_valid[l]);
+            std::swap(tr.dir_shift[l - 1], tr.dir_shift[l]);
+            std::swap(tr.dir_buckets[l - 1], tr.dir_buckets[l]);
+            tr.level_n[l - 1] = tr.level_n[l];
+            tr.level_n[l] = 0;
+            continue;
+        }
+        const u64 mn = tr.level_n[l - 1] + tr.level_n[l];
+        u64 launched = 0;
+        int rc = merge_buffers(st, tr, l - 1, mn, s);
+        if (rc) return rc;
+        const int tm = ex->begin(SPARKALOG_K_MERGE, s);
+        rc = merge_into_level(st, tr, l - 1, tr.level[l - 1].as<u64>(), tr.level_n[l - 1], tr.level[l].as<u64>(),
+                              tr.level_n[l], s, &launched);
+        if (rc) return rc;
+        ex->end(tm, s, 16.0 * static_cast<double>(mn), launched);
+        ex->stats.total_launches += launched;
+        tr.level_n[l] = 0;
+        tr.dir_valid[l] = false;
+    }
+    return 0;
+}
 
 }  // namespace
 
@@ -1661,7 +1711,7 @@ int sparkalog_store_append(sparkalog_store* st, u32 id, const u32* first, const 
             return fail(SPARKALOG_E_TOO_MANY_ROWS, "relation would exceed 2^32 - 1 rows (u32 row ids)");
         // FULL: new rows are disjoint from every level, so they merge into TAIL
         // (level 0 for a static relation, which keeps a single run).
-        const int l = r->recursive ? spk::kMaxLevels - 1 : 0;
+        const int l = r->recursive ? static_cast<int>(st->levels) - 1 : 0;
         const u64 tn = r->level_n[l] + fresh_n;
         SPK_CUDA(r->spare.ensure(tn * 8, s), "cudaMallocAsync");
         SPK_CUDA(launch_merge(r->level[l].as<u64>(), r->level_n[l], fresh.as<u64>(), fresh_n, r->spare.as<u64>(),
@@ -1998,6 +2048,29 @@ int sparkalog_executor_set_member_set(sparkalog_executor* ex, int enable) {
     return 0;
 }
 
+int sparkalog_tuning_defaults(sparkalog_tuning* out) {
+    if (!out) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null output");
+    *out = default_tuning();
+    return 0;
+}
+
+int sparkalog_executor_set_tuning(sparkalog_executor* ex, const sparkalog_tuning* tuning) {
+    if (!ex || !tuning) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null argument");
+    if (!tuning_valid(*tuning)) return fail(SPARKALOG_E_INVALID_ARGUMENT, "tuning value out of range");
+    ex->tuning = *tuning;
+    for (auto& t : ex->targets) {
+        t.fused_rows_cap = tuning->fused_rows_cap;
+        t.fused_rows = std::min(t.fused_rows, t.fused_rows_cap);
+    }
+    return 0;
+}
+
+int sparkalog_executor_get_tuning(sparkalog_executor* ex, sparkalog_tuning* out) {
+    if (!ex || !out) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null argument");
+    *out = ex->tuning;
+    return 0;
+}
+
 int sparkalog_executor_stats(sparkalog_executor* ex, sparkalog_kernel_stats* out, int reset) {
     if (!ex || !out) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null argument");
     *out = ex->stats;
@@ -2025,6 +2098,15 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
             p.anti_right[0] != 0 || p.anti_right[1] != 1 || p.union_left[0] != 0 || p.union_left[1] != 1 ||
             p.union_right[0] != 0 || p.union_right[1] != 1)
             return fail(SPARKALOG_E_INVALID_ARGUMENT, "set operators must use columns [0, 1]");
+    }
+    // The directory granularity is the store's (its levels carry their
+    // directories): a different one invalidates them, and they are rebuilt
+    // on first use.
+    st->levels = ex->tuning.levels;
+    if (st->dir_rows_log2 != ex->tuning.dir_rows_log2) {
+        st->dir_rows_log2 = ex->tuning.dir_rows_log2;
+        for (auto& kv : st->relations)
+            for (int l = 0; l < spk::kMaxLevels; ++l) kv.second.dir_valid[l] = false;
     }
     u32* counters = ex->tile_counters();
     u32* err = ex->err_words();
@@ -2074,6 +2156,21 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                 r.dir_valid[0] = false;
                 r.member_valid = false;
             }
+        }
+    }
+
+    // Levels past the tuning's count (rows appended into the last slot, or a
+    // smaller count than the last run's) fold into the tuning's TAIL.
+    for (u32 id : ex->relations) {
+        RelState& r = *st->find(id);
+        const int tail = static_cast<int>(ex->tuning.levels) - 1;
+        for (int l = tail + 1; l < spk::kMaxLevels; ++l) {
+            if (r.level_n[l] == 0) continue;
+            int rc = merge_into_level(st, r, tail, r.level[tail].as<u64>(), r.level_n[tail], r.level[l].as<u64>(),
+                                      r.level_n[l], s, nullptr);
+            if (rc) return rc;
+            r.level_n[l] = 0;
+            r.dir_valid[l] = false;
         }
     }
 
@@ -2146,9 +2243,10 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                 // One status word per anti-join tile (the sparse kernel's
                 // tiles are the smallest)...
                 max_status_words = std::max<size_t>(max_status_words, (t.j_cap + kSparseTile - 1) / kSparseTile + 1);
-                // ...or the group-searched kernel's, over at most kWideCandidates.
-                const u64 wide = std::min<u64>(t.j_cap, kWideCandidates);
-                max_status_words = std::max<size_t>(max_status_words, (wide + kWideTile - 1) / kWideTile + 1);
+                // ...or the group-searched kernel's, over at most group_candidates.
+                const u64 wide = std::min<u64>(t.j_cap, ex->tuning.group_candidates);
+                const u64 wide_tile = kWideThreads / ex->tuning.group_lanes;
+                max_status_words = std::max<size_t>(max_status_words, (wide + wide_tile - 1) / wide_tile + 1);
                 // ...and per fused tile, which are DELTA-row tiles.
                 u64 delta_rows = 0;
                 for (size_t k : t.rules) delta_rows += ex->host_rule_delta[k];
@@ -2323,17 +2421,20 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                                                tr.newt.as<u64>(), tc + t.rules.size() + 1, ex->status.as<u64>(),
                                                counters + counter_slot++, ex->epoch++, err, unique_word);
                     SPK_CUDA(cudaGetLastError(), "anti_join_member_kernel");
-                } else if (cand_bound <= kWideCandidates) {
-                    // A few candidates: lookup latency dominates, so 8 lanes
-                    // search each one together.
-                    auto kernel = spk::anti_join_levels_wide_kernel<kWideThreads, kWideGroup>;
-                    const size_t tiles = (cand_bound + kWideTile - 1) / kWideTile;
+                } else if (cand_bound <= ex->tuning.group_candidates) {
+                    // A few candidates: lookup latency dominates, so a group
+                    // of lanes searches each one together.
+                    auto kernel = spk::anti_join_levels_wide_kernel<kWideThreads, 8>;
+                    if (ex->tuning.group_lanes == 4) kernel = spk::anti_join_levels_wide_kernel<kWideThreads, 4>;
+                    if (ex->tuning.group_lanes == 16) kernel = spk::anti_join_levels_wide_kernel<kWideThreads, 16>;
+                    const u64 wide_tile = kWideThreads / ex->tuning.group_lanes;
+                    const size_t tiles = (cand_bound + wide_tile - 1) / wide_tile;
                     kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kWideThreads, std::max<size_t>(tiles, 1)),
                              kWideThreads, 0, s>>>(cand, t.j_b.as<u64>(), cand_sel, jn, lv, tr.newt.as<u64>(),
                                                    tc + t.rules.size() + 1, ex->status.as<u64>(),
                                                    counters + counter_slot++, ex->epoch++, err, unique_word);
                     SPK_CUDA(cudaGetLastError(), "anti_join_levels_wide_kernel");
-                } else if (cand_bound <= kSparseCandidates) {
+                } else if (cand_bound <= ex->tuning.sparse_candidates) {
                     // Few candidates, far apart in every level: look each up
                     // in all levels at once.
                     auto kernel = spk::anti_join_levels_sparse_kernel<kSparseThreads, kSparseItems>;
@@ -2447,7 +2548,7 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
             const u64 newt_n = ex->host_counts[target_count_base(ex, ti) + t.rules.size() + 1];
             if (newt_n > 0) {
                 // TAIL <- TAIL u NEWT
-                const int tail = spk::kMaxLevels - 1;
+                const int tail = static_cast<int>(ex->tuning.levels) - 1;
                 const u64 tn = tr.level_n[tail] + newt_n;
                 {
                     u64 launched = 0;
@@ -2460,32 +2561,8 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                     ex->end(tm, s, 16.0 * static_cast<double>(tn), launched);
                     ex->stats.total_launches += launched;
                 }
-                // Cascade: a level merges down once it outgrows 1/kLevelRatio of the next.
-                for (int l = tail; l > 0; --l) {
-                    if (tr.level_n[l] == 0 || tr.level_n[l] * kLevelRatio <= tr.level_n[l - 1]) continue;
-                    if (tr.level_n[l - 1] == 0) {
-                        swap_arrays(tr.level[l - 1], tr.level[l]);
-                        swap_arrays(tr.dir[l - 1], tr.dir[l]);
-                        std::swap(tr.dir_valid[l - 1], tr.dir_valid[l]);
-                        std::swap(tr.dir_shift[l - 1], tr.dir_shift[l]);
-                        std::swap(tr.dir_buckets[l - 1], tr.dir_buckets[l]);
-                        tr.level_n[l - 1] = tr.level_n[l];
-                        tr.level_n[l] = 0;
-                        continue;
-                    }
-                    const u64 mn = tr.level_n[l - 1] + tr.level_n[l];
-                    u64 launched = 0;
-                    int rc = merge_buffers(st, tr, l - 1, mn, s);
-                    if (rc) return rc;
-                    const int tm = ex->begin(SPARKALOG_K_MERGE, s);
-                    rc = merge_into_level(st, tr, l - 1, tr.level[l - 1].as<u64>(), tr.level_n[l - 1],
-                                              tr.level[l].as<u64>(), tr.level_n[l], s, &launched);
-                    if (rc) return rc;
-                    ex->end(tm, s, 16.0 * static_cast<double>(mn), launched);
-                    ex->stats.total_launches += launched;
-                    tr.level_n[l] = 0;
-                    tr.dir_valid[l] = false;
-                }
+                int rc = cascade_levels(ex, st, tr);
+                if (rc) return rc;
             }
             {
                 // FULL's hash set takes the round's new rows (or is dropped

@@ -14,7 +14,7 @@
 
 namespace spk {
 
-constexpr int kMaxLevels = 3;
+constexpr int kMaxLevels = 4;
 
 // A level's bucket directory: dir[b] = first row whose key >> shift >= b, for
 // b in [0, buckets]; about 64 rows per bucket. It turns a search over a level

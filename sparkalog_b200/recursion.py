@@ -295,7 +295,14 @@ class RecursiveExecutor:
         h = ctypes.c_void_p()
         _check(_native.load().sparkalog_executor_compile(store.handle, rel.ctypes.data_as(_native.c_u32p), len(rel),
                                                          rules, len(plan.rules), ctypes.byref(h)))
-        return cls(h, plan)
+        ex = cls(h, plan)
+        # The autotuner's saved choice for this device, when there is one.
+        from . import autotune
+
+        tuned = autotune.saved_tuning()
+        if tuned is not None:
+            ex.set_tuning(tuned)
+        return ex
 
     def close(self) -> None:
         h, self._h = getattr(self, "_h", None), None
@@ -374,6 +381,22 @@ class RecursiveExecutor:
     def set_member_set(self, enable: bool) -> None:
         """Enables or disables (default) FULL's hash set for the anti-join; results are identical."""
         _check(_native.load().sparkalog_executor_set_member_set(self._h, 1 if enable else 0))
+
+    def tuning(self) -> dict:
+        """The executor's launch shapes and thresholds (sparkalog_tuning)."""
+        t = _native.TuningC()
+        _check(_native.load().sparkalog_executor_get_tuning(self._h, ctypes.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, tuning: dict) -> None:
+        """Replaces some or all tuning values; results are identical for every valid value."""
+        t = _native.TuningC()
+        _check(_native.load().sparkalog_executor_get_tuning(self._h, ctypes.byref(t)))
+        for name, value in tuning.items():
+            if name not in dict(_native.TuningC._fields_):
+                raise KeyError(f"unknown tuning value {name!r}")
+            setattr(t, name, int(value))
+        _check(_native.load().sparkalog_executor_set_tuning(self._h, ctypes.byref(t)))
 
     def stats(self, reset: bool = False) -> dict:
         """Per-kernel-class launches, milliseconds and algorithmic bytes, plus total launches."""
