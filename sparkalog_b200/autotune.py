@@ -48,6 +48,7 @@ SPACE: dict[str, list[int]] = {
     "fused_rows_cap": [384, 512, 672, 768],
     "level_ratio": [3, 4, 6, 8],
     "levels": [3, 4],
+    "merge_items": [7, 11, 15],
 }
 
 

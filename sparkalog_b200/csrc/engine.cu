@@ -182,8 +182,6 @@ constexpr int kSparseThreads = 256;  // anti-join of small candidate sets
 constexpr int kSparseItems = 4;
 constexpr int kSparseTile = kSparseThreads * kSparseItems;
 constexpr int kWideThreads = 256;    // group-searched anti-join (lanes per candidate: tuning.group_lanes)
-constexpr int kMergeItems = 8;
-constexpr int kMergeTile = kThreads * kMergeItems;
 constexpr int kSortThreads = spk::RadixSortConfig::kThreads;
 constexpr int kSortItems = spk::RadixSortConfig::kItems;
 constexpr int kSortTile = spk::RadixSortConfig::kTile;
@@ -199,7 +197,7 @@ sparkalog_tuning default_tuning() {
     t.group_candidates = 1ull << 17;
     t.sparse_candidates = 1ull << 26;
     t.fused_rows_cap = 672;
-    t.merge_items = 8;
+    t.merge_items = 11;
     t.level_ratio = 4;
     t.levels = 3;
     return t;
@@ -208,7 +206,7 @@ sparkalog_tuning default_tuning() {
 bool tuning_valid(const sparkalog_tuning& t) {
     const bool lanes = t.group_lanes == 4 || t.group_lanes == 8 || t.group_lanes == 16;
     return t.dir_rows_log2 <= 10 && lanes && t.fused_rows_cap >= 64 && t.fused_rows_cap <= 768 &&
-           t.merge_items == 8 && t.level_ratio >= 2 && t.level_ratio <= 64 && t.levels >= 2 &&
+           (t.merge_items == 7 || t.merge_items == 11 || t.merge_items == 15) && t.level_ratio >= 2 && t.level_ratio <= 64 && t.levels >= 2 &&
            t.levels <= static_cast<u32>(spk::kMaxLevels) && t.group_candidates <= t.sparse_candidates;
 }
 
@@ -307,6 +305,8 @@ struct sparkalog_store {
     DevArray merge_splits;     // diagonal splits of the merge pre-pass
     u32 max_value = 0;         // largest value stored in any column
     u32 dir_rows_log2 = 6;     // ~2^k rows per level-directory bucket
+    u32 merge_items = 11;      // rows per thread of a merge tile
+    DevArray fault;            // u32 error bits of the store's merges (read when a run ends)
     u32 levels = 3;            // sorted runs of a recursive FULL (the last executor run's tuning)
     StoreOps* ops = nullptr;   // scratch of store-level operations (anti-join, append, segments)
     u32* pinned = nullptr;     // small pinned host buffer
@@ -330,37 +330,89 @@ unsigned simple_grid(size_t n) {
 }
 
 // Merge of two disjoint sorted runs into `out` (capacity checked by caller):
-// a parallel diagonal-split pre-pass, then the merge. Returns the number of
-// kernels launched through *launches.
-cudaError_t launch_merge(const u64* a, u64 na, const u64* b, u64 nb, u64* out, DevArray& splits, cudaStream_t s,
-                         u64* launches = nullptr, spk::MergeDirectory md = spk::MergeDirectory{nullptr, 0, 0}) {
+// the diagonal splits (one warp per diagonal), then the bulk-copy merge with
+// `items` rows per thread (7, 11 or 15). Returns the number of kernels
+// launched through *launches. Errors of the merge's barrier waits go to *err.
+template <int ITEMS>
+cudaError_t launch_merge_items(const u64* a, u64 na, const u64* b, u64 nb, u64* out, DevArray& splits,
+                               cudaStream_t s, u32* err, spk::MergeDirectory md) {
+    constexpr int kTile = kThreads * ITEMS;
+    using Layout = spk::MergeBulkLayout<kThreads, ITEMS>;
+    auto kernel = spk::merge_bulk_kernel<kThreads, ITEMS>;
     const u64 total = na + nb;
-    if (launches) *launches = 0;
-    if (total == 0) return cudaSuccess;
-    if (nb == 0) return cudaMemcpyAsync(out, a, na * 8, cudaMemcpyDeviceToDevice, s);
-    if (na == 0) return cudaMemcpyAsync(out, b, nb * 8, cudaMemcpyDeviceToDevice, s);
-    const size_t tiles = (total + kMergeTile - 1) / kMergeTile;
+    const u64 tiles = (total + kTile - 1) / kTile;
     cudaError_t st = splits.ensure((tiles + 1) * 8, s);
     if (st != cudaSuccess) return st;
-    spk::merge_partition_kernel<<<simple_grid(tiles + 1), 256, 0, s>>>(a, na, b, nb, kMergeTile, splits.as<u64>());
-    st = cudaGetLastError();
+    {
+        const u64 warps = tiles + 1;
+        const u64 blocks = std::min<u64>((warps + 7) / 8, static_cast<u64>(spk::device_sm_count()) * 8);
+        spk::merge_split_kernel<<<static_cast<unsigned>(std::max<u64>(blocks, 1)), 256, 0, s>>>(
+            a, na, b, nb, kTile, tiles, splits.as<u64>());
+        st = cudaGetLastError();
+        if (st != cudaSuccess) return st;
+    }
+    // The shared-memory opt-in is per device.
+    static std::atomic<u64> configured{0};
+    int device = 0;
+    st = cudaGetDevice(&device);
     if (st != cudaSuccess) return st;
-    auto kernel = spk::merge_disjoint_kernel<kThreads, kMergeItems>;
-    kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, tiles), kThreads, 0, s>>>(
-        a, na, b, nb, splits.as<u64>(), out, md);
-    if (launches) *launches = 2;
+    const u64 bit = 1ull << (device & 63);
+    if (!(configured.load() & bit)) {
+        st = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(Layout::kBytes));
+        if (st != cudaSuccess) return st;
+        configured.fetch_or(bit);
+    }
+    const u64 grid0 = spk::persistent_grid(reinterpret_cast<const void*>(kernel), kThreads, Layout::kBytes, tiles);
+    const u64 chunk = (tiles + grid0 - 1) / grid0;
+    const u64 grid = (tiles + chunk - 1) / chunk;
+    kernel<<<static_cast<unsigned>(grid), kThreads, Layout::kBytes, s>>>(a, na, b, nb, splits.as<u64>(), chunk, out,
+                                                                         md, err);
     return cudaGetLastError();
 }
 
+cudaError_t launch_merge(const u64* a, u64 na, const u64* b, u64 nb, u64* out, DevArray& splits, cudaStream_t s,
+                         u32 items, u32* err, u64* launches = nullptr,
+                         spk::MergeDirectory md = spk::MergeDirectory{nullptr, 0, 0}) {
+    if (launches) *launches = 0;
+    if (na + nb == 0) return cudaSuccess;
+    if (nb == 0) return cudaMemcpyAsync(out, a, na * 8, cudaMemcpyDeviceToDevice, s);
+    if (na == 0) return cudaMemcpyAsync(out, b, nb * 8, cudaMemcpyDeviceToDevice, s);
+    if (launches) *launches = 2;
+    if (items == 7) return launch_merge_items<7>(a, na, b, nb, out, splits, s, err, md);
+    if (items == 15) return launch_merge_items<15>(a, na, b, nb, out, splits, s, err, md);
+    return launch_merge_items<11>(a, na, b, nb, out, splits, s, err, md);
+}
+
+// A store's merges: its split buffer, merge shape and fault word.
+cudaError_t store_merge(sparkalog_store* st, const u64* a, u64 na, const u64* b, u64 nb, u64* out,
+                        u64* launches = nullptr, spk::MergeDirectory md = spk::MergeDirectory{nullptr, 0, 0}) {
+    return launch_merge(a, na, b, nb, out, st->merge_splits, st->stream, st->merge_items, st->fault.as<u32>(),
+                        launches, md);
+}
+
+// Reads (and clears) the store's merge fault bits; non-zero bits fail.
+int check_store_fault(sparkalog_store* st) {
+    cudaStream_t s = st->stream;
+    SPK_CUDA(cudaMemcpyAsync(st->pinned + 2, st->fault.ptr, 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+    SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    const u32 bits = st->pinned[2];
+    if (bits) {
+        SPK_CUDA(cudaMemsetAsync(st->fault.ptr, 0, 4, s), "cudaMemsetAsync");
+        return fail(SPARKALOG_E_DEVICE_FAULT, "device error bits " + std::to_string(bits) + " (merge)");
+    }
+    return 0;
+}
+
 // Collapses all levels of a relation into level[0] (a single sorted run).
-int materialize(RelState& r, DevArray& splits, cudaStream_t s) {
+int materialize(sparkalog_store* st, RelState& r) {
+    cudaStream_t s = st->stream;
     for (int l = 1; l < spk::kMaxLevels; ++l) {
         if (r.level_n[l] == 0) continue;
         const u64 total = r.level_n[0] + r.level_n[l];
         SPK_CUDA(r.spare.ensure(total * 8, s), "cudaMallocAsync");
-        SPK_CUDA(launch_merge(r.level[0].as<u64>(), r.level_n[0], r.level[l].as<u64>(), r.level_n[l],
-                              r.spare.as<u64>(), splits, s),
-                 "merge_disjoint_kernel");
+        SPK_CUDA(store_merge(st, r.level[0].as<u64>(), r.level_n[0], r.level[l].as<u64>(), r.level_n[l],
+                             r.spare.as<u64>()),
+                 "merge_bulk_kernel");
         swap_arrays(r.level[0], r.spare);
         r.level_n[0] = total;
         r.level_n[l] = 0;
@@ -451,9 +503,9 @@ int merge_into_level(sparkalog_store* st, RelState& r, int l, const u64* a, u64 
     directory_shape(st, n, &shift, &buckets);
     SPK_CUDA(r.dir[l].ensure((buckets + 1) * 4, s), "cudaMallocAsync");
     u64 launched = 0;
-    SPK_CUDA(launch_merge(a, na, b, nb, r.spare.as<u64>(), st->merge_splits, s, &launched,
-                          spk::MergeDirectory{r.dir[l].as<u32>(), shift, buckets}),
-             "merge_disjoint_kernel");
+    SPK_CUDA(store_merge(st, a, na, b, nb, r.spare.as<u64>(), &launched,
+                         spk::MergeDirectory{r.dir[l].as<u32>(), shift, buckets}),
+             "merge_bulk_kernel");
     swap_arrays(r.level[l], r.spare);
     r.level_n[l] = n;
     r.dir_valid[l] = launched > 0;  // a plain copy (one side empty) wrote no directory
@@ -883,7 +935,7 @@ int build_index_impl(sparkalog_executor* ex, sparkalog_store* st, IndexCache& ic
     RelState* r = st->find(relation);
     if (!r) return fail(SPARKALOG_E_MISSING, "relation " + std::to_string(relation) + " is not registered");
     if (r->recursive) {
-        int rc = materialize(*r, st->merge_splits, s);
+        int rc = materialize(st, *r);
         if (rc) return rc;
     }
     const u64 n = r->level_n[0];
@@ -1139,8 +1191,8 @@ int sparkalog_catalog_intern_u32(sparkalog_catalog* c, const u32* values, size_t
             if (rc) return rc;
             SPK_CUDA(c->keys_spare.ensure((c->size + m) * 8, s), "cudaMallocAsync");
             SPK_CUDA(launch_merge(c->keys.as<u64>(), c->size, sorted_pairs->as<u64>(), m, c->keys_spare.as<u64>(),
-                                  c->splits, s),
-                     "merge_disjoint_kernel");
+                                  c->splits, s, 11, err),
+                     "merge_bulk_kernel");
             swap_arrays(c->keys, c->keys_spare);
             c->size += m;
         }
@@ -1204,6 +1256,8 @@ int sparkalog_store_create(void* stream, sparkalog_store** out) {
         }
     }
     cudaError_t e = st->flags.ensure(256, st->stream);
+    if (e == cudaSuccess) e = st->fault.ensure(256, st->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(st->fault.ptr, 0, 256, st->stream);
     if (e == cudaSuccess) e = pinned_get(reinterpret_cast<void**>(&st->pinned), 256);
     if (e != cudaSuccess) {
         delete st;
@@ -1228,6 +1282,7 @@ void sparkalog_store_destroy(sparkalog_store* st) {
     st->scratch_u32[0].release(s);
     st->scratch_u32[1].release(s);
     st->flags.release(s);
+    st->fault.release(s);
     st->merge_splits.release(s);
     release_store_ops(st);
     cudaStreamSynchronize(s);
@@ -1622,7 +1677,7 @@ int sparkalog_store_read(sparkalog_store* st, u32 id, int version, u32* first, u
     u64 n;
     if (version == SPARKALOG_FULL) {
         if (r->recursive) {
-            int rc = materialize(*r, st->merge_splits, s);
+            int rc = materialize(st, *r);
             if (rc) return rc;
         }
         src = r->level[0].as<u64>();
@@ -1646,7 +1701,7 @@ int sparkalog_store_read(sparkalog_store* st, u32 id, int version, u32* first, u
     SPK_CUDA(cudaGetLastError(), "unpack_rows_kernel");
     if (location == SPARKALOG_HOST) SPK_CUDA(columns_to_host(first, second, d0, d1, n, s), "cudaMemcpyAsync");
     SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
-    return 0;
+    return check_store_fault(st);
 }
 
 int sparkalog_store_anti_join(sparkalog_store* st, u32 left_id, u32 right_id, u32 out_id) {
@@ -1658,7 +1713,7 @@ int sparkalog_store_anti_join(sparkalog_store* st, u32 left_id, u32 right_id, u3
     if (st->find(out_id))
         return fail(SPARKALOG_E_DUPLICATE, "relation " + std::to_string(out_id) + " is already registered");
     cudaStream_t s = st->stream;
-    int rc = materialize(*left, st->merge_splits, s);
+    int rc = materialize(st, *left);
     if (rc) return rc;
     if (!right->sorted && right->level_n[0] > 1)
         return fail(SPARKALOG_E_UNSORTED_FULL, "FULL of relation " + std::to_string(right_id) + " is not sorted");
@@ -1692,7 +1747,7 @@ int sparkalog_store_append(sparkalog_store* st, u32 id, const u32* first, const 
     if (rows == 0) return 0;
     cudaStream_t s = st->stream;
     if (!r->sorted || r->has_dups) {
-        int rc = materialize(*r, st->merge_splits, s);
+        int rc = materialize(st, *r);
         if (rc) return rc;
         if (!r->sorted) return fail(SPARKALOG_E_UNSORTED_FULL, "FULL of relation " + std::to_string(id) + " is not sorted");
     }
@@ -1714,9 +1769,8 @@ int sparkalog_store_append(sparkalog_store* st, u32 id, const u32* first, const 
         const int l = r->recursive ? static_cast<int>(st->levels) - 1 : 0;
         const u64 tn = r->level_n[l] + fresh_n;
         SPK_CUDA(r->spare.ensure(tn * 8, s), "cudaMallocAsync");
-        SPK_CUDA(launch_merge(r->level[l].as<u64>(), r->level_n[l], fresh.as<u64>(), fresh_n, r->spare.as<u64>(),
-                              st->merge_splits, s),
-                 "merge_disjoint_kernel");
+        SPK_CUDA(store_merge(st, r->level[l].as<u64>(), r->level_n[l], fresh.as<u64>(), fresh_n, r->spare.as<u64>()),
+                 "merge_bulk_kernel");
         swap_arrays(r->level[l], r->spare);
         r->level_n[l] = tn;
         r->dir_valid[l] = false;
@@ -1730,9 +1784,8 @@ int sparkalog_store_append(sparkalog_store* st, u32 id, const u32* first, const 
             }
             const u64 dn = r->delta_n + fresh_n;
             SPK_CUDA(r->newt.ensure(std::max<u64>(dn, 1) * 8, s), "cudaMallocAsync");
-            SPK_CUDA(launch_merge(r->delta.as<u64>(), r->delta_n, fresh.as<u64>(), fresh_n, r->newt.as<u64>(),
-                                  st->merge_splits, s),
-                     "merge_disjoint_kernel");
+            SPK_CUDA(store_merge(st, r->delta.as<u64>(), r->delta_n, fresh.as<u64>(), fresh_n, r->newt.as<u64>()),
+                     "merge_bulk_kernel");
             swap_arrays(r->delta, r->newt);
             r->delta_n = dn;
         }
@@ -1794,8 +1847,7 @@ int extract_segment(sparkalog_store* st, u32 id, u32 shift, u32 segment, u32* fi
         const u64 len = bounds[2 * k + 1] - bounds[2 * k];
         if (len == 0) continue;
         const u64* slice = r->level[map[k]].as<u64>() + bounds[2 * k];
-        SPK_CUDA(launch_merge(ops.a.as<u64>(), have, slice, len, ops.b.as<u64>(), st->merge_splits, s),
-                 "merge_disjoint_kernel");
+        SPK_CUDA(store_merge(st, ops.a.as<u64>(), have, slice, len, ops.b.as<u64>()), "merge_bulk_kernel");
         swap_arrays(ops.a, ops.b);
         have += len;
     }
@@ -2103,6 +2155,7 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
     // directories): a different one invalidates them, and they are rebuilt
     // on first use.
     st->levels = ex->tuning.levels;
+    st->merge_items = ex->tuning.merge_items;
     if (st->dir_rows_log2 != ex->tuning.dir_rows_log2) {
         st->dir_rows_log2 = ex->tuning.dir_rows_log2;
         for (auto& kv : st->relations)
@@ -2125,7 +2178,7 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
         for (u32 id : ex->relations) {
             RelState& r = *st->find(id);
             if (r.sorted && !r.has_dups) continue;  // levels are already sorted, disjoint runs
-            int rc = materialize(r, st->merge_splits, s);
+            int rc = materialize(st, r);
             if (rc) return rc;
             if (!r.sorted)
                 return fail(SPARKALOG_E_UNSORTED_FULL,
@@ -2626,6 +2679,10 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
     if (*member_err_host)
         return fail(SPARKALOG_E_DEVICE_FAULT, "device error bits " + std::to_string(*member_err_host) +
                                                   " (hash set of FULL)");
+    {
+        const int rc = check_store_fault(st);
+        if (rc) return rc;
+    }
     if (summary) {
         summary->iterations = iterations;
         summary->total_new_rows = total_new;

@@ -21,6 +21,7 @@ enum : u32 {
     kErrCapacity = 1u << 1,          // an output did not fit its buffer
     kErrIndexRange = 1u << 2,        // a key outside the dense index range
     kErrMemberProbe = 1u << 3,       // a hash-set probe walked every group (the set was full)
+    kErrBarrierTimeout = 1u << 4,    // a bulk-copy barrier wait hit its cap
 };
 
 __device__ __forceinline__ u32 lanemask_lt() {
@@ -47,6 +48,86 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 __device__ __forceinline__ u32 warp_id() { return threadIdx.x / kWarp; }
+
+// ---------------------------------------------------------------------------
+// Bulk (TMA, one-dimensional) copies between global and shared memory
+// (cp.async.bulk, sm_90+), completed on a shared-memory mbarrier for loads
+// and tracked by bulk groups for stores. One thread issues a whole
+// contiguous range, so staging a tile costs one instruction instead of one
+// per row. Addresses and sizes must be multiples of 16 bytes. No multicast
+// form is used anywhere: every copy reads this GPU's own memory.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ u32 smem_addr(const void* p) { return static_cast<u32>(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, u32 count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+// Makes initialised barriers visible to the asynchronous (bulk copy) proxy.
+__device__ __forceinline__ void mbar_fence_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Arrives once and announces `bytes` of bulk-copy transactions for the
+// current phase.
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, u32 bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, u32 parity) {
+    u32 done;
+    asm volatile(
+        "{\n"
+        ".reg .pred p;\n"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        "selp.u32 %0, 1, 0, p;\n"
+        "}\n"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+// Spin cap of one mbarrier wait. A bulk copy of a tile from HBM completes in
+// microseconds; a wait this long means something is broken, and the caller
+// records an error bit instead of waiting forever.
+constexpr u32 kBarrierSpinCap = 1u << 24;
+
+// Waits for the barrier's phase `parity` to complete, at most
+// kBarrierSpinCap polls; returns false when the cap was hit.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, u32 parity) {
+    for (u32 spins = 0; spins < kBarrierSpinCap; ++spins) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (spins > 64) __nanosleep(32);
+    }
+    return false;
+}
+
+// Global -> shared bulk copy of `bytes` completing on `bar`.
+__device__ __forceinline__ void bulk_load(void* smem_dst, const void* gmem_src, u32 bytes, unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(smem_dst)),
+        "l"(gmem_src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// Orders this thread's earlier shared-memory writes before later bulk-copy
+// reads of them (generic proxy -> async proxy).
+__device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Shared -> global bulk copy, tracked by the issuing thread's bulk groups.
+__device__ __forceinline__ void bulk_store(void* gmem_dst, const void* smem_src, u32 bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gmem_dst), "r"(smem_addr(smem_src)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// Waits until the issuing thread's bulk stores have finished reading shared memory.
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// Waits until the issuing thread's bulk stores are complete.
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
 __device__ __forceinline__ u64 ld_volatile(const u64* p) {
     u64 v;

@@ -548,20 +548,6 @@ static __global__ void key_directory_kernel(const u32* keys, u64 n, u32 shift, u
     }
 }
 
-// Diagonal splits for merge_disjoint_kernel: splits[t] = number of `a` rows
-// among the first t * tile merged rows, for t in [0, tiles]; one thread per
-// diagonal.
-static __global__ void merge_partition_kernel(const u64* a, u64 na, const u64* b, u64 nb, u32 tile, u64* splits) {
-    const u64 total = na + nb;
-    const u64 tiles = (total + tile - 1) / tile;
-    const PackedKeys ka{a}, kb{b};
-    const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
-    for (u64 t = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; t <= tiles; t += stride) {
-        const u64 d = t * tile < total ? t * tile : total;
-        splits[t] = merge_path(ka, na, kb, nb, d);
-    }
-}
-
 // Directory of a merge's output, written by the merge itself (see Levels):
 // dir[b] = first output row whose key >> shift >= b, for b in [0, buckets].
 struct MergeDirectory {
@@ -570,50 +556,154 @@ struct MergeDirectory {
     u64 buckets;
 };
 
-// Merge of two sorted, mutually disjoint runs (levels are disjoint by
-// construction: NEWT excludes FULL). Output position = merge diagonal, so no
-// compaction or look-back is needed: a tile's two input slices arrive in
-// shared memory by asynchronous copies, each thread merges ITEMS rows from
-// its diagonal, and the tile leaves with coalesced stores. With a directory,
-// every output row that starts a bucket (or a run of empty buckets) writes
-// the directory entries up to its bucket, so the merged level needs no
-// separate directory pass.
-// Shared-memory rows of a merge tile are padded by one slot every 8 rows: a
-// thread's merge walk starts ITEMS = 8 rows after its neighbour's, which
-// without padding puts the 32 lanes of a warp on 2 of the 32 banks.
-struct PaddedKeys {
-    const u64* keys;
-    u32 base;
-    __device__ __forceinline__ static u32 slot(u32 i) { return i + (i >> 3); }
-    __device__ __forceinline__ u64 operator()(u64 i) const { return keys[slot(base + static_cast<u32>(i))]; }
+// Diagonal splits for merge_bulk_kernel: splits[t] = number of `a` rows among
+// the first min(t * tile, na + nb) merged rows (ties put a's row first), for
+// t in [0, tiles]. One warp per diagonal: each step its 32 lanes test 32
+// evenly spaced candidates at once, so a split over n rows costs about
+// log32(n) dependent loads instead of log2(n).
+__device__ __forceinline__ void merge_splits(const u64* a, u64 na, const u64* b, u64 nb, u32 tile, u64 tiles,
+                                             u64* splits) {
+    const u32 lane = lane_id();
+    const u64 warps = static_cast<u64>(gridDim.x) * (blockDim.x / kWarp);
+    const u64 total = na + nb;
+    for (u64 t = static_cast<u64>(blockIdx.x) * (blockDim.x / kWarp) + warp_id(); t <= tiles; t += warps) {
+        const u64 d = t * tile < total ? t * tile : total;
+        // The split is the smallest i in [lo, hi] with a[i] > b[d - 1 - i];
+        // "b[d - 1 - i] >= a[i]" holds exactly for the i below it.
+        u64 lo = d > nb ? d - nb : 0;
+        u64 hi = d < na ? d : na;
+        while (hi - lo > kWarp) {
+            const u64 step = (hi - lo + kWarp - 1) / kWarp;
+            const u64 pos = lo + (static_cast<u64>(lane) + 1) * step - 1;
+            const bool below = pos < hi && b[d - 1 - pos] >= a[pos];
+            const u32 c = __popc(__ballot_sync(0xffffffffu, below));
+            const u64 nlo = lo + c * step;
+            const u64 nhi = lo + (static_cast<u64>(c) + 1) * step;
+            lo = nlo < hi ? nlo : hi;
+            hi = nhi < hi ? nhi : hi;
+        }
+        const u64 pos = lo + lane;
+        const bool below = pos < hi && b[d - 1 - pos] >= a[pos];
+        const u64 split = lo + __popc(__ballot_sync(0xffffffffu, below));
+        if (lane == 0) splits[t] = split;
+    }
+}
+
+static __global__ void merge_split_kernel(const u64* a, u64 na, const u64* b, u64 nb, u32 tile, u64 tiles,
+                                          u64* splits) {
+    merge_splits(a, na, b, nb, tile, tiles, splits);
+}
+
+// Shared-memory layout of merge_bulk_kernel: two input stages (a's slice,
+// then b's slice at the next 16-byte boundary, each with up to one leading
+// row of alignment slack), the output tile, per-stage slice bounds and the
+// stages' barriers.
+template <int THREADS, int ITEMS>
+struct MergeBulkLayout {
+    static constexpr int kTile = THREADS * ITEMS;
+    static constexpr int kInRows = kTile + 4;
+    static constexpr size_t kIn = static_cast<size_t>(kInRows) * sizeof(u64);
+    static constexpr size_t kOut = 2 * kIn;
+    static constexpr size_t kMeta = kOut + static_cast<size_t>(kTile) * sizeof(u64);
+    static constexpr size_t kBars = kMeta + 2 * 8 * sizeof(u64);
+    static constexpr size_t kBytes = kBars + 2 * sizeof(unsigned long long);
 };
 
+// Merge of two sorted, mutually disjoint runs (FULL's levels are disjoint by
+// construction: NEWT excludes FULL) into `out`, with the output's directory
+// written on the way.
+//
+// Each CTA takes a contiguous chunk of output tiles (THREADS * ITEMS rows
+// each). A tile's two input slices, bounded by the diagonal splits, arrive
+// in shared memory by two bulk copies that one thread issues, completed on
+// the stage's mbarrier; the next tile's copies are in flight while the
+// current tile is merged (two stages). Each thread finds its diagonal by a
+// merge-path search in shared memory and merges ITEMS rows; ITEMS is odd, so
+// the lanes' walks (ITEMS rows apart) fall on different banks without
+// padding. The merged tile leaves by one bulk store. Every output row that
+// starts a directory bucket (or a run of empty ones) writes the entries up
+// to its bucket. Waits are capped: on expiry the kernel sets
+// kErrBarrierTimeout, waits once more for its copies, and returns.
 template <int THREADS, int ITEMS>
-__global__ void __launch_bounds__(THREADS) merge_disjoint_kernel(const u64* a, u64 na, const u64* b, u64 nb,
-                                                                 const u64* splits, u64* out, MergeDirectory md) {
-    constexpr int kTile = THREADS * ITEMS;
-    __shared__ __align__(16) u64 sm[kTile + kTile / 8];
-    __shared__ u64 before_tile;  // the output row just before the tile
+__device__ __forceinline__ void merge_bulk(const u64* a, u64 na, const u64* b, u64 nb, const u64* splits, u64 chunk,
+                                           u64* out, const MergeDirectory& md, u32* err) {
+    static_assert(ITEMS % 2 == 1, "odd rows per thread keep the merge walks on distinct banks");
+    using L = MergeBulkLayout<THREADS, ITEMS>;
+    constexpr int kTile = L::kTile;
+    extern __shared__ __align__(16) unsigned char smem[];
+    auto in_s = [&](int st) { return reinterpret_cast<u64*>(smem + st * L::kIn); };
+    u64* out_s = reinterpret_cast<u64*>(smem + L::kOut);
+    u64* meta = reinterpret_cast<u64*>(smem + L::kMeta);  // per stage: i0, i1, j0, j1, a_lead, a_rows, b_lead
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem + L::kBars);
+    __shared__ u64 before_tile;
+    __shared__ int failed;
+
     const u64 total = na + nb;
     const u64 num_tiles = (total + kTile - 1) / kTile;
-    for (u64 tile = blockIdx.x; tile < num_tiles; tile += gridDim.x) {
-        const u64 d0 = tile * kTile;
+    // Bulk stores need a 16-byte aligned destination (tiles are an even
+    // number of rows); otherwise the tile leaves by plain stores.
+    const bool out16 = (reinterpret_cast<uintptr_t>(out) & 15) == 0;
+    const u64 t_begin = static_cast<u64>(blockIdx.x) * chunk;
+    const u64 t_end = t_begin + chunk < num_tiles ? t_begin + chunk : num_tiles;
+    if (t_begin >= t_end) return;
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_fence_init();
+        failed = 0;
+    }
+    __syncthreads();
+
+    // Thread 0: the bulk copies of tile t into stage `st`.
+    auto issue = [&](u64 t, int st) {
+        const u64 i0 = splits[t], i1 = splits[t + 1];
+        const u64 d0 = t * kTile;
         const u64 d1 = d0 + kTile < total ? d0 + kTile : total;
-        const u64 i0 = splits[tile], i1 = splits[tile + 1];
         const u64 j0 = d0 - i0, j1 = d1 - i1;
-        const u32 sa_n = static_cast<u32>(i1 - i0), sb_n = static_cast<u32>(j1 - j0);
-        for (u32 t = threadIdx.x; t < sa_n; t += THREADS) cp_async_8(sm + PaddedKeys::slot(t), a + i0 + t);
-        for (u32 t = threadIdx.x; t < sb_n; t += THREADS) cp_async_8(sm + PaddedKeys::slot(sa_n + t), b + j0 + t);
-        cp_async_commit();
+        // A slice starts on the 16-byte boundary at or before its first row
+        // (one leading row when that row is not aligned; inputs may be
+        // slices of a larger array) and ends on the next 16-byte boundary,
+        // which stays inside the allocation because allocations are
+        // 16-byte multiples.
+        const u64 a_lead = (reinterpret_cast<uintptr_t>(a + i0) >> 3) & 1;
+        const u64 b_lead = (reinterpret_cast<uintptr_t>(b + j0) >> 3) & 1;
+        const u32 a_rows = i1 > i0 ? static_cast<u32>((a_lead + i1 - i0 + 1) & ~1ull) : 0u;
+        const u32 b_rows = j1 > j0 ? static_cast<u32>((b_lead + j1 - j0 + 1) & ~1ull) : 0u;
+        u64* m = meta + st * 8;
+        m[0] = i0; m[1] = i1; m[2] = j0; m[3] = j1; m[4] = a_lead; m[5] = a_rows; m[6] = b_lead;
+        mbar_arrive_expect_tx(&bars[st], (a_rows + b_rows) * 8u);
+        if (a_rows) bulk_load(in_s(st), a + (i0 - a_lead), a_rows * 8u, &bars[st]);
+        if (b_rows) bulk_load(in_s(st) + a_rows, b + (j0 - b_lead), b_rows * 8u, &bars[st]);
+    };
+
+    if (threadIdx.x == 0) issue(t_begin, 0);
+    u32 parity = 0;   // bit st: the phase parity stage st waits for next
+    u32 pending = 1;  // bit st: stage st's copies were issued and not yet waited for
+    for (u64 t = t_begin, k = 0; t < t_end; ++t, ++k) {
+        const int st = static_cast<int>(k & 1);
+        if (t + 1 < t_end) {
+            if (threadIdx.x == 0) issue(t + 1, st ^ 1);
+            pending |= 1u << (st ^ 1);
+        }
+        if (mbar_wait(&bars[st], (parity >> st) & 1u)) {
+            pending &= ~(1u << st);
+            parity ^= 1u << st;
+        } else {
+            atomicOr(err, kErrBarrierTimeout);
+            failed = 1;
+        }
+        const u64 d0 = t * kTile;
+        const u64 d1 = d0 + kTile < total ? d0 + kTile : total;
+        const u32 len = static_cast<u32>(d1 - d0);
+        const u64* m = meta + st * 8;
+        const u64 i0 = m[0], j0 = m[2];
+        const u32 sa_n = static_cast<u32>(m[1] - i0), sb_n = static_cast<u32>(m[3] - j0);
+        const SmemKeys sa{in_s(st) + m[4]}, sb{in_s(st) + m[5] + m[6]};
         if (md.dir && threadIdx.x == 0 && d0 > 0) {
             const u64 pa = i0 > 0 ? a[i0 - 1] : 0, pb = j0 > 0 ? b[j0 - 1] : 0;
             before_tile = i0 == 0 ? pb : (j0 == 0 ? pa : (pa > pb ? pa : pb));
         }
-        cp_async_wait<0>();
-        __syncthreads();
-        const PaddedKeys sa{sm, 0}, sb{sm, sa_n};
         const u32 diag = threadIdx.x * ITEMS;
-        const u32 len = static_cast<u32>(d1 - d0);
         u64 v[ITEMS];
         if (diag < len) {
             u32 ia = static_cast<u32>(merge_path(sa, sa_n, sb, sb_n, diag));
@@ -626,25 +716,53 @@ __global__ void __launch_bounds__(THREADS) merge_disjoint_kernel(const u64* a, u
                 }
             }
         }
+        // The previous tile's bulk store must have read out_s before it is
+        // overwritten.
+        if (threadIdx.x == 0) bulk_wait_read();
         __syncthreads();
 #pragma unroll
         for (int i = 0; i < ITEMS; ++i)
-            if (diag + i < len) sm[PaddedKeys::slot(diag + i)] = v[i];
+            if (diag + i < len) out_s[diag + i] = v[i];
+        fence_async_shared();
         __syncthreads();
-        for (u32 j = threadIdx.x; j < len; j += THREADS) out[d0 + j] = sm[PaddedKeys::slot(j)];
+        if (out16) {
+            const u32 even = len & ~1u;
+            if (threadIdx.x == 0 && even) {
+                bulk_store(out + d0, out_s, even * 8u);
+                bulk_commit();
+            }
+            if (threadIdx.x == 1 && (len & 1u)) out[d0 + even] = out_s[even];
+        } else {
+            for (u32 j = threadIdx.x; j < len; j += THREADS) out[d0 + j] = out_s[j];
+        }
         if (md.dir) {
             for (u32 j = threadIdx.x; j < len; j += THREADS) {
                 const u64 o = d0 + j;
-                const u64 bucket = sm[PaddedKeys::slot(j)] >> md.shift;
+                const u64 bucket = out_s[j] >> md.shift;
                 u64 from = 0;
-                if (o > 0) from = ((j > 0 ? sm[PaddedKeys::slot(j - 1)] : before_tile) >> md.shift) + 1;
+                if (o > 0) from = ((j > 0 ? out_s[j - 1] : before_tile) >> md.shift) + 1;
                 for (u64 e = from; e <= bucket && e <= md.buckets; ++e) md.dir[e] = static_cast<u32>(o);
                 if (o == total - 1)
                     for (u64 e = bucket + 1; e <= md.buckets; ++e) md.dir[e] = static_cast<u32>(total);
             }
         }
         __syncthreads();
+        if (failed) break;
     }
+    if (threadIdx.x == 0) {
+        // After a timeout, copies may still be in flight into shared memory:
+        // wait once more (capped) for every issued stage before the CTA exits.
+        for (int st = 0; st < 2; ++st)
+            if ((pending >> st) & 1u) mbar_wait(&bars[st], (parity >> st) & 1u);
+        bulk_wait_all();
+    }
+}
+
+template <int THREADS, int ITEMS>
+__global__ void __launch_bounds__(THREADS) merge_bulk_kernel(const u64* a, u64 na, const u64* b, u64 nb,
+                                                             const u64* splits, u64 chunk, u64* out,
+                                                             MergeDirectory md, u32* err) {
+    merge_bulk<THREADS, ITEMS>(a, na, b, nb, splits, chunk, out, md, err);
 }
 
 // Packs SoA columns (c0, c1) into u64 rows and flags whether the rows are
