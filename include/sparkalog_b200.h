@@ -340,6 +340,22 @@ SPARKALOG_API int sparkalog_executor_set_fused(sparkalog_executor* executor, int
  * reference. */
 SPARKALOG_API int sparkalog_executor_set_member_set(sparkalog_executor* executor, int enable);
 
+/* Enables (default) or disables device-driven rounds: while a single
+ * transitive-closure-shaped target's rounds stay within the group-searched
+ * anti-join's candidate bound, the executor runs them as a CUDA graph whose
+ * WHILE node repeats one round (fused join + order, anti-join, merge into
+ * TAIL, and a round-end kernel that applies the round and tests convergence
+ * on the device), with one host synchronisation per launch instead of one
+ * per round. Results, iteration counts and the round trace are identical
+ * either way. Profiling (sparkalog_executor_set_profiling) runs every round
+ * from the host. The reference runs every round from the host
+ * (generic.rs:472-516). */
+SPARKALOG_API int sparkalog_executor_set_device_loop(sparkalog_executor* executor, int enable);
+/* Graph launches of the device-driven loop and the rounds they applied, over
+ * the executor's lifetime. */
+SPARKALOG_API int sparkalog_executor_device_loop_stats(sparkalog_executor* executor, uint64_t* launches,
+                                                       uint64_t* rounds);
+
 /* Launch shapes and thresholds of the executor's kernels, chosen per device
  * by the autotuner (sparkalog_b200/autotune.py) on a short calibration
  * fixpoint. Every value gives identical results; only speed changes. The

@@ -65,6 +65,8 @@ TIER_B = [
     "sparkalog_executor_set_profiling",
     "sparkalog_executor_set_fused",
     "sparkalog_executor_set_member_set",
+    "sparkalog_executor_set_device_loop",
+    "sparkalog_executor_device_loop_stats",
     "sparkalog_tuning_defaults",
     "sparkalog_executor_set_tuning",
     "sparkalog_executor_get_tuning",
@@ -261,6 +263,10 @@ def load() -> ctypes.CDLL:
     L.sparkalog_executor_set_fused.restype = i
     L.sparkalog_executor_set_member_set.argtypes = [vp, i]
     L.sparkalog_executor_set_member_set.restype = i
+    L.sparkalog_executor_set_device_loop.argtypes = [vp, i]
+    L.sparkalog_executor_set_device_loop.restype = i
+    L.sparkalog_executor_device_loop_stats.argtypes = [vp, c_u64p, c_u64p]
+    L.sparkalog_executor_device_loop_stats.restype = i
     L.sparkalog_tuning_defaults.argtypes = [ctypes.POINTER(TuningC)]
     L.sparkalog_tuning_defaults.restype = i
     L.sparkalog_executor_set_tuning.argtypes = [vp, ctypes.POINTER(TuningC)]

@@ -29,6 +29,7 @@
 #include "spk_fused.cuh"
 #include "spk_member.cuh"
 #include "spk_ingest.cuh"
+#include "spk_loop.cuh"
 #include "spk_setops.cuh"
 
 #include <algorithm>
@@ -644,6 +645,9 @@ struct sparkalog_executor {
     };
     bool profiling = false;
     bool fused_enabled = true;
+    bool device_loop = true;       // tail rounds as a CUDA graph WHILE loop (see spk_loop.cuh)
+    u64 loop_launches = 0;         // graph launches of the device loop
+    u64 loop_rounds = 0;           // rounds applied by the device loop
     sparkalog_tuning tuning = default_tuning();
     // `counters` holds, in this order: the per-round tile counters
     // (kCounterWords u32), the per-target counts (counts_words u64), the error
@@ -1050,6 +1054,351 @@ int cascade_levels(sparkalog_executor* ex, sparkalog_store* st, RelState& tr) {
         tr.level_n[l] = 0;
         tr.dir_valid[l] = false;
     }
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Device-driven tail rounds (spk_loop.cuh): a CUDA graph whose WHILE node runs
+// one round per iteration until the round-end kernel stops it. The graph and
+// the small buffers it names (descriptor, counters, look-back words, trace)
+// are cached per (device, stream, shape), so executors created one after the
+// other (a fresh executor per fixpoint) reuse one instantiated graph.
+// ---------------------------------------------------------------------------
+constexpr u64 kLoopTraceCap = 4096;     // rounds one graph launch may apply
+constexpr int kLoopWordBytes = 256;     // counts[4] u64 | tile counters u32[16] | error bits u32[16]
+constexpr u32 kLoopMinFusedRows = 64;
+
+struct LoopGraph {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    u64 bound = 0;
+    u32 lanes = 0, items = 0;
+    bool segments = false;
+    std::mutex use;
+    spk::LoopDesc* desc = nullptr;        // device
+    spk::LoopDesc* host_desc = nullptr;   // pinned
+    u64* words = nullptr;                 // device
+    u64* fused_status = nullptr;
+    u64* anti_status = nullptr;
+    size_t fused_status_words = 0, anti_status_words = 0;
+    spk::LoopTrace* trace = nullptr;      // device, kLoopTraceCap records
+    spk::LoopTrace* host_trace = nullptr; // pinned
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+std::mutex g_loop_mu;
+std::vector<LoopGraph*> g_loops;  // kept for the life of the process
+
+struct LoopGrids {
+    unsigned fused, anti, merge, split, segment;
+};
+
+// Shared-memory opt-ins and persistent grid sizes of the loop's kernels
+// (queried before the capture starts).
+template <int G, int ITEMS>
+cudaError_t prepare_loop_kernels(const LoopGraph& g, LoopGrids* grids) {
+    using FL = spk::FusedLayout<kFusedThreads, kFusedCap, kFusedRowCap>;
+    using ML = spk::MergeBulkLayout<kThreads, ITEMS>;
+    auto fused = spk::loop_fused_kernel<kFusedThreads, kFusedCap, kFusedRowCap>;
+    auto anti = spk::loop_anti_join_kernel<kWideThreads, G>;
+    auto merge = spk::loop_merge_kernel<kThreads, ITEMS>;
+    cudaError_t e = cudaFuncSetAttribute(fused, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(FL::kBytes));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(merge, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(ML::kBytes));
+    if (e != cudaSuccess) return e;
+    const u64 fused_tiles = (g.bound + kLoopMinFusedRows - 1) / kLoopMinFusedRows;
+    const u64 anti_tiles = (g.bound + (kWideThreads / G) - 1) / (kWideThreads / G);
+    grids->fused = spk::persistent_grid(reinterpret_cast<const void*>(fused), kFusedThreads, FL::kBytes, fused_tiles);
+    grids->anti = spk::persistent_grid(reinterpret_cast<const void*>(anti), kWideThreads, 0, anti_tiles);
+    grids->merge = spk::persistent_grid(reinterpret_cast<const void*>(merge), kThreads, ML::kBytes, ~0ull >> 1);
+    grids->split = static_cast<unsigned>(spk::device_sm_count()) * 4;
+    grids->segment = simple_grid(g.bound);
+    return cudaGetLastError();
+}
+
+template <int G, int ITEMS>
+cudaError_t capture_loop_body(LoopGraph& g, cudaStream_t s, cudaGraphConditionalHandle handle, const LoopGrids& gr) {
+    using FL = spk::FusedLayout<kFusedThreads, kFusedCap, kFusedRowCap>;
+    using ML = spk::MergeBulkLayout<kThreads, ITEMS>;
+    cudaError_t e = cudaMemsetAsync(g.words, 0, kLoopWordBytes, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(g.fused_status, 0, g.fused_status_words * 8, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(g.anti_status, 0, g.anti_status_words * 8, s);
+    if (e != cudaSuccess) return e;
+    spk::loop_fused_kernel<kFusedThreads, kFusedCap, kFusedRowCap><<<gr.fused, kFusedThreads, FL::kBytes, s>>>(g.desc);
+    spk::loop_anti_join_kernel<kWideThreads, G><<<gr.anti, kWideThreads, 0, s>>>(g.desc);
+    spk::loop_split_kernel<<<gr.split, 256, 0, s>>>(g.desc, static_cast<u32>(kThreads * ITEMS));
+    spk::loop_merge_kernel<kThreads, ITEMS><<<gr.merge, kThreads, ML::kBytes, s>>>(g.desc);
+    spk::loop_round_end_kernel<<<1, 32, 0, s>>>(g.desc, handle);
+    if (g.segments) spk::loop_segment_kernel<<<gr.segment, 256, 0, s>>>(g.desc);
+    return cudaGetLastError();
+}
+
+// The graph: a WHILE node (condition 1 at every launch) whose body is one
+// round captured from stream `s`.
+template <int G, int ITEMS>
+cudaError_t build_loop_graph_shape(LoopGraph& g, cudaStream_t s) {
+    LoopGrids grids{};
+    cudaError_t e = prepare_loop_kernels<G, ITEMS>(g, &grids);
+    if (e != cudaSuccess) return e;
+    e = cudaGraphCreate(&g.graph, 0);
+    if (e != cudaSuccess) return e;
+    cudaGraphConditionalHandle handle;
+    e = cudaGraphConditionalHandleCreate(&handle, g.graph, 1, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) return e;
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = handle;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    e = cudaGraphAddNode(&node, g.graph, nullptr, 0, &cp);
+    if (e != cudaSuccess) return e;
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    const cudaError_t ce = capture_loop_body<G, ITEMS>(g, s, handle, grids);
+    cudaGraph_t captured = nullptr;
+    e = cudaStreamEndCapture(s, &captured);
+    if (ce != cudaSuccess) return ce;
+    if (e != cudaSuccess) return e;
+    return cudaGraphInstantiate(&g.exec, g.graph, 0);
+}
+
+template <int G>
+cudaError_t build_loop_graph_lanes(LoopGraph& g, cudaStream_t s) {
+    if (g.items == 7) return build_loop_graph_shape<G, 7>(g, s);
+    if (g.items == 15) return build_loop_graph_shape<G, 15>(g, s);
+    return build_loop_graph_shape<G, 11>(g, s);
+}
+
+// Captured on a private stream: the legacy default stream, which callers may
+// use, cannot be captured, and the graph launches on any stream.
+cudaError_t build_loop_graph(LoopGraph& g) {
+    cudaStream_t s = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return e;
+    if (g.lanes == 4) e = build_loop_graph_lanes<4>(g, s);
+    else if (g.lanes == 16) e = build_loop_graph_lanes<16>(g, s);
+    else e = build_loop_graph_lanes<8>(g, s);
+    cudaStreamDestroy(s);
+    return e;
+}
+
+// The cached graph for this shape (built on first use).
+cudaError_t loop_graph(cudaStream_t s, u64 bound, u32 lanes, u32 items, bool segments, LoopGraph** out) {
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(g_loop_mu);
+    for (LoopGraph* g : g_loops) {
+        if (g->device == device && g->stream == s && g->bound == bound && g->lanes == lanes && g->items == items &&
+            g->segments == segments) {
+            *out = g;
+            return cudaSuccess;
+        }
+    }
+    auto* g = new LoopGraph();
+    g->device = device;
+    g->stream = s;
+    g->bound = bound;
+    g->lanes = lanes;
+    g->items = items;
+    g->segments = segments;
+    g->fused_status_words = (bound + kLoopMinFusedRows - 1) / kLoopMinFusedRows + 2;
+    g->anti_status_words = (bound + (kWideThreads / lanes) - 1) / (kWideThreads / lanes) + 2;
+    e = cudaMalloc(reinterpret_cast<void**>(&g->desc), sizeof(spk::LoopDesc));
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&g->words), kLoopWordBytes);
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&g->fused_status), g->fused_status_words * 8);
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&g->anti_status), g->anti_status_words * 8);
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&g->trace), kLoopTraceCap * sizeof(spk::LoopTrace));
+    if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&g->host_desc), sizeof(spk::LoopDesc));
+    if (e == cudaSuccess)
+        e = cudaMallocHost(reinterpret_cast<void**>(&g->host_trace), kLoopTraceCap * sizeof(spk::LoopTrace));
+    if (e == cudaSuccess) e = build_loop_graph(*g);
+    // A half-built entry is dropped (not freed: freeing device memory here
+    // would synchronise the device) and never reused.
+    if (e != cudaSuccess) return e;
+    g_loops.push_back(g);
+    *out = g;
+    return cudaSuccess;
+}
+
+// Runs device-driven rounds of a single-rule, fused-eligible target while
+// its rounds stay small; returns the rounds applied through *applied and
+// their new rows through *new_rows. On return the host state (levels,
+// DELTA, trace) matches what the same rounds run by the host would leave.
+int run_device_loop(sparkalog_executor* ex, sparkalog_store* st, size_t ti, u64 max_rounds, u64* applied,
+                    u64* new_rows) {
+    cudaStream_t s = st->stream;
+    *applied = 0;
+    *new_rows = 0;
+    TargetRT& t = ex->targets[ti];
+    const size_t k = t.rules[0];
+    const sparkalog_rule_plan& p = ex->rules[k];
+    RelState& tr = *st->find(t.id);
+    RelState& right = *st->find(p.right_input);
+    IndexCache& ic = ex->index[k];
+    const int tail = static_cast<int>(ex->tuning.levels) - 1;
+    const u64 bound = ex->tuning.group_candidates;
+    const u64 max_degree = std::max<u64>(ic.max_degree, 1);
+    const u64 ratio = ex->tuning.level_ratio;
+    const u64 upper_n = tr.level_n[tail - 1];
+    const u64 tail_max = upper_n / ratio + bound + 1;
+
+    // Capacities for every round the loop may run (it stops before a round
+    // that could exceed them).
+    if (t.j_cap < bound) {
+        const u64 cap = bound + bound / 4;
+        SPK_CUDA(t.j_a.ensure(cap * 8, s), "cudaMallocAsync");
+        SPK_CUDA(t.j_b.ensure(cap * 8, s), "cudaMallocAsync");
+        t.j_cap = cap;
+    }
+    SPK_CUDA(tr.delta.ensure(bound * 8, s, tr.delta_n * 8), "cudaMallocAsync");
+    SPK_CUDA(tr.newt.ensure(bound * 8, s), "cudaMallocAsync");
+    SPK_CUDA(tr.level[tail].ensure(tail_max * 8, s, tr.level_n[tail] * 8), "cudaMallocAsync");
+    SPK_CUDA(tr.spare.ensure(tail_max * 8, s), "cudaMallocAsync");
+    SPK_CUDA(st->merge_splits.ensure((tail_max / (kThreads * 7) + 4) * 8, s), "cudaMallocAsync");
+    // TAIL's directory in the loop's fixed shape (sized for its largest TAIL).
+    u32 shift;
+    u64 buckets;
+    directory_shape(st, tail_max, &shift, &buckets);
+    if (!tr.dir_valid[tail] || tr.dir_shift[tail] != shift || tr.dir_buckets[tail] != buckets) {
+        SPK_CUDA(tr.dir[tail].ensure((buckets + 1) * 4, s), "cudaMallocAsync");
+        if (tr.level_n[tail]) {
+            spk::level_directory_kernel<<<simple_grid(buckets + 1), 256, 0, s>>>(
+                tr.level[tail].as<u64>(), tr.level_n[tail], shift, buckets, tr.dir[tail].as<u32>());
+            SPK_CUDA(cudaGetLastError(), "level_directory_kernel");
+            ex->stats.total_launches += 1;
+        }
+        tr.dir_shift[tail] = shift;
+        tr.dir_buckets[tail] = buckets;
+        tr.dir_valid[tail] = true;
+    }
+    int rc = refresh_directories(st, tr, s, nullptr);
+    if (rc) return rc;
+
+    LoopGraph* g = nullptr;
+    SPK_CUDA(loop_graph(s, bound, ex->tuning.group_lanes, st->merge_items, ex->seg_count != 0, &g),
+             "device loop graph");
+    std::lock_guard<std::mutex> use(g->use);
+    spk::LoopDesc& d = *g->host_desc;
+    d = spk::LoopDesc{};
+    u64* counts = g->words;
+    u32* counters = reinterpret_cast<u32*>(g->words + 4);
+    u32* err = reinterpret_cast<u32*>(g->words + 12);
+    spk::FusedRoundArgs& a = d.fused;
+    a.delta = tr.delta.as<u64>();
+    a.delta_rows = 0;
+    a.delta_rows_ptr = &g->desc->delta_n;
+    a.rows_per_tile = std::max(t.fused_rows, kLoopMinFusedRows);
+    a.left_key = p.left_key;
+    if (ic.bucketed) {
+        a.bucket_dir = ic.bucket_dir.as<u32>();
+        a.bucket_shift = ic.bucket_shift;
+        a.buckets = ic.buckets;
+        a.keys32 = ic.keys32.as<u32>();
+    } else {
+        a.dense_offsets = ic.offsets.as<u32>();
+        a.dense_keys = ic.num_keys;
+    }
+    a.rows = ic.identity ? nullptr : ic.rows.as<u32>();
+    a.right = right.level[0].as<u64>();
+    a.v1_side = p.proj_side[1];
+    a.v1_col = p.proj_col[1];
+    a.v1_bits = static_cast<u32>(32 - __builtin_clz(st->max_value | 1));
+    a.out = t.j_a.as<u64>();
+    a.out_count = counts + 1;
+    a.join_rows = reinterpret_cast<unsigned long long*>(counts);
+    a.status = g->fused_status;
+    a.tile_counter = counters;
+    a.epoch = 1;
+    a.err = err;
+    a.fallback = err + 8;
+    d.lv.n = tail + 1;
+    u64 other = 0;
+    for (int l = 0; l <= tail; ++l) {
+        d.lv.keys[l] = tr.level[l].as<u64>();
+        d.lv.count[l] = tr.level_n[l];
+        d.lv.dir[l] = tr.dir[l].as<u32>();
+        d.lv.shift[l] = tr.dir_shift[l];
+        // An empty level is never searched (every key falls past its buckets).
+        d.lv.buckets[l] = tr.level_n[l] ? tr.dir_buckets[l] : 0;
+        if (l != tail) other += tr.level_n[l];
+    }
+    for (int l = tail + 1; l < spk::kMaxLevels; ++l) other += tr.level_n[l];
+    d.tail_slot = static_cast<u32>(tail);
+    d.counts = counts;
+    d.counters = counters;
+    d.anti_status = g->anti_status;
+    d.err = err;
+    d.delta = tr.delta.as<u64>();
+    d.newt = tr.newt.as<u64>();
+    d.delta_n = tr.delta_n;
+    d.tail = tr.level[tail].as<u64>();
+    d.spare = tr.spare.as<u64>();
+    d.tail_n = tr.level_n[tail];
+    d.splits = st->merge_splits.as<u64>();
+    d.md = spk::MergeDirectory{tr.dir[tail].as<u32>(), shift, buckets};
+    d.bound = bound;
+    d.max_degree = max_degree;
+    d.upper_n = upper_n;
+    d.ratio = ratio;
+    d.other_rows = other;
+    d.limit = std::min<u64>(max_rounds, kLoopTraceCap);
+    d.rounds_total = ex->rounds_total;
+    d.seg_shift = ex->seg_shift;
+    d.seg_count = ex->seg_count;
+    d.seg_seen = ex->seg_seen.as<u32>();
+    d.seg_new = ex->seg_new.as<unsigned long long>();
+    d.trace = g->trace;
+    SPK_CUDA(cudaMemcpyAsync(g->desc, &d, sizeof(d), cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
+    SPK_CUDA(cudaGraphLaunch(g->exec, s), "cudaGraphLaunch");
+    SPK_CUDA(cudaMemcpyAsync(&d, g->desc, sizeof(d), cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+    SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    const u64 done = d.iterations;
+    if (done) {
+        SPK_CUDA(cudaMemcpyAsync(g->host_trace, g->trace, done * sizeof(spk::LoopTrace), cudaMemcpyDeviceToHost, s),
+                 "cudaMemcpyAsync");
+        SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    }
+    ex->loop_launches += 1;
+    ex->loop_rounds += done;
+    // The host state after the applied rounds.
+    if (d.tail != tr.level[tail].as<u64>()) swap_arrays(tr.level[tail], tr.spare);
+    tr.level_n[tail] = d.tail_n;
+    if (d.delta != tr.delta.as<u64>()) swap_arrays(tr.delta, tr.newt);
+    tr.delta_n = d.delta_n;
+    tr.delta_sorted = true;
+    tr.version += done;
+    if (done) tr.member_valid = false;
+    // A refused round's merge wrote the directory of rows that were not
+    // applied: rebuild it from TAIL when next needed.
+    if (d.stop == spk::kLoopRedo || d.stop == spk::kLoopFault || d.stop == spk::kLoopRowLimit)
+        tr.dir_valid[tail] = false;
+    for (u64 r = 0; r < done; ++r) {
+        const spk::LoopTrace& lt = g->host_trace[r];
+        sparkalog_round_trace rec{};
+        rec.round = ex->rounds_total + r + 1;
+        rec.delta_rows = lt.delta_rows;
+        rec.join_rows = lt.join_rows;
+        rec.unique_rows = lt.unique_rows;
+        rec.new_rows = lt.new_rows;
+        rec.full_rows = lt.full_rows;
+        if (ex->trace.size() < kMaxTraceRounds) ex->trace.push_back(rec);
+    }
+    ex->rounds_total += done;
+    ex->stats.rounds += done;
+    ex->stats.total_launches += done * (ex->seg_count ? 6 : 5);
+    *applied = done;
+    *new_rows = d.total_new;
+    if (d.stop == spk::kLoopFault) {
+        u32* bits = reinterpret_cast<u32*>(ex->host_counts + ex->counts_words) + 31;
+        SPK_CUDA(cudaMemcpyAsync(bits, err, 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+        SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+        return fail(SPARKALOG_E_DEVICE_FAULT, "device error bits " + std::to_string(*bits) + " (device loop)");
+    }
+    if (d.stop == spk::kLoopCascade) return cascade_levels(ex, st, tr);
     return 0;
 }
 
@@ -2100,6 +2449,19 @@ int sparkalog_executor_set_member_set(sparkalog_executor* ex, int enable) {
     return 0;
 }
 
+int sparkalog_executor_set_device_loop(sparkalog_executor* ex, int enable) {
+    if (!ex) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null executor");
+    ex->device_loop = enable != 0;
+    return 0;
+}
+
+int sparkalog_executor_device_loop_stats(sparkalog_executor* ex, uint64_t* launches, uint64_t* rounds) {
+    if (!ex || !launches || !rounds) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null argument");
+    *launches = ex->loop_launches;
+    *rounds = ex->loop_rounds;
+    return 0;
+}
+
 int sparkalog_tuning_defaults(sparkalog_tuning* out) {
     if (!out) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null output");
     *out = default_tuning();
@@ -2267,6 +2629,27 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                 ic.column != p.right_key) {
                 int rc = build_index(ex, st, ic, p.right_input, p.right_key);
                 if (rc) return rc;
+            }
+        }
+
+        // Small rounds of a single transitive-closure-shaped target run on the
+        // device, many per host round trip (spk_loop.cuh).
+        if (ex->device_loop && !ex->profiling && !ex->member_enabled && ex->targets.size() == 1 &&
+            ex->tuning.levels >= 2 && fused_eligible(ex, st, 0)) {
+            const TargetRT& t = ex->targets[0];
+            const sparkalog_rule_plan& p = ex->rules[t.rules[0]];
+            RelState& tr = *st->find(t.id);
+            const u64 dn = st->find(p.delta_input)->delta_n;
+            const u64 bound = dn * static_cast<u64>(std::max<u32>(ex->index[t.rules[0]].max_degree, 1));
+            const int tail = static_cast<int>(ex->tuning.levels) - 1;
+            if (p.delta_input == t.id && dn > 0 && bound <= ex->tuning.group_candidates &&
+                tr.level_n[tail - 1] > 0 && tr.level_n[tail] * ex->tuning.level_ratio <= tr.level_n[tail - 1]) {
+                u64 applied = 0, added = 0;
+                int rc = run_device_loop(ex, st, 0, max_iterations - iterations, &applied, &added);
+                if (rc) return rc;
+                iterations += applied;
+                total_new += added;
+                if (applied) continue;
             }
         }
 

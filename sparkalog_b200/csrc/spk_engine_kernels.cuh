@@ -337,11 +337,10 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_sparse_kernel(const 
 // log_{G+1}(S) steps instead of log_2(S) dependent loads. A tile is
 // THREADS / G candidates, one per group.
 template <int THREADS, int G>
-__global__ void __launch_bounds__(THREADS) anti_join_levels_wide_kernel(const u64* buf_a, const u64* buf_b,
-                                                                        const u32* final_sel, const u64* n_ptr,
-                                                                        Levels levels, u64* out, u64* out_count,
-                                                                        u64* status, u32* tile_counter, u32 epoch,
-                                                                        u32* err, unsigned long long* unique_count) {
+__device__ __forceinline__ void anti_join_group(const u64* buf_a, const u64* buf_b, const u32* final_sel,
+                                                const u64* n_ptr, const Levels& levels, u64* out, u64* out_count,
+                                                u64* status, u32* tile_counter, u32 epoch, u32* err,
+                                                unsigned long long* unique_count) {
     static_assert(G >= 2 && G <= 32 && 32 % G == 0 && THREADS % 32 == 0, "groups tile the warp");
     constexpr int kTile = THREADS / G;
     // Each step shrinks a window of S > G rows to at most S / (G + 1) + 1;
@@ -427,12 +426,22 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_wide_kernel(const u6
     }
 }
 
+template <int THREADS, int G>
+__global__ void __launch_bounds__(THREADS) anti_join_levels_wide_kernel(const u64* buf_a, const u64* buf_b,
+                                                                        const u32* final_sel, const u64* n_ptr,
+                                                                        Levels levels, u64* out, u64* out_count,
+                                                                        u64* status, u32* tile_counter, u32 epoch,
+                                                                        u32* err, unsigned long long* unique_count) {
+    anti_join_group<THREADS, G>(buf_a, buf_b, final_sel, n_ptr, levels, out, out_count, status, tile_counter, epoch,
+                                err, unique_count);
+}
+
 // Per-segment activity of one round's NEWT rows (sorted, so a segment's rows
 // are contiguous): seen[seg] = max(seen[seg], round1), new_rows[seg] += rows.
 // Lanes holding the same segment are grouped with match.any and one lane per
 // group updates the counters.
-static __global__ void segment_activity_kernel(const u64* rows, u64 n, u32 shift, u32 count, u32 round1,
-                                               u32* seen, unsigned long long* new_rows) {
+__device__ __forceinline__ void segment_activity(const u64* rows, u64 n, u32 shift, u32 count, u32 round1,
+                                                 u32* seen, unsigned long long* new_rows) {
     const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
     const u64 rounds = (n + stride - 1) / stride;
     for (u64 r = 0; r < rounds; ++r) {
@@ -448,6 +457,11 @@ static __global__ void segment_activity_kernel(const u64* rows, u64 n, u32 shift
             atomicAdd(&new_rows[seg], static_cast<unsigned long long>(__popc(peers)));
         }
     }
+}
+
+static __global__ void segment_activity_kernel(const u64* rows, u64 n, u32 shift, u32 count, u32 round1,
+                                               u32* seen, unsigned long long* new_rows) {
+    segment_activity(rows, n, shift, count, round1, seen, new_rows);
 }
 
 // Row range of one key interval [lo_key, hi_key) in every level: out[2l] and

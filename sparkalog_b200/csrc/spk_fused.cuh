@@ -31,6 +31,7 @@ namespace spk {
 struct FusedRoundArgs {
     const u64* delta;
     u64 delta_rows;
+    const u64* delta_rows_ptr;  // when set, the DELTA row count is read here (device-driven rounds)
     u32 rows_per_tile;        // nominal DELTA rows per tile (x boundaries move it)
     u32 left_key;             // DELTA column joined on the right relation's key
     // Index of the right relation on the join key (DELTA's second column).
@@ -188,7 +189,7 @@ constexpr int kCountBits = 52;
 constexpr u64 kCountMask = (1ull << kCountBits) - 1;
 
 template <int THREADS, int CAP, int ROWCAP>
-__global__ void __launch_bounds__(THREADS, 1024 / THREADS) fused_join_distinct_kernel(FusedRoundArgs a) {
+__device__ __forceinline__ void fused_round(const FusedRoundArgs& a) {
     using L = FusedLayout<THREADS, CAP, ROWCAP>;
     constexpr int kRowItems = ROWCAP / THREADS;
     static_assert(ROWCAP % THREADS == 0, "rows split evenly over threads");
@@ -209,7 +210,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) fused_join_distinct_k
     __shared__ u64 bounds[2];
     __shared__ u64 tile_shared, out_base;
 
-    const u64 n = a.delta_rows;
+    const u64 n = a.delta_rows_ptr ? *a.delta_rows_ptr : a.delta_rows;
     const u64 R = a.rows_per_tile;
     const u64 num_tiles = (n + R - 1) / R;
     if (num_tiles == 0) {
@@ -397,6 +398,11 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) fused_join_distinct_k
         if (tile == num_tiles - 1 && threadIdx.x == 0) *a.out_count = base + total;
         __syncthreads();
     }
+}
+
+template <int THREADS, int CAP, int ROWCAP>
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS) fused_join_distinct_kernel(FusedRoundArgs a) {
+    fused_round<THREADS, CAP, ROWCAP>(a);
 }
 
 }  // namespace spk

@@ -382,6 +382,16 @@ class RecursiveExecutor:
         """Enables or disables (default) FULL's hash set for the anti-join; results are identical."""
         _check(_native.load().sparkalog_executor_set_member_set(self._h, 1 if enable else 0))
 
+    def set_device_loop(self, enable: bool) -> None:
+        """Enables (default) or disables device-driven tail rounds; results are identical."""
+        _check(_native.load().sparkalog_executor_set_device_loop(self._h, 1 if enable else 0))
+
+    def device_loop_stats(self) -> tuple[int, int]:
+        """(graph launches, rounds applied) of the device-driven loop over the executor's lifetime."""
+        a, b = ctypes.c_uint64(0), ctypes.c_uint64(0)
+        _check(_native.load().sparkalog_executor_device_loop_stats(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return int(a.value), int(b.value)
+
     def tuning(self) -> dict:
         """The executor's launch shapes and thresholds (sparkalog_tuning)."""
         t = _native.TuningC()

@@ -395,3 +395,81 @@ def test_round_trace_cardinalities(cuda, fused):
     assert got == expect
     assert [r["round"] for r in ex.trace(reset=True)] == list(range(1, len(expect) + 1))
     assert ex.trace() == []
+
+
+def _run_tc(src, dst, tuning=None, device_loop=True, steps=None):
+    R = rec()
+    e0, e1 = oracle.btree_pairs(src, dst)
+    store = R.RelationStore()
+    store.insert_static(0, (e0, e1))
+    store.insert_recursive(1, (e0, e1), (e0, e1))
+    ex = R.RecursiveExecutor.compile(R.transitive_closure_scc(_rid(1), _rid(0)), store)
+    if tuning:
+        ex.set_tuning(tuning)
+    ex.set_device_loop(device_loop)
+    if steps is None:
+        summary = ex.run(store)
+        iterations, new = summary.iterations, summary.total_new_rows
+    else:
+        iterations = new = 0
+        while True:
+            summary, done = ex.step(store, steps)
+            iterations += summary.iterations
+            new += summary.total_new_rows
+            if done:
+                break
+    trace = ex.trace()
+    loop = ex.device_loop_stats()
+    full = store.full(1)
+    ex.close()
+    store.close()
+    return full, iterations, new, trace, loop
+
+
+TUNINGS = [
+    {},
+    {"merge_items": 7, "levels": 4, "dir_rows_log2": 2, "group_lanes": 4},
+    {"merge_items": 15, "levels": 2, "dir_rows_log2": 0, "group_lanes": 16, "group_candidates": 1 << 21},
+    {"level_ratio": 2, "sparse_candidates": 1 << 22, "group_candidates": 1 << 12, "fused_rows_cap": 128},
+]
+
+
+@pytest.mark.parametrize("tuning", TUNINGS)
+def test_every_tuning_gives_the_oracle_fixpoint(cuda, tuning):
+    # Launch shapes, directory granularity, level count and thresholds change
+    # speed only: FULL, iteration count and the per-round trace are the same.
+    src, dst = generators.er_edges(300_000, 262_500, 6)
+    (w0, w1), it, new = oracle.transitive_closure(src, dst, threads=8)
+    full, iterations, derived, trace, _ = _run_tc(src, dst, tuning)
+    base = _run_tc(src, dst, None, device_loop=False)
+    assert iterations == it and derived == new
+    assert np.array_equal(full[0], w0) and np.array_equal(full[1], w1)
+    assert [(r["delta_rows"], r["unique_rows"], r["new_rows"], r["full_rows"]) for r in trace] == \
+        [(r["delta_rows"], r["unique_rows"], r["new_rows"], r["full_rows"]) for r in base[3]]
+
+
+@pytest.mark.parametrize("n,e,seed", [(300_000, 262_500, 6), (1_000_000, 875_000, 8), (5000, 4500, 2)])
+def test_device_loop_matches_host_loop(cuda, n, e, seed):
+    # The tail rounds run as a CUDA graph WHILE loop with a device-side
+    # convergence test; FULL, iterations and every round's cardinalities equal
+    # the host-driven loop's, and the loop really ran.
+    src, dst = generators.er_edges(n, e, seed)
+    on = _run_tc(src, dst, None, device_loop=True)
+    off = _run_tc(src, dst, None, device_loop=False)
+    assert on[1] == off[1] and on[2] == off[2]
+    assert np.array_equal(on[0][0], off[0][0]) and np.array_equal(on[0][1], off[0][1])
+    assert on[3] == off[3]
+    assert off[4] == (0, 0)
+    if n >= 300_000:
+        launches, rounds = on[4]
+        assert launches >= 1 and rounds >= 10
+
+
+def test_device_loop_respects_step_limits(cuda):
+    # executor_step with a few rounds at a time: the device loop stops at each
+    # step's limit and resumes, with the same result.
+    src, dst = generators.er_edges(300_000, 262_500, 6)
+    (w0, w1), it, new = oracle.transitive_closure(src, dst, threads=8)
+    full, iterations, derived, _, loop = _run_tc(src, dst, None, device_loop=True, steps=3)
+    assert iterations == it and derived == new
+    assert np.array_equal(full[0], w0) and np.array_equal(full[1], w1)
