@@ -13,7 +13,9 @@ Metric: derived TC tuples per second, i.e. the executor's total_new_rows
   device-resident edges + compile + run to the fixpoint; K steps timed with
   CUDA events, barrier + synchronize on both sides, max over ranks.
 * ``e2e``: the same through the public API from pinned host buffers: every
-  step uploads the edges (static EDB and seed), runs, and reads FULL back.
+  step copies the edges to the device once (they are both the static EDB and
+  the seed), runs, and reads FULL back; the last step's FULL is then compared
+  with the oracle's (its committed digest at full size): ``bit_exact_vs_oracle``.
 * ``roofline``: the dominant kernel class of one profiled step (CUDA events
   on the executor's stream around every kernel class, algorithmic bytes =
   each input row read once and each output row written once).
@@ -25,7 +27,8 @@ Multi-GPU (torchrun): ranks split the nodes into contiguous x ranges; each
 rank closes the paths starting in its range against the replicated EDB. The
 join output keeps x, so every operator stays partition-local and no data
 crosses ranks; a final all-reduce combines iteration counts (max) and new
-rows (sum). ``--impl reference`` times the CPU oracle alone (rank 0).
+rows (sum). ``--impl reference`` times the CPU oracle alone (rank 0) over the
+whole fixpoint, once, with the same ``config`` object as this arm.
 """
 
 from __future__ import annotations
@@ -50,8 +53,12 @@ WORKLOADS = {
     "er_16m_14_68m": (16_777_216, 14_680_064, 2),
     "er_2000_8000": (2_000, 8_000, 1),
 }
-# Rounds of the fixpoint run by one CPU-baseline sample.
+# Rounds of the fixpoint run by one CPU-baseline sample of the GPU arm's line
+# (the reference arm times the whole fixpoint).
 CPU_SAMPLE_ROUNDS = {"er_16m_14_68m": 4, "er_2000_8000": 13}
+# Oracle digests of the full-size outputs (tests/golden/full_size.py).
+DIGEST_KEYS = {"er_16m_14_68m": "er_16m"}
+L2_NOTE = "inputs larger than L2 (FULL ~1 GB, candidates ~100 MB per round)"
 
 
 # DRAM traffic measured by ncu for one fixpoint of a smaller graph of the same
@@ -249,30 +256,45 @@ def general_cpu_baseline(cols, delta_rows_total, new_rows, time_cap_s=10.0):
                       f"binding per test), so a lower bound on its time"}
 
 
+def workload_config(workload, nodes, edges, seed, derived, iterations):
+    """The config object both arms print (identical keys and values for one workload)."""
+    return {"workload": workload, "nodes": nodes, "edges": edges, "seed": seed, "derived_tuples": int(derived),
+            "iterations": int(iterations), "l2": L2_NOTE}
+
+
 def run_reference(args):
+    """The reference's CPU implementation of the path (the oracle's restatement
+    of its *_cpu_parallel operators inside RecursiveExecutor::run, all host
+    threads) over the WHOLE fixpoint of the same workload. One full fixpoint
+    takes minutes on the CPU, so it is timed once whatever --steps and
+    --warmup ask for (the line says so); rank 0 alone runs it."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    import oracle
     from sparkalog_b200 import generators
 
     nodes, edges, seed = WORKLOADS[args.workload]
-    cols = generators.er_edges(nodes, edges, seed)
-    samples = []
-    base = None
-    for i in range(args.warmup + args.steps):
-        b = cpu_baseline(args.workload, cols)
-        if i >= args.warmup:
-            samples.append(b["value"])
-            base = b
-    value = statistics.median(samples)
-    nodes, edges, _ = WORKLOADS[args.workload]
+    src, dst = generators.er_edges(nodes, edges, seed)
+    cores = os.cpu_count() or 1
+    st = oracle.Store()
+    st.insert_static(0, (src, dst))
+    st.insert_recursive(1, (src, dst), (src, dst))
+    t0 = time.perf_counter()
+    iterations, new = st.run_scc([1], [oracle.tc_rule(1, 0)], threads=cores)
+    dt = time.perf_counter() - t0
+    value = new / dt
     line = {
         "impl": "reference", "metric": "TC derived tuples/s", "value": value, "unit": "tuples/s",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-        "scaling": "strong", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded ER)",
-        "config": {"workload": args.workload, "nodes": nodes, "edges": edges},
-        "cpu_baseline": {"value": value, "unit": "tuples/s", "cores": base["cores"], "kind": base["kind"],
-                         "sample": base["sample"]},
+        "n_gpus": args.gpus, "steps": 1, "warmup": 0, "ms_per_step": dt * 1e3, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded ER, splitmix64)",
+        "config": workload_config(args.workload, nodes, edges, seed, new, iterations),
+        "requested": {"steps": args.steps, "warmup": args.warmup,
+                      "note": "one whole fixpoint is timed once: it takes minutes on the CPU"},
+        "cpu_baseline": {"value": value, "unit": "tuples/s", "cores": cores, "kind": "port",
+                         "sample": f"the whole {iterations}-round fixpoint once ({new} derived tuples in "
+                                   f"{dt:.1f} s); restatement of the reference's *_cpu_parallel operators "
+                                   f"inside RecursiveExecutor::run"},
         "e2e": {"value": value, "unit": "tuples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -314,11 +336,14 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
+    tuning = {}
+
     def step(profile=False):
         store = RelationStore(stream)
         store.insert_static(0, (e0, e1))
         store.insert_recursive(1, (s0, s1), (s0, s1))
         ex = RecursiveExecutor.compile(plan, store)
+        tuning.update(ex.tuning())
         if profile:
             ex.set_profiling(True)
         summary = ex.run(store)
@@ -374,14 +399,22 @@ def run_ours(args):
     achieved = per_launch_bytes / (per_launch_ms / 1e3) / 1e9 if per_launch_ms > 0 else 0.0
     traffic, traffic_source = profiled_traffic(dominant, float(new_rows) / max(world, 1))
     pipe = float(pipeline_bytes(pstats["trace"]))
+    own_bytes = float(sum(v["bytes"] for v in classes.values()))
+    own_gbs = own_bytes / (ms / args.steps / 1e3) / 1e9
     if dist is not None:
         t = torch.tensor([pipe], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
         pipe = float(t[0])
 
-    # End to end through the public API: pinned host buffers, H2D + run + D2H.
-    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
-    h_src, h_dst, h_ps, h_pd = pin(src), pin(dst), pin(ps), pin(pd)
+    # End to end through the public API: the step's inputs copied once from
+    # pinned host buffers (the edges; at N > 1 also this rank's seed rows),
+    # the run, FULL read back into pinned host buffers.
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).pin_memory()
+    h_src, h_dst = pin(src), pin(dst)
+    h_ps, h_pd = (h_src, h_dst) if world == 1 else (pin(ps), pin(pd))
+    d_src, d_dst = torch.empty_like(h_src, device="cuda"), torch.empty_like(h_dst, device="cuda")
+    d_ps, d_pd = (d_src, d_dst) if world == 1 else (torch.empty_like(h_ps, device="cuda"),
+                                                    torch.empty_like(h_pd, device="cuda"))
     full_rows = None
     out0 = out1 = None
     e2e_ms = []
@@ -390,9 +423,14 @@ def run_ours(args):
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
         a.record(stream)
+        d_src.copy_(h_src, non_blocking=True)
+        d_dst.copy_(h_dst, non_blocking=True)
+        if world > 1:
+            d_ps.copy_(h_ps, non_blocking=True)
+            d_pd.copy_(h_pd, non_blocking=True)
         store = RelationStore(stream)
-        store.insert_static(0, (h_src, h_dst))
-        store.insert_recursive(1, (h_ps, h_pd), (h_ps, h_pd))
+        store.insert_static(0, (d_src, d_dst))
+        store.insert_recursive(1, (d_ps, d_pd), (d_ps, d_pd))
         ex = RecursiveExecutor.compile(plan, store)
         ex.run(store)
         n = store.rows(1, FULL)
@@ -413,8 +451,28 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_local = float(t[0])
     e2e_value = new_rows / (e2e_local / 1e3)
-    h2d = (len(h_src) + 2 * len(h_ps)) * 8
+    h2d = len(h_src) * 8 + (len(h_ps) * 8 if world > 1 else 0)
     d2h = full_rows * 8
+    # Parity of the last end-to-end step's FULL (read back above) with the
+    # oracle: its committed digest at full size, the oracle itself on small
+    # workloads. Outside every timed region.
+    exact = None
+    if world == 1:
+        f0 = out0.numpy()[:full_rows].view(np.uint32)
+        f1 = out1.numpy()[:full_rows].view(np.uint32)
+        if args.workload in DIGEST_KEYS and args.nodes is None and args.edges is None:
+            sys.path.insert(0, str(ROOT / "tests" / "golden"))
+            import full_size
+
+            if full_size.DIGESTS.exists():
+                want = json.loads(full_size.DIGESTS.read_text())[DIGEST_KEYS[args.workload]]
+                exact = bool(full_size.pair_digest(f0, f1) == want["digest"] and
+                             want["iterations"] == iterations and want["new_rows"] == new_rows)
+        elif rank == 0 and not args.no_cpu_baseline:
+            import oracle
+
+            (w0, w1), it, new = oracle.transitive_closure(src, dst, threads=os.cpu_count() or 1)
+            exact = bool(np.array_equal(f0, w0) and np.array_equal(f1, w1) and it == iterations and new == new_rows)
 
     clock = clocks.summary()
     cpu = None
@@ -436,10 +494,10 @@ def run_ours(args):
             "vs_baseline": None,
             "dtype": "u32",
             "data": "synthetic (seeded ER, splitmix64)",
-            "config": {"workload": args.workload, "nodes": nodes, "edges": edges, "seed": seed,
-                       "derived_tuples": new_rows, "iterations": iterations, "device_pool_gb": pool_gb,
-                       "parallelism": f"x-range partition x{world}" if world > 1 else "single GPU",
-                       "l2": "inputs larger than L2 (FULL ~1 GB, candidates ~100 MB per round)"},
+            "config": workload_config(args.workload, nodes, edges, seed, new_rows, iterations),
+            "setup": {"device_pool_gb": pool_gb, "tuning": tuning,
+                      "parallelism": f"x-range partition x{world}" if world > 1 else "single GPU"},
+            "bit_exact_vs_oracle": exact,
             "e2e": {"value": e2e_value, "unit": "tuples/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": e2e_local},
             "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved / 1.0, "peak": peak,
@@ -450,6 +508,11 @@ def run_ours(args):
                          "classes": {k: {"ms": v["ms"], "launches": v["launches"],
                                          "gbs": (v["bytes"] / (v["ms"] / 1e3) / 1e9) if v["ms"] > 0 else 0.0}
                                      for k, v in classes.items()}},
+            "step_roofline": {"algorithmic_bytes": own_bytes, "achieved_gbs": own_gbs, "peak": peak,
+                              "frac": own_gbs / peak,
+                              "what": "the algorithmic bytes of every kernel class of one profiled step (each "
+                                      "input row read once, each output row written once) over the measured "
+                                      "step time"},
             "pipeline": {"algorithmic_bytes": pipe,
                          "achieved_gbs": pipe / (ms / args.steps / 1e3) / 1e9,
                          "frac": pipe / (ms / args.steps / 1e3) / 1e9 / peak,

@@ -111,3 +111,12 @@ def test_bench_reference_arm_line():
         assert key in line, key
     assert line["impl"] == "reference" and line["value"] > 0
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["cpu_baseline"]["cores"] >= 1
+    # The whole fixpoint is timed, and the config equals the GPU arm's.
+    assert line["config"] == bench_config("er_2000_8000", 3_829_620, 13)
+
+
+def bench_config(workload, derived, iterations):
+    import bench
+
+    nodes, edges, seed = bench.WORKLOADS[workload]
+    return bench.workload_config(workload, nodes, edges, seed, derived, iterations)
