@@ -224,24 +224,37 @@ class RelationStore:
         _check(_native.load().sparkalog_store_append(self._h, int(getattr(rid, "value", rid)), p0, p1, n, loc))
         del keep
 
-    def extract_segment(self, rid: RelationId | int, shift: int, segment: int,
-                        untag: bool = False) -> tuple[np.ndarray, np.ndarray]:
+    def extract_segment(self, rid: RelationId | int, shift: int, segment: int, untag: bool = False,
+                        device: bool = False):
         """Sorted rows of FULL whose first column >> shift == segment; with
-        ``untag`` the segment bits of both columns are cleared on the device."""
+        ``untag`` the segment bits of both columns are cleared on the device.
+        Host numpy columns, or with ``device`` two int32 CUDA tensors (the u32
+        bits) allocated on the store's stream."""
         L = _native.load()
         rid = int(getattr(rid, "value", rid))
         n = ctypes.c_size_t(0)
+        loc = DEVICE if device else HOST
         if untag:
-            call = lambda a, b: L.sparkalog_store_extract_segment_untagged(self._h, rid, shift, segment, 1, a, b, HOST,
+            call = lambda a, b: L.sparkalog_store_extract_segment_untagged(self._h, rid, shift, segment, 1, a, b, loc,
                                                                             ctypes.byref(n))
         else:
-            call = lambda a, b: L.sparkalog_store_extract_segment(self._h, rid, shift, segment, a, b, HOST,
+            call = lambda a, b: L.sparkalog_store_extract_segment(self._h, rid, shift, segment, a, b, loc,
                                                                   ctypes.byref(n))
         _check(call(None, None))
+        if device:
+            with torch.cuda.stream(self._stream):
+                a = torch.empty(max(n.value, 1), dtype=torch.int32, device="cuda")
+                b = torch.empty(max(n.value, 1), dtype=torch.int32, device="cuda")
+            _check(call(a.data_ptr(), b.data_ptr()))
+            return a[: n.value], b[: n.value]
         a = np.empty(max(n.value, 1), dtype=np.uint32)
         b = np.empty(max(n.value, 1), dtype=np.uint32)
         _check(call(a.ctypes.data, b.ctypes.data))
         return a[: n.value], b[: n.value]
+
+    @property
+    def stream(self):
+        return self._stream
 
     def remove_segments(self, rid: RelationId | int, shift: int, segments) -> None:
         """Drops every row whose first column >> shift is in ``segments`` from FULL and DELTA."""

@@ -22,10 +22,19 @@ kernel launches. Between rounds the server
 Per request, the result (rows and iteration count) equals the request run
 alone: tags keep requests disjoint, and the executor's per-segment activity
 gives each one the number of rounds its own RecursiveExecutor::run would take.
+
+A step may run several rounds (``rounds_per_step``); the executor then runs
+the small ones as one device-driven graph launch. Results can be completed
+into device memory (``readout="device"``: each completion holds two CUDA
+tensors) or read to the host. ``LanedServer`` splits requests by size into
+lanes, each a server with its own store, executor and CUDA stream (the lane
+of small requests at a higher stream priority), stepped by its own host
+thread: a small request does not wait behind the long rounds of a large one.
 """
 
 from __future__ import annotations
 
+import threading
 import time
 from dataclasses import dataclass, field
 
@@ -75,12 +84,16 @@ class FixpointServer:
     """Continuous-batching TC server over one device-resident store."""
 
     def __init__(self, id_bits: int = 23, budget_bytes: float = 120e9, growth_prior: float = 16.0, stream=None,
-                 clock=time.perf_counter):
+                 clock=time.perf_counter, readout: str = "host", rounds_per_step: int = 1):
+        if readout not in ("host", "device"):
+            raise ValueError("readout is 'host' or 'device'")
         self.shift = id_bits
         self.slots = 1 << (32 - id_bits)
         self.budget = budget_bytes
         self.growth = growth_prior
         self.clock = clock
+        self.readout = readout
+        self.rounds_per_step = max(1, int(rounds_per_step))
         self.store = RelationStore(stream)
         empty = (np.zeros(0, dtype=np.uint32), np.zeros(0, dtype=np.uint32))
         self.store.insert_static(EDB, empty)
@@ -166,10 +179,11 @@ class FixpointServer:
     # ------------------------------------------------------------ rounds
 
     def step(self) -> list[Completion]:
-        """One round for every active request, then completes the finished ones."""
+        """Up to rounds_per_step rounds for every active request, then completes
+        the finished ones."""
         if not self.active:
             return []
-        summary, _ = self.executor.step(self.store, 1)
+        summary, _ = self.executor.step(self.store, self.rounds_per_step)
         self.rounds += summary.iterations
         seen, new_rows = self.executor.segment_stats()
         done = [slot for slot in self.active if int(seen[slot]) != self.rounds]
@@ -177,7 +191,7 @@ class FixpointServer:
         now = None
         for slot in done:
             a = self.active.pop(slot)
-            f0, f1 = self.store.extract_segment(PATH, self.shift, slot, untag=True)
+            f0, f1 = self.store.extract_segment(PATH, self.shift, slot, untag=True, device=self.readout == "device")
             iterations = int(seen[slot]) - a.admit_round + 1 if int(seen[slot]) > a.admit_round else 1
             now = self.clock()
             c = Completion(a.request.request_id, (f0, f1), iterations,
@@ -188,6 +202,10 @@ class FixpointServer:
             self.retired.append(slot)
             self.retired_bytes += 16.0 * (len(f0) + edges)
         self.completions.extend(finished)
+        # Retired rows cost every later round (FULL holds them): drop them at
+        # once when the server falls idle or they outweigh the live rows.
+        if self.retired and (not self.active or self.retired_bytes > self.resident_bytes() - self.retired_bytes):
+            self.purge()
         return finished
 
     def purge(self) -> None:
@@ -250,8 +268,112 @@ def serve(requests: list[ServeRequest], server: FixpointServer, realtime: bool =
     return report
 
 
+class LanedServer:
+    """Requests split by edge count into lanes (lane k takes requests with at
+    most bounds[k] edges, the last lane the rest), each lane a FixpointServer
+    with its own store, executor and stream, stepped by its own host thread.
+    Lane 0 (the smallest requests) runs at the highest stream priority."""
+
+    def __init__(self, bounds=(1 << 17,), budget_bytes: float = 120e9, shares=None, readout: str = "host",
+                 rounds_per_step: int = 1, clock=time.perf_counter, **kw):
+        import torch
+
+        self.bounds = list(bounds)
+        n = len(self.bounds) + 1
+        shares = shares or ([0.25 / (n - 1)] * (n - 1) + [0.75] if n > 1 else [1.0])
+        low, high = torch.cuda.Stream.priority_range()
+        self.lanes = []
+        for k in range(n):
+            stream = torch.cuda.Stream(priority=high if k == 0 else low)
+            self.lanes.append(FixpointServer(budget_bytes=budget_bytes * shares[k], stream=stream, clock=clock,
+                                             readout=readout, rounds_per_step=rounds_per_step, **kw))
+
+    def lane_for(self, request: ServeRequest) -> int:
+        e = len(request.src)
+        for k, b in enumerate(self.bounds):
+            if e <= b:
+                return k
+        return len(self.bounds)
+
+    @property
+    def completions(self) -> list[Completion]:
+        return [c for lane in self.lanes for c in lane.completions]
+
+    @property
+    def rounds(self) -> int:
+        return sum(lane.rounds for lane in self.lanes)
+
+    def close(self) -> None:
+        for lane in self.lanes:
+            lane.close()
+
+
+def serve_laned(requests: list[ServeRequest], server: LanedServer, realtime: bool = True) -> ServeReport:
+    """Replays an arrival stream against a LanedServer: the caller's thread
+    hands each request to its lane at its arrival time; every lane's thread
+    admits, steps and completes its own requests."""
+    pending = sorted(requests, key=lambda r: r.arrival_s)
+    start = time.perf_counter()
+    clock = lambda: time.perf_counter() - start
+    for lane in server.lanes:
+        lane.clock = clock
+    queues = [[] for _ in server.lanes]
+    cond = threading.Condition()
+    finished = [False]
+    errors = []
+
+    def run_lane(k: int, device: int) -> None:
+        import torch
+
+        lane = server.lanes[k]
+        try:
+            torch.cuda.set_device(device)
+            while True:
+                with cond:
+                    while not queues[k] and not lane.active and not finished[0]:
+                        cond.wait(0.05)
+                    if not queues[k] and not lane.active and finished[0]:
+                        return
+                    arrived = list(queues[k])
+                    queues[k].clear()
+                batch = []
+                while arrived and lane.can_admit(arrived[0], batch):
+                    batch.append(arrived.pop(0))
+                if arrived:
+                    with cond:
+                        queues[k][:0] = arrived
+                lane.admit(batch)
+                if lane.active:
+                    lane.step()
+        except BaseException as e:  # surfaced by the caller
+            errors.append(e)
+
+    import torch
+
+    device = torch.cuda.current_device()
+    threads = [threading.Thread(target=run_lane, args=(k, device), daemon=True) for k in range(len(server.lanes))]
+    for t in threads:
+        t.start()
+    for r in pending:
+        if realtime:
+            wait = r.arrival_s - clock()
+            if wait > 0:
+                time.sleep(wait)
+        with cond:
+            queues[server.lane_for(r)].append(r)
+            cond.notify_all()
+    with cond:
+        finished[0] = True
+        cond.notify_all()
+    for t in threads:
+        t.join()
+    if errors:
+        raise errors[0]
+    return ServeReport(server.completions, clock(), server.rounds)
+
+
 def serve_one_at_a_time(requests: list[ServeRequest], stream=None, realtime: bool = True,
-                        clock=time.perf_counter) -> ServeReport:
+                        clock=time.perf_counter, readout: str = "host") -> ServeReport:
     """The baseline: a FIFO loop that runs each request alone through the same engine."""
     pending = sorted(requests, key=lambda r: r.arrival_s)
     start = clock()
@@ -272,7 +394,17 @@ def serve_one_at_a_time(requests: list[ServeRequest], stream=None, realtime: boo
         store.append(PATH, (s, d))
         ex = RecursiveExecutor.compile(transitive_closure_scc(RelationId(PATH), RelationId(EDB)), store)
         summary = ex.run(store)
-        path = store.full(PATH)
+        if readout == "device":
+            import torch
+
+            n = store.rows(PATH)
+            with torch.cuda.stream(store.stream):
+                path = (torch.empty(max(n, 1), dtype=torch.int32, device="cuda"),
+                        torch.empty(max(n, 1), dtype=torch.int32, device="cuda"))
+            store.read_into(PATH, 0, path[0], path[1])
+            path = (path[0][:n], path[1][:n])
+        else:
+            path = store.full(PATH)
         ex.close()
         store.close()
         report.rounds += summary.iterations

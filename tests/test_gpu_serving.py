@@ -17,6 +17,12 @@ def make_requests(count, seed, e_max=20_000):
     return [ServeRequest(k, p.arrival_s, *generators.er_edges(p.nodes, p.edges, p.seed)) for k, p in enumerate(params)]
 
 
+def _host(col):
+    if hasattr(col, "is_cuda"):
+        return col.cpu().numpy().view(np.uint32)
+    return col
+
+
 def check_against_alone(report, requests):
     by_id = {c.request_id: c for c in report.completions}
     assert sorted(by_id) == [r.request_id for r in requests]
@@ -25,7 +31,7 @@ def check_against_alone(report, requests):
         c = by_id[r.request_id]
         assert c.iterations == it, r.request_id
         assert c.new_rows == new, r.request_id
-        assert np.array_equal(c.path[0], w0) and np.array_equal(c.path[1], w1), r.request_id
+        assert np.array_equal(_host(c.path[0]), w0) and np.array_equal(_host(c.path[1]), w1), r.request_id
 
 
 def test_served_results_equal_alone(cuda):
@@ -134,3 +140,33 @@ def test_large_pageable_reads_equal_pinned_reads(cuda):
     assert len(u0) * 4 >= 32 << 20
     assert np.array_equal(u0, t0 & np.uint32(0x7FFFFFFF)) and np.array_equal(u1, t1 & np.uint32(0x7FFFFFFF))
     store.close()
+
+
+@pytest.mark.parametrize("readout,rounds", [("device", 1), ("host", 4), ("device", 8)])
+def test_laned_server_results_equal_alone(cuda, readout, rounds):
+    # Size lanes on their own streams and threads, several rounds per step
+    # (the device-driven loop), results in device or host memory: every
+    # request's rows and iteration count equal its run alone.
+    from sparkalog_b200.serving import LanedServer, serve_laned, serve_one_at_a_time
+
+    reqs = make_requests(40, 13, e_max=60_000)
+    server = LanedServer(bounds=(6_000,), readout=readout, rounds_per_step=rounds)
+    report = serve_laned(reqs, server, realtime=False)
+    lanes = [len(lane.completions) for lane in server.lanes]
+    server.close()
+    check_against_alone(report, reqs)
+    assert all(n > 0 for n in lanes)
+    alone = serve_one_at_a_time(reqs, realtime=False, readout=readout)
+    check_against_alone(alone, reqs)
+
+
+def test_laned_server_realtime(cuda):
+    from sparkalog_b200.serving import LanedServer, serve_laned
+
+    reqs = make_requests(30, 21, e_max=40_000)
+    server = LanedServer(bounds=(5_000,), readout="device", rounds_per_step=4)
+    report = serve_laned(reqs, server, realtime=True)
+    server.close()
+    check_against_alone(report, reqs)
+    s = report.summary()
+    assert s["requests"] == 30 and s["p99_ms"] >= s["p50_ms"] > 0
