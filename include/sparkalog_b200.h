@@ -242,6 +242,43 @@ SPARKALOG_API int sparkalog_store_read(sparkalog_store* store, uint32_t id, int 
 SPARKALOG_API int sparkalog_store_anti_join(sparkalog_store* store, uint32_t left_id, uint32_t right_id,
                                             uint32_t out_id);
 
+/* ---- Non-recursive clauses on the device ----
+ * GeneralCpu evaluates every non-recursive clause of a stratified program
+ * with nested loops (crates/sparkalog-datalog/src/general.rs:478-551:
+ * positive atoms matched term by term, constants compared, negated atoms
+ * checked against a completed relation), and the binary lowering rejects
+ * such clauses (subset.rs:56-63). These two operations, with
+ * sparkalog_store_anti_join, evaluate the binary ones on the GPU; each
+ * stores its result as a new static relation (sorted, deduplicated: the
+ * BTreeSet GeneralCpu builds) and fails with SPARKALOG_E_DUPLICATE when
+ * out_id exists. */
+
+/* Removes relation id from the store and frees its device memory (stream-
+ * ordered). */
+SPARKALOG_API int sparkalog_store_drop(sparkalog_store* store, uint32_t id);
+
+/* out(c0, c1) :- in(x, y), where(x, y): where_mask bit 0 keeps rows with
+ * x == where_value[0], bit 1 rows with y == where_value[1], bit 2 rows with
+ * x == y (an atom with constants or a repeated variable, the equality
+ * predicate of the reference's filter, column_ops.cu:20-43); out column k
+ * is x (out_source[k] = 0), y (1) or the constant out_value[k] (2). */
+typedef struct sparkalog_select {
+    uint32_t where_mask;
+    uint32_t where_value[2];
+    uint32_t out_source[2];
+    uint32_t out_value[2];
+} sparkalog_select;
+SPARKALOG_API int sparkalog_store_select(sparkalog_store* store, uint32_t in_id, const sparkalog_select* spec,
+                                         uint32_t out_id, size_t* rows);
+
+/* out(p0, p1) :- left(..), right(..) joined on left's column left_key equal
+ * to right's column right_key; output column k is column proj_col[k] of the
+ * left (proj_side[k] = 0) or right (1) row (BinaryEqualityJoin,
+ * relational/src/lib.rs:46-50), deduplicated. */
+SPARKALOG_API int sparkalog_store_join(sparkalog_store* store, uint32_t left_id, uint32_t right_id,
+                                       uint32_t left_key, uint32_t right_key, const uint32_t* proj_side,
+                                       const uint32_t* proj_col, uint32_t out_id, size_t* rows);
+
 /* RecursiveExecutor::compile, generic.rs:407-470. */
 SPARKALOG_API int sparkalog_executor_compile(sparkalog_store* store, const uint32_t* relations,
                                              size_t relation_count, const sparkalog_rule_plan* rules,

@@ -45,6 +45,9 @@ TIER_B = [
     "sparkalog_store_rows",
     "sparkalog_store_read",
     "sparkalog_store_anti_join",
+    "sparkalog_store_drop",
+    "sparkalog_store_select",
+    "sparkalog_store_join",
     "sparkalog_store_load_binary_u32",
     "sparkalog_store_load_delimited_u32",
     "sparkalog_catalog_create",
@@ -125,6 +128,17 @@ class TuningC(ctypes.Structure):
 
     def as_dict(self) -> dict:
         return {name: int(getattr(self, name)) for name, _ in self._fields_}
+
+
+class SelectC(ctypes.Structure):
+    """sparkalog_select."""
+
+    _fields_ = [
+        ("where_mask", ctypes.c_uint32),
+        ("where_value", ctypes.c_uint32 * 2),
+        ("out_source", ctypes.c_uint32 * 2),
+        ("out_value", ctypes.c_uint32 * 2),
+    ]
 
 
 KERNEL_CLASSES = ["join", "sort_histogram", "sort_pass", "anti_join", "merge", "index", "join_distinct"]
@@ -217,6 +231,13 @@ def load() -> ctypes.CDLL:
     L.sparkalog_store_read.restype = i
     L.sparkalog_store_anti_join.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]
     L.sparkalog_store_anti_join.restype = i
+    L.sparkalog_store_drop.argtypes = [vp, ctypes.c_uint32]
+    L.sparkalog_store_drop.restype = i
+    L.sparkalog_store_select.argtypes = [vp, ctypes.c_uint32, ctypes.POINTER(SelectC), ctypes.c_uint32, c_sizep]
+    L.sparkalog_store_select.restype = i
+    L.sparkalog_store_join.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                       c_u32p, c_u32p, ctypes.c_uint32, c_sizep]
+    L.sparkalog_store_join.restype = i
     L.sparkalog_store_load_binary_u32.argtypes = [vp, ctypes.c_uint32, vp, ctypes.c_size_t, i, i, c_sizep,
                                                    ctypes.POINTER(LoadErrorC)]
     L.sparkalog_store_load_binary_u32.restype = i

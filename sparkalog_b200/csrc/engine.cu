@@ -2087,6 +2087,176 @@ int sparkalog_store_anti_join(sparkalog_store* st, u32 left_id, u32 right_id, u3
     return 0;
 }
 
+namespace {
+
+// Stores `n` packed rows of ops.a, sorted and deduplicated, as the new static
+// relation out_id.
+int store_sorted_unique(sparkalog_store* st, u64 n, u32 out_id, size_t* rows) {
+    cudaStream_t s = st->stream;
+    RelState out;
+    u64 out_n = 0;
+    if (n > 0) {
+        RelState none;
+        int rc = sorted_difference(st, n, none, out.level[0], &out_n);
+        if (rc) return rc;
+    } else {
+        SPK_CUDA(out.level[0].ensure(8, s), "cudaMallocAsync");
+    }
+    out.level_n[0] = out_n;
+    out.sorted = true;
+    out.has_dups = false;
+    st->relations[out_id] = std::move(out);
+    if (rows) *rows = out_n;
+    return 0;
+}
+
+// Reads a device count word (synchronises the stream).
+int read_count(sparkalog_store* st, StoreOps& ops, const u64* word, u64* out) {
+    cudaStream_t s = st->stream;
+    SPK_CUDA(cudaMemcpyAsync(ops.host, word, 8, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+    SPK_CUDA(cudaMemcpyAsync(reinterpret_cast<u32*>(ops.host + 1), ops.counters.as<u32>() + 32, 4,
+                             cudaMemcpyDeviceToHost, s),
+             "cudaMemcpyAsync");
+    SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    const u32 bits = static_cast<u32>(ops.host[1] & 0xffffffffu);
+    if (bits) return fail(SPARKALOG_E_DEVICE_FAULT, "device error bits " + std::to_string(bits));
+    *out = ops.host[0];
+    return 0;
+}
+
+}  // namespace
+
+int sparkalog_store_drop(sparkalog_store* st, u32 id) {
+    if (!st) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null store");
+    auto it = st->relations.find(id);
+    if (it == st->relations.end()) return fail(SPARKALOG_E_MISSING, "relation " + std::to_string(id) + " is not registered");
+    cudaStream_t s = st->stream;
+    RelState& r = it->second;
+    for (auto& l : r.level) l.release(s);
+    for (auto& d : r.dir) d.release(s);
+    for (DevArray* d : {&r.spare, &r.delta, &r.newt, &r.member, &r.member_flag}) d->release(s);
+    st->relations.erase(it);
+    return 0;
+}
+
+int sparkalog_store_select(sparkalog_store* st, u32 in_id, const sparkalog_select* spec, u32 out_id, size_t* rows) {
+    if (!st || !spec) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null argument");
+    if (spec->where_mask > 7 || spec->out_source[0] > 2 || spec->out_source[1] > 2)
+        return fail(SPARKALOG_E_INVALID_ARGUMENT, "select names a column outside a binary relation");
+    RelState* in = st->find(in_id);
+    if (!in) return fail(SPARKALOG_E_MISSING, "relation " + std::to_string(in_id) + " is not registered");
+    if (st->find(out_id))
+        return fail(SPARKALOG_E_DUPLICATE, "relation " + std::to_string(out_id) + " is already registered");
+    cudaStream_t s = st->stream;
+    int rc = materialize(st, *in);
+    if (rc) return rc;
+    const u64 n = in->level_n[0];
+    StoreOps* ops_ptr = store_ops(st);
+    if (!ops_ptr) return static_cast<int>(cudaErrorMemoryAllocation);
+    StoreOps& ops = *ops_ptr;
+    u64 m = 0;
+    if (n > 0) {
+        SPK_CUDA(ops.a.ensure(n * 8, s), "cudaMallocAsync");
+        SPK_CUDA(ops.status.ensure_zeroed(((n + kSetTile - 1) / kSetTile + 1) * 8, s), "cudaMallocAsync");
+        SPK_CUDA(cudaMemsetAsync(ops.counters.ptr, 0, 33 * 4, s), "cudaMemsetAsync");
+        spk::SelectSpec sp{spec->where_mask,
+                           {spec->where_value[0], spec->where_value[1]},
+                           {spec->out_source[0], spec->out_source[1]},
+                           {spec->out_value[0], spec->out_value[1]}};
+        auto kernel = spk::select_rows_kernel<kThreads, kSetItems>;
+        const size_t tiles = (n + kSetTile - 1) / kSetTile;
+        kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, tiles), kThreads, 0, s>>>(
+            in->level[0].as<u64>(), n, sp, ops.a.as<u64>(), ops.counts.as<u64>(), ops.status.as<u64>(),
+            ops.counters.as<u32>(), ops.ex.epoch++, ops.counters.as<u32>() + 32);
+        SPK_CUDA(cudaGetLastError(), "select_rows_kernel");
+        rc = read_count(st, ops, ops.counts.as<u64>(), &m);
+        if (rc) return rc;
+    }
+    if (m > 0) {
+        const u32 mv = std::max(spec->out_source[0] == 2 ? spec->out_value[0] : 0u,
+                                spec->out_source[1] == 2 ? spec->out_value[1] : 0u);
+        st->max_value = std::max(st->max_value, mv);
+    }
+    return store_sorted_unique(st, m, out_id, rows);
+}
+
+int sparkalog_store_join(sparkalog_store* st, u32 left_id, u32 right_id, u32 left_key, u32 right_key,
+                         const u32* proj_side, const u32* proj_col, u32 out_id, size_t* rows) {
+    if (!st || !proj_side || !proj_col) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null argument");
+    if (left_key > 1 || right_key > 1 || proj_side[0] > 1 || proj_side[1] > 1 || proj_col[0] > 1 || proj_col[1] > 1)
+        return fail(SPARKALOG_E_MISSING_COLUMN, "join names a column outside a binary relation");
+    RelState* left = st->find(left_id);
+    RelState* right = st->find(right_id);
+    if (!left) return fail(SPARKALOG_E_MISSING, "relation " + std::to_string(left_id) + " is not registered");
+    if (!right) return fail(SPARKALOG_E_MISSING, "relation " + std::to_string(right_id) + " is not registered");
+    if (st->find(out_id))
+        return fail(SPARKALOG_E_DUPLICATE, "relation " + std::to_string(out_id) + " is already registered");
+    cudaStream_t s = st->stream;
+    int rc = materialize(st, *left);
+    if (rc) return rc;
+    StoreOps* ops_ptr = store_ops(st);
+    if (!ops_ptr) return static_cast<int>(cudaErrorMemoryAllocation);
+    StoreOps& ops = *ops_ptr;
+    sparkalog_executor& ex = ops.ex;
+    if (!ex.counters.ptr) {
+        // The index build reports through the executor's error words.
+        const size_t bytes = (kCounterWords + 64) * 4;
+        SPK_CUDA(ex.counters.ensure(bytes, s), "cudaMallocAsync");
+        SPK_CUDA(cudaMemsetAsync(ex.counters.ptr, 0, bytes, s), "cudaMemsetAsync");
+    }
+    IndexCache ic;
+    rc = build_index(&ex, st, ic, right_id, right_key);
+    if (rc) return rc;
+    const u64 n = left->level_n[0];
+    const u64 bound = n * static_cast<u64>(ic.max_degree);
+    u64 m = 0;
+    if (bound > 0) {
+        SPK_CUDA(ops.a.ensure(bound * 8, s), "cudaMallocAsync");
+        SPK_CUDA(ops.status.ensure_zeroed(((n + kJoinTile - 1) / kJoinTile + 1) * 8, s), "cudaMallocAsync");
+        SPK_CUDA(cudaMemsetAsync(ops.counters.ptr, 0, 33 * 4, s), "cudaMemsetAsync");
+        SPK_CUDA(cudaMemsetAsync(ops.counts.ptr, 0, 32, s), "cudaMemsetAsync");
+        ops.host[0] = n;
+        SPK_CUDA(cudaMemcpyAsync(ops.counts.as<u64>() + 1, ops.host, 8, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
+        spk::FusedJoinArgs a{};
+        a.delta = left->level[0].as<u64>();
+        a.delta_count = ops.counts.as<u64>() + 1;
+        a.left_key = left_key;
+        if (ic.bucketed) {
+            a.bucket_dir = ic.bucket_dir.as<u32>();
+            a.bucket_shift = ic.bucket_shift;
+            a.buckets = ic.buckets;
+            a.keys = ic.keys32.as<u32>();
+        } else {
+            a.dense_offsets = ic.offsets.as<u32>();
+            a.dense_keys = ic.num_keys;
+        }
+        a.rows = ic.identity ? nullptr : ic.rows.as<u32>();
+        a.right = right->level[0].as<u64>();
+        a.side[0] = proj_side[0];
+        a.side[1] = proj_side[1];
+        a.col[0] = proj_col[0];
+        a.col[1] = proj_col[1];
+        a.out = ops.a.as<u64>();
+        a.capacity = bound;
+        a.count_in = ops.counts.as<u64>() + 2;
+        a.count_out = ops.counts.as<u64>() + 3;
+        a.status = ops.status.as<u64>();
+        a.tile_counter = ops.counters.as<u32>();
+        a.epoch_ptr = nullptr;
+        a.epoch_add = ex.epoch++;
+        a.err = ops.counters.as<u32>() + 32;
+        auto kernel = spk::join_fused_kernel<kThreads, kJoinItems>;
+        const size_t tiles = (n + kJoinTile - 1) / kJoinTile;
+        kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, std::max<size_t>(tiles, 1)), kThreads, 0,
+                 s>>>(a);
+        SPK_CUDA(cudaGetLastError(), "join_fused_kernel");
+        rc = read_count(st, ops, ops.counts.as<u64>() + 3, &m);
+        if (rc) return rc;
+    }
+    for (DevArray* d : {&ic.offsets, &ic.rows, &ic.keys32, &ic.bucket_dir}) d->release(s);
+    return store_sorted_unique(st, m, out_id, rows);
+}
+
 int sparkalog_store_append(sparkalog_store* st, u32 id, const u32* first, const u32* second, size_t rows,
                            int location) {
     if (!st) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null store");

@@ -519,6 +519,73 @@ __global__ void __launch_bounds__(THREADS) filter_segments_kernel(const u64* in,
     }
 }
 
+// Selection and projection of packed rows (an atom with constants or a
+// repeated variable, and a clause head with constants): a row is kept when
+// every set bit of where_mask holds (bit 0: first == where_value[0], bit 1:
+// second == where_value[1], bit 2: first == second), and leaves as the pair
+// (out column 0, out column 1), each an input column (source 0 or 1) or a
+// constant (source 2). Compacted in order with a decoupled look-back.
+struct SelectSpec {
+    u32 where_mask;
+    u32 where_value[2];
+    u32 out_source[2];
+    u32 out_value[2];
+};
+
+__device__ __forceinline__ u32 select_column(u64 row, u32 source, u32 value) {
+    return source == 0 ? static_cast<u32>(row >> 32) : (source == 1 ? static_cast<u32>(row) : value);
+}
+
+template <int THREADS, int ITEMS>
+__global__ void __launch_bounds__(THREADS) select_rows_kernel(const u64* in, u64 n, SelectSpec sp, u64* out,
+                                                              u64* out_count, u64* status, u32* tile_counter,
+                                                              u32 epoch, u32* err) {
+    constexpr int kTile = THREADS * ITEMS;
+    __shared__ CompactShared<THREADS> cs;
+    __shared__ u64 stage[kTile];
+    const u64 num_tiles = (n + kTile - 1) / kTile;
+    if (num_tiles == 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) *out_count = 0;
+        return;
+    }
+    for (;;) {
+        if (threadIdx.x == 0) cs.tile = atomicAdd(tile_counter, 1u);
+        __syncthreads();
+        const u64 tile = cs.tile;
+        if (tile >= num_tiles) break;
+        const u64 base = tile * kTile + static_cast<u64>(threadIdx.x) * ITEMS;
+        u64 v[ITEMS];
+        u32 keep = 0;
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i) {
+            const u64 idx = base + i;
+            v[i] = 0;
+            if (idx < n) {
+                const u64 row = in[idx];
+                const u32 c0 = static_cast<u32>(row >> 32), c1 = static_cast<u32>(row);
+                const bool ok = (!(sp.where_mask & 1u) || c0 == sp.where_value[0]) &&
+                                (!(sp.where_mask & 2u) || c1 == sp.where_value[1]) &&
+                                (!(sp.where_mask & 4u) || c0 == c1);
+                if (ok) {
+                    keep |= 1u << i;
+                    v[i] = pack2(select_column(row, sp.out_source[0], sp.out_value[0]),
+                                 select_column(row, sp.out_source[1], sp.out_value[1]));
+                }
+            }
+        }
+        u32 excl, total;
+        const u64 off = compact_offsets<THREADS>(__popc(keep), &excl, &total, tile, status, epoch, err, cs);
+        u32 w = excl;
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i)
+            if (keep & (1u << i)) stage[w++] = v[i];
+        __syncthreads();
+        for (u32 j = threadIdx.x; j < total; j += THREADS) out[off + j] = stage[j];
+        if (tile == num_tiles - 1 && threadIdx.x == 0) *out_count = off + total;
+        __syncthreads();
+    }
+}
+
 // Longest run of equal first-column keys in sorted rows (the index's largest
 // match count, which bounds a join's output).
 static __global__ void max_run_kernel(const u64* sorted, u64 n, u32* max_degree) {

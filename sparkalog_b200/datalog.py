@@ -63,6 +63,41 @@ class NegationClause:
     negative: RelationId
 
 
+@dataclass(frozen=True)
+class PlannedAtom:
+    """PlannedAtom (crates/sparkalog-relational/src/lib.rs:104-109) of a binary
+    predicate: each term is ``("b", id)``, a binding, or ``("v", value)``, a
+    constant (an interned value id)."""
+
+    relation: RelationId
+    terms: tuple
+
+
+@dataclass(frozen=True)
+class GeneralClause:
+    """A non-recursive clause (RelationalClausePlan, relational/src/lib.rs:113-121):
+    ``target(head) :- positive..., !negative...``, evaluated on the device."""
+
+    target: RelationId
+    head: tuple
+    positive: tuple
+    negative: tuple = ()
+
+
+@dataclass(frozen=True)
+class NonRecursiveScc:
+    """A non-recursive SCC of a stratified program: every clause deriving
+    ``target`` (general.rs:391-402 evaluates them once, in order, and unions
+    their outputs)."""
+
+    target: RelationId
+    clauses: tuple
+
+
+class UnsupportedClause(ValueError):
+    """A clause shape the device lowering does not take (see evaluate_clause)."""
+
+
 @dataclass
 class GeneralSccSummary:
     """GeneralSccSummary (general.rs:344-349): rows of each SCC relation,
@@ -205,9 +240,11 @@ def execute_stratified(predicate_count: int, strata: list, facts=None,
     """Runs a stratified binary program on the device, SCC by SCC in order.
 
     ``strata`` lists, in schedule order, ``BinarySccPlan`` entries (recursive
-    SCCs: seeded from the facts, then iterated by the RecursiveExecutor) and
+    SCCs: seeded from the facts, then iterated by the RecursiveExecutor),
     ``NegationClause`` entries (evaluated with the store's anti-join against
-    the completed FULL of the negated relation). Returns the store and one
+    the completed FULL of the negated relation) and ``NonRecursiveScc``
+    entries (general non-recursive clauses: constants, repeated bindings,
+    joins of two atoms, head constants, negated atoms; see evaluate_clause). Returns the store and one
     GeneralSccSummary per SCC, as execute_general does (general.rs:371-389).
     """
     plan = BinaryProgramPlan(predicate_count=predicate_count, facts=list(facts or []),
@@ -231,6 +268,7 @@ def execute_stratified(predicate_count: int, strata: list, facts=None,
             sets[seed.target.value] = np.unique(np.concatenate([sets[seed.target.value], projected]))
     recursive = {r.value for scc in plan.recursive_sccs for r in scc.plan.relations}
     derived = {s.target.value for s in strata if isinstance(s, NegationClause)}
+    derived |= {s.target.value for s in strata if isinstance(s, NonRecursiveScc) and len(sets[s.target.value]) == 0}
     store = RelationStore(stream)
     for rid, packed in enumerate(sets):
         if rid in derived:
@@ -247,7 +285,163 @@ def execute_stratified(predicate_count: int, strata: list, facts=None,
             s = executor.run(store, max_iterations)
             executor.close()
             summaries.append(GeneralSccSummary(s.relation_rows, s.iterations, s.total_new_rows))
+        elif isinstance(item, NonRecursiveScc):
+            summaries.append(evaluate_nonrecursive(store, item))
         else:
             rows = store.anti_join(item.positive, item.negative, item.target)
             summaries.append(GeneralSccSummary([(item.target, rows)], 1, 0))
     return store, summaries
+
+
+# Relation ids at and above this are the clause evaluator's temporaries.
+_TEMP_BASE = 1 << 30
+
+
+class _Temps:
+    def __init__(self, store: RelationStore):
+        self.store = store
+        self.next = _TEMP_BASE
+        self.live: list[int] = []
+
+    def new(self) -> int:
+        self.next += 1
+        self.live.append(self.next)
+        return self.next
+
+    def drop_all(self, keep=()) -> None:
+        for t in self.live:
+            if t not in keep and self.store.has(t):
+                self.store.drop(t)
+        self.live = [t for t in self.live if t in keep]
+
+
+def _bindings(atom: PlannedAtom) -> dict:
+    """binding id -> the first column that binds it."""
+    out = {}
+    for col, (kind, x) in enumerate(atom.terms):
+        if kind == "b" and x not in out:
+            out[x] = col
+    return out
+
+
+def _atom_filter(atom: PlannedAtom):
+    """(where, same) of an atom: constants compared, a repeated binding equal."""
+    where = [None, None]
+    for col, (kind, x) in enumerate(atom.terms):
+        if kind == "v":
+            where[col] = int(x)
+    same = (atom.terms[0][0] == "b" and atom.terms[1][0] == "b" and atom.terms[0][1] == atom.terms[1][1])
+    return tuple(where), same
+
+
+def evaluate_clause(store: RelationStore, clause: GeneralClause, temps: _Temps) -> int:
+    """Evaluates one non-recursive binary clause on the device (general.rs:478-551)
+    into a new temporary relation and returns its id.
+
+    Taken: one positive atom, or two that share exactly one binding; constants
+    and repeated bindings in positive atoms and constants in the head; negated
+    atoms whose two bindings are the head's two bindings (in either order).
+    Other shapes raise UnsupportedClause (GeneralCpu evaluates them)."""
+    pos = list(clause.positive)
+    for atom in pos + list(clause.negative):
+        if len(atom.terms) != 2:
+            raise UnsupportedClause("binary predicates only")
+    if len(clause.head) != 2:
+        raise UnsupportedClause("binary predicates only")
+    if len(pos) == 1:
+        a = pos[0]
+        where, same = _atom_filter(a)
+        cols = _bindings(a)
+        project = []
+        for kind, x in clause.head:
+            if kind == "v":
+                project.append(("const", int(x)))
+            elif x in cols:
+                project.append(cols[x])
+            else:
+                raise UnsupportedClause("head binding not bound by a positive atom")
+        out = temps.new()
+        store.select(a.relation, out, where, same, tuple(project))
+    elif len(pos) == 2:
+        a, b = pos
+        ca, cb = _bindings(a), _bindings(b)
+        shared = sorted(set(ca) & set(cb))
+        if len(shared) != 1:
+            raise UnsupportedClause("two positive atoms must share exactly one binding")
+        z = shared[0]
+        inputs = []
+        for atom in (a, b):
+            where, same = _atom_filter(atom)
+            if where != (None, None) or same:
+                t = temps.new()
+                store.select(atom.relation, t, where, same, (0, 1))
+                inputs.append(t)
+            else:
+                inputs.append(atom.relation)
+        projection, post, consts = [], [], False
+        for kind, x in clause.head:
+            if kind == "v":
+                projection.append((0, ca[z]))
+                post.append(("const", int(x)))
+                consts = True
+            elif x in ca:
+                projection.append((0, ca[x]))
+                post.append(len(post))
+            elif x in cb:
+                projection.append((1, cb[x]))
+                post.append(len(post))
+            else:
+                raise UnsupportedClause("head binding not bound by a positive atom")
+        out = temps.new()
+        store.join(inputs[0], inputs[1], ca[z], cb[z], tuple(projection), out)
+        if consts:
+            t = temps.new()
+            store.select(out, t, (None, None), False, tuple(post))
+            out = t
+    else:
+        raise UnsupportedClause("one or two positive atoms")
+    head = [x if kind == "b" else None for kind, x in clause.head]
+    for n in clause.negative:
+        kinds = [k for k, _ in n.terms]
+        ids = [x for _, x in n.terms]
+        if kinds != ["b", "b"] or None in head:
+            raise UnsupportedClause("a negated atom must bind the head's two bindings")
+        if ids == head:
+            right = n.relation
+        elif ids == head[::-1]:
+            right = temps.new()
+            store.select(n.relation, right, (None, None), False, (1, 0))
+        else:
+            raise UnsupportedClause("a negated atom must bind the head's two bindings")
+        t = temps.new()
+        store.anti_join(out, right, t)
+        out = t
+    return out
+
+
+def evaluate_nonrecursive(store: RelationStore, scc: NonRecursiveScc) -> GeneralSccSummary:
+    """Every clause of a non-recursive SCC, unioned into its target (which may
+    already hold facts); GeneralCpu's summary for it: 1 round when it has a
+    clause, 0 new rows (general.rs:391-402)."""
+    temps = _Temps(store)
+    try:
+        results = [evaluate_clause(store, c, temps) for c in scc.clauses]
+        target = scc.target.value
+        for k, t in enumerate(results):
+            if not store.has(target):
+                store.select(t, target, (None, None), False, (0, 1))
+                continue
+            n = store.rows(t)
+            if n:
+                import torch
+
+                cols = (torch.empty(n, dtype=torch.int32, device="cuda"),
+                        torch.empty(n, dtype=torch.int32, device="cuda"))
+                store.read_into(t, 0, cols[0], cols[1])
+                store.append(target, cols)
+        if not store.has(target):
+            empty = np.zeros(0, dtype=np.uint32)
+            store.insert_static(target, (empty, empty))
+    finally:
+        temps.drop_all()
+    return GeneralSccSummary([(scc.target, store.rows(scc.target))], 1 if scc.clauses else 0, 0)

@@ -158,6 +158,48 @@ class RelationStore:
         _check(_native.load().sparkalog_store_anti_join(self._h, *ids))
         return self.rows(ids[2])
 
+    def drop(self, rid: RelationId | int) -> None:
+        """Removes a relation and frees its device memory."""
+        _check(_native.load().sparkalog_store_drop(self._h, int(getattr(rid, "value", rid))))
+
+    def has(self, rid: RelationId | int) -> bool:
+        n = ctypes.c_size_t(0)
+        return _native.load().sparkalog_store_rows(self._h, int(getattr(rid, "value", rid)), FULL,
+                                                   ctypes.byref(n)) == 0
+
+    def select(self, rid: RelationId | int, out: RelationId | int, where=(None, None), same: bool = False,
+               project=(0, 1)) -> int:
+        """out = {(c0, c1)} over the rows (x, y) of FULL(rid) with x == where[0] and
+        y == where[1] (each when not None) and x == y when ``same``; each output
+        column is ``0`` (x), ``1`` (y) or ``("const", value)``. Returns |out|."""
+        sp = _native.SelectC()
+        sp.where_mask = (1 if where[0] is not None else 0) | (2 if where[1] is not None else 0) | (4 if same else 0)
+        sp.where_value[0] = where[0] or 0
+        sp.where_value[1] = where[1] or 0
+        for k, src in enumerate(project):
+            if isinstance(src, tuple):
+                sp.out_source[k], sp.out_value[k] = 2, int(src[1])
+            else:
+                sp.out_source[k] = int(src)
+        n = ctypes.c_size_t(0)
+        _check(_native.load().sparkalog_store_select(self._h, int(getattr(rid, "value", rid)), ctypes.byref(sp),
+                                                     int(getattr(out, "value", out)), ctypes.byref(n)))
+        return int(n.value)
+
+    def join(self, left: RelationId | int, right: RelationId | int, left_key: int, right_key: int,
+             projection, out: RelationId | int) -> int:
+        """out = distinct projection of left ⋈ right on left[left_key] == right[right_key];
+        ``projection`` is ((side, column), (side, column)) with side 0 = left, 1 = right."""
+        sides = _u32([projection[0][0], projection[1][0]])
+        cols = _u32([projection[0][1], projection[1][1]])
+        n = ctypes.c_size_t(0)
+        _check(_native.load().sparkalog_store_join(self._h, int(getattr(left, "value", left)),
+                                                   int(getattr(right, "value", right)), left_key, right_key,
+                                                   sides.ctypes.data_as(_native.c_u32p),
+                                                   cols.ctypes.data_as(_native.c_u32p),
+                                                   int(getattr(out, "value", out)), ctypes.byref(n)))
+        return int(n.value)
+
     def load_binary_u32(self, rid: RelationId | int, text, recursive: bool = False) -> int:
         """Parses whitespace-separated u32 pairs on the GPU and inserts them as relation
         ``rid`` (load_binary_u32, crates/sparkalog-storage/src/io.rs:72-141); ``text``
