@@ -20,9 +20,29 @@ def x_range(nodes: int, rank: int, world: int) -> tuple[int, int]:
     return nodes * rank // world, nodes * (rank + 1) // world
 
 
-def partition_seed(src: np.ndarray, dst: np.ndarray, nodes: int, rank: int, world: int):
-    """Seed rows whose x lies in this rank's range (src must be sorted)."""
-    lo, hi = x_range(nodes, rank, world)
+def balanced_bounds(src: np.ndarray, nodes: int, world: int) -> list[int]:
+    """x boundaries [b_0 = 0, ..., b_world = nodes] that give every rank about
+    the same number of seed rows (src sorted): for skewed graphs, where equal
+    node ranges would give some ranks most of the work. Boundaries fall on x
+    values, so no x is split between ranks."""
+    n = len(src)
+    bounds = [0]
+    for r in range(1, world):
+        k = n * r // world
+        x = int(src[k]) if k < n else nodes
+        bounds.append(max(bounds[-1], min(x, nodes)))
+    bounds.append(nodes)
+    return bounds
+
+
+def partition_seed(src: np.ndarray, dst: np.ndarray, nodes: int, rank: int, world: int, balanced: bool = False):
+    """Seed rows whose x lies in this rank's range (src must be sorted):
+    equal node ranges, or with ``balanced`` the ranges of balanced_bounds."""
+    if balanced:
+        bounds = balanced_bounds(src, nodes, world)
+        lo, hi = bounds[rank], bounds[rank + 1]
+    else:
+        lo, hi = x_range(nodes, rank, world)
     a = np.searchsorted(src, lo, side="left")
     b = np.searchsorted(src, hi, side="left")
     return src[a:b], dst[a:b]

@@ -70,3 +70,12 @@ def test_x_ranges_tile_the_nodes():
         ranges = [sharding.x_range(1001, r, world) for r in range(world)]
         assert ranges[0][0] == 0 and ranges[-1][1] == 1001
         assert all(a[1] == b[0] for a, b in zip(ranges, ranges[1:]))
+
+
+def test_balanced_bounds_split_no_x():
+    src = np.sort(np.random.default_rng(3).integers(0, 50, 10_000)).astype(np.uint32)
+    for world in (2, 3, 7):
+        b = sharding.balanced_bounds(src, 50, world)
+        assert b[0] == 0 and b[-1] == 50 and b == sorted(b)
+        rows = [len(sharding.partition_seed(src, src, 50, r, world, balanced=True)[0]) for r in range(world)]
+        assert sum(rows) == len(src)
