@@ -151,10 +151,11 @@ def measured_peaks():
 
 
 def partition(src, dst, nodes, rank, world):
-    """Seed rows whose x lies in this rank's contiguous node range."""
+    """Seed rows whose x lies in this rank's contiguous node range (ranges
+    balanced by seed rows)."""
     from sparkalog_b200.sharding import partition_seed
 
-    return partition_seed(src, dst, nodes, rank, world)
+    return partition_seed(src, dst, nodes, rank, world, balanced=True)
 
 
 class ClockSampler:
