@@ -4,7 +4,7 @@ workload generators, x-range partitioning."""
 import numpy as np
 import pytest
 
-from sparkalog_b200 import generators
+from sparkalog_b200 import generators, sharding
 
 
 def test_batched_tagging_and_split():
@@ -68,9 +68,12 @@ def test_bench_partition_covers_every_row():
     parts = [bench.partition(src, dst, 1000, r, 3) for r in range(3)]
     assert sum(len(p[0]) for p in parts) == len(src)
     assert np.array_equal(np.concatenate([p[0] for p in parts]), src)
+    # Ranges are balanced by seed rows and never split an x between ranks.
+    bounds = sharding.balanced_bounds(src, 1000, 3)
     for r, (s, _) in enumerate(parts):
         if len(s):
-            assert s.min() >= 1000 * r // 3 and s.max() < 1000 * (r + 1) // 3
+            assert s.min() >= bounds[r] and s.max() < bounds[r + 1]
+        assert abs(len(s) - len(src) / 3) <= 0.05 * len(src)
 
 
 def test_bench_baseline_helpers_on_cpu():
