@@ -645,6 +645,7 @@ struct sparkalog_executor {
     };
     bool profiling = false;
     bool fused_enabled = true;
+    cudaStream_t stream = nullptr;  // the store's stream at compile time (syncs of executor-only state)
     bool device_loop = true;       // tail rounds as a CUDA graph WHILE loop (see spk_loop.cuh)
     u64 loop_launches = 0;         // graph launches of the device loop
     u64 loop_rounds = 0;           // rounds applied by the device loop
@@ -1062,7 +1063,8 @@ int cascade_levels(sparkalog_executor* ex, sparkalog_store* st, RelState& tr) {
 // one round per iteration until the round-end kernel stops it. The graph and
 // the small buffers it names (descriptor, counters, look-back words, trace)
 // are cached per (device, stream, shape), so executors created one after the
-// other (a fresh executor per fixpoint) reuse one instantiated graph.
+// other (a fresh executor per fixpoint) reuse one instantiated graph. Streams
+// of different host threads get different entries.
 // ---------------------------------------------------------------------------
 constexpr u64 kLoopTraceCap = 4096;     // rounds one graph launch may apply
 constexpr int kLoopWordBytes = 256;     // counts[4] u64 | tile counters u32[16] | error bits u32[16]
@@ -1094,8 +1096,7 @@ struct LoopGrids {
     unsigned fused, anti, merge, split, segment;
 };
 
-// Shared-memory opt-ins and persistent grid sizes of the loop's kernels
-// (queried before the capture starts).
+// Shared-memory opt-ins and persistent grid sizes of the loop's kernels.
 template <int G, int ITEMS>
 cudaError_t prepare_loop_kernels(const LoopGraph& g, LoopGrids* grids) {
     using FL = spk::FusedLayout<kFusedThreads, kFusedCap, kFusedRowCap>;
@@ -1117,29 +1118,44 @@ cudaError_t prepare_loop_kernels(const LoopGraph& g, LoopGrids* grids) {
     return cudaGetLastError();
 }
 
-template <int G, int ITEMS>
-cudaError_t capture_loop_body(LoopGraph& g, cudaStream_t s, cudaGraphConditionalHandle handle, const LoopGrids& gr) {
-    using FL = spk::FusedLayout<kFusedThreads, kFusedCap, kFusedRowCap>;
-    using ML = spk::MergeBulkLayout<kThreads, ITEMS>;
-    cudaError_t e = cudaMemsetAsync(g.words, 0, kLoopWordBytes, s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(g.fused_status, 0, g.fused_status_words * 8, s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(g.anti_status, 0, g.anti_status_words * 8, s);
-    if (e != cudaSuccess) return e;
-    spk::loop_fused_kernel<kFusedThreads, kFusedCap, kFusedRowCap><<<gr.fused, kFusedThreads, FL::kBytes, s>>>(g.desc);
-    spk::loop_anti_join_kernel<kWideThreads, G><<<gr.anti, kWideThreads, 0, s>>>(g.desc);
-    spk::loop_split_kernel<<<gr.split, 256, 0, s>>>(g.desc, static_cast<u32>(kThreads * ITEMS));
-    spk::loop_merge_kernel<kThreads, ITEMS><<<gr.merge, kThreads, ML::kBytes, s>>>(g.desc);
-    spk::loop_round_end_kernel<<<1, 32, 0, s>>>(g.desc, handle);
-    if (g.segments) spk::loop_segment_kernel<<<gr.segment, 256, 0, s>>>(g.desc);
-    return cudaGetLastError();
+// Appends a node to the round body, depending on the previous one.
+cudaError_t add_kernel_node(cudaGraph_t body, cudaGraphNode_t* last, const void* func, unsigned grid,
+                            unsigned threads, size_t smem, void** args) {
+    cudaKernelNodeParams kp{};
+    kp.func = const_cast<void*>(func);
+    kp.gridDim = dim3(grid);
+    kp.blockDim = dim3(threads);
+    kp.sharedMemBytes = static_cast<unsigned>(smem);
+    kp.kernelParams = args;
+    cudaGraphNode_t node;
+    cudaError_t e = cudaGraphAddKernelNode(&node, body, *last ? last : nullptr, *last ? 1 : 0, &kp);
+    if (e == cudaSuccess) *last = node;
+    return e;
+}
+
+cudaError_t add_memset_node(cudaGraph_t body, cudaGraphNode_t* last, void* dst, size_t bytes) {
+    cudaMemsetParams mp{};
+    mp.dst = dst;
+    mp.value = 0;
+    mp.elementSize = 4;
+    mp.width = bytes / 4;
+    mp.height = 1;
+    mp.pitch = 0;
+    cudaGraphNode_t node;
+    cudaError_t e = cudaGraphAddMemsetNode(&node, body, *last ? last : nullptr, *last ? 1 : 0, &mp);
+    if (e == cudaSuccess) *last = node;
+    return e;
 }
 
 // The graph: a WHILE node (condition 1 at every launch) whose body is one
-// round captured from stream `s`.
+// round, built node by node (no stream capture, so other host threads'
+// device-wide calls cannot interfere with its construction).
 template <int G, int ITEMS>
-cudaError_t build_loop_graph_shape(LoopGraph& g, cudaStream_t s) {
-    LoopGrids grids{};
-    cudaError_t e = prepare_loop_kernels<G, ITEMS>(g, &grids);
+cudaError_t build_loop_graph_shape(LoopGraph& g) {
+    using FL = spk::FusedLayout<kFusedThreads, kFusedCap, kFusedRowCap>;
+    using ML = spk::MergeBulkLayout<kThreads, ITEMS>;
+    LoopGrids gr{};
+    cudaError_t e = prepare_loop_kernels<G, ITEMS>(g, &gr);
     if (e != cudaSuccess) return e;
     e = cudaGraphCreate(&g.graph, 0);
     if (e != cudaSuccess) return e;
@@ -1155,34 +1171,49 @@ cudaError_t build_loop_graph_shape(LoopGraph& g, cudaStream_t s) {
     e = cudaGraphAddNode(&node, g.graph, nullptr, 0, &cp);
     if (e != cudaSuccess) return e;
     cudaGraph_t body = cp.conditional.phGraph_out[0];
-    e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
-    if (e != cudaSuccess) return e;
-    const cudaError_t ce = capture_loop_body<G, ITEMS>(g, s, handle, grids);
-    cudaGraph_t captured = nullptr;
-    e = cudaStreamEndCapture(s, &captured);
-    if (ce != cudaSuccess) return ce;
+    spk::LoopDesc* desc = g.desc;
+    u32 tile = static_cast<u32>(kThreads * ITEMS);
+    void* desc_args[] = {&desc};
+    void* split_args[] = {&desc, &tile};
+    void* end_args[] = {&desc, &handle};
+    cudaGraphNode_t last = nullptr;
+    if (e == cudaSuccess) e = add_memset_node(body, &last, g.words, kLoopWordBytes);
+    if (e == cudaSuccess) e = add_memset_node(body, &last, g.fused_status, g.fused_status_words * 8);
+    if (e == cudaSuccess) e = add_memset_node(body, &last, g.anti_status, g.anti_status_words * 8);
+    if (e == cudaSuccess)
+        e = add_kernel_node(body, &last,
+                            reinterpret_cast<const void*>(spk::loop_fused_kernel<kFusedThreads, kFusedCap, kFusedRowCap>),
+                            gr.fused, kFusedThreads, FL::kBytes, desc_args);
+    if (e == cudaSuccess)
+        e = add_kernel_node(body, &last, reinterpret_cast<const void*>(spk::loop_anti_join_kernel<kWideThreads, G>),
+                            gr.anti, kWideThreads, 0, desc_args);
+    if (e == cudaSuccess)
+        e = add_kernel_node(body, &last, reinterpret_cast<const void*>(spk::loop_split_kernel), gr.split, 256, 0,
+                            split_args);
+    if (e == cudaSuccess)
+        e = add_kernel_node(body, &last, reinterpret_cast<const void*>(spk::loop_merge_kernel<kThreads, ITEMS>),
+                            gr.merge, kThreads, ML::kBytes, desc_args);
+    if (e == cudaSuccess)
+        e = add_kernel_node(body, &last, reinterpret_cast<const void*>(spk::loop_round_end_kernel), 1, 32, 0,
+                            end_args);
+    if (e == cudaSuccess && g.segments)
+        e = add_kernel_node(body, &last, reinterpret_cast<const void*>(spk::loop_segment_kernel), gr.segment, 256, 0,
+                            desc_args);
     if (e != cudaSuccess) return e;
     return cudaGraphInstantiate(&g.exec, g.graph, 0);
 }
 
 template <int G>
-cudaError_t build_loop_graph_lanes(LoopGraph& g, cudaStream_t s) {
-    if (g.items == 7) return build_loop_graph_shape<G, 7>(g, s);
-    if (g.items == 15) return build_loop_graph_shape<G, 15>(g, s);
-    return build_loop_graph_shape<G, 11>(g, s);
+cudaError_t build_loop_graph_lanes(LoopGraph& g) {
+    if (g.items == 7) return build_loop_graph_shape<G, 7>(g);
+    if (g.items == 15) return build_loop_graph_shape<G, 15>(g);
+    return build_loop_graph_shape<G, 11>(g);
 }
 
-// Captured on a private stream: the legacy default stream, which callers may
-// use, cannot be captured, and the graph launches on any stream.
 cudaError_t build_loop_graph(LoopGraph& g) {
-    cudaStream_t s = nullptr;
-    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
-    if (e != cudaSuccess) return e;
-    if (g.lanes == 4) e = build_loop_graph_lanes<4>(g, s);
-    else if (g.lanes == 16) e = build_loop_graph_lanes<16>(g, s);
-    else e = build_loop_graph_lanes<8>(g, s);
-    cudaStreamDestroy(s);
-    return e;
+    if (g.lanes == 4) return build_loop_graph_lanes<4>(g);
+    if (g.lanes == 16) return build_loop_graph_lanes<16>(g);
+    return build_loop_graph_lanes<8>(g);
 }
 
 // The cached graph for this shape (built on first use).
@@ -2510,6 +2541,7 @@ int sparkalog_executor_compile(sparkalog_store* st, const u32* relations, size_t
         ex->targets.push_back(std::move(trt));
     }
     ex->index.resize(rule_count);
+    ex->stream = st->stream;
     ex->counts_words = 0;
     for (auto& t : ex->targets) ex->counts_words += t.rules.size() + 3;
     cudaStream_t s = st->stream;
@@ -2530,7 +2562,9 @@ int sparkalog_executor_compile(sparkalog_store* st, const u32* relations, size_t
 
 void sparkalog_executor_destroy(sparkalog_executor* ex) {
     if (!ex) return;
-    cudaStream_t s = nullptr;
+    // Buffers are freed in the order of the stream that used them, and the
+    // pinned count buffers go back to the pool once that stream is idle.
+    cudaStream_t s = ex->stream;
     for (auto& t : ex->targets) {
         t.j_a.release(s);
         t.j_b.release(s);
@@ -2552,7 +2586,7 @@ void sparkalog_executor_destroy(sparkalog_executor* ex) {
     ex->index_sort.status.release(s);
     ex->index_pairs[0].release(s);
     ex->index_pairs[1].release(s);
-    cudaDeviceSynchronize();
+    cudaStreamSynchronize(s);
     pinned_put(ex->host_counts, ex->counts_words * 8 + 512);
     pinned_put(ex->host_rule_delta, std::max<size_t>(ex->rules.size(), 1) * 8);
     pinned_put(ex->host_active, ex->relations.size() * spk::kMaxPasses * 4 + 64);
@@ -2566,7 +2600,7 @@ void sparkalog_executor_destroy(sparkalog_executor* ex) {
 
 int sparkalog_executor_track_segments(sparkalog_executor* ex, u32 shift, u32 count) {
     if (!ex || shift > 31) return fail(SPARKALOG_E_INVALID_ARGUMENT, "invalid segment tracking arguments");
-    cudaStream_t s = nullptr;
+    cudaStream_t s = ex->stream;
     ex->seg_shift = shift;
     ex->seg_count = count;
     if (count) {
@@ -2582,12 +2616,14 @@ int sparkalog_executor_track_segments(sparkalog_executor* ex, u32 shift, u32 cou
 int sparkalog_executor_segment_stats(sparkalog_executor* ex, u32* last_active_round, u64* new_rows) {
     if (!ex || !last_active_round || !new_rows) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null argument");
     if (ex->seg_count == 0) return 0;
-    SPK_CUDA(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
-    SPK_CUDA(cudaMemcpy(last_active_round, ex->seg_seen.ptr, static_cast<size_t>(ex->seg_count) * 4,
-                        cudaMemcpyDeviceToHost),
-             "cudaMemcpy");
-    SPK_CUDA(cudaMemcpy(new_rows, ex->seg_new.ptr, static_cast<size_t>(ex->seg_count) * 8, cudaMemcpyDeviceToHost),
-             "cudaMemcpy");
+    cudaStream_t s = ex->stream;
+    SPK_CUDA(cudaMemcpyAsync(last_active_round, ex->seg_seen.ptr, static_cast<size_t>(ex->seg_count) * 4,
+                             cudaMemcpyDeviceToHost, s),
+             "cudaMemcpyAsync");
+    SPK_CUDA(cudaMemcpyAsync(new_rows, ex->seg_new.ptr, static_cast<size_t>(ex->seg_count) * 8,
+                             cudaMemcpyDeviceToHost, s),
+             "cudaMemcpyAsync");
+    SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
     return 0;
 }
 
