@@ -8,9 +8,9 @@
 // (rounds of a few thousand to a hundred thousand rows) that round trip and
 // the launch latency around it cost about as much as the kernels. Here one
 // round is a fixed sequence of kernels whose pointers and sizes live in a
-// device descriptor (LoopDesc), so the same graph body serves every round: clear the round's counters, fused join + order, group-searched
-// anti-join, diagonal splits, bulk merge of NEWT into TAIL, and the round-end
-// kernel. The round-end kernel applies the round on the device
+// device descriptor (LoopDesc), so the same graph body serves every round:
+// clear the round's counters, fused join + order, group-searched anti-join,
+// diagonal splits, bulk merge of NEWT into TAIL, and the round-end kernel. The round-end kernel applies the round on the device
 // (TargetRuntime::apply, generic.rs:360-397: FULL's TAIL <- TAIL u NEWT,
 // DELTA <- NEWT), counts it, tests convergence, and sets the WHILE node's
 // condition. It stops the loop, leaving everything to the host, when:
