@@ -490,6 +490,37 @@ SPARKALOG_API int sparkalog_store_load_delimited_u32(sparkalog_store* store, uin
                                                      size_t bytes, int location, unsigned char delimiter,
                                                      int has_header, int recursive, size_t* rows,
                                                      sparkalog_load_error* error);
+/* Database::load_delimited (database.rs:165-177 over parse_delimited_parallel,
+ * ingest.rs:20-120) for a binary relation of any values: U32, String (a
+ * quoted field, '""' a quote) and Symbol (any other field that is not a
+ * u32), parsed on the GPU, every value interned into `catalog` in row order
+ * as Database::insert interns them (ValueCatalog::intern, catalog.rs:
+ * 108-117: String, Symbol and U32 are distinct values), and the rows of
+ * value ids inserted as relation `id`. Errors as for
+ * sparkalog_store_load_delimited_u32, except that any two values make a
+ * row (a row of another length reports SPARKALOG_LOAD_ARITY). Strings and
+ * symbols are interned by a 62-bit key of their bytes and every value is
+ * compared byte for byte with the value already holding its key, so a key
+ * shared by two different values fails with SPARKALOG_E_DEVICE_FAULT (it
+ * never merges them); a value may be at most 16 MiB - 1 bytes. The catalog's
+ * U32 entry points still work on the same catalog; decode_u32 fails on the
+ * id of a String or Symbol. */
+SPARKALOG_API int sparkalog_store_load_delimited_values(sparkalog_store* store, sparkalog_catalog* catalog,
+                                                        uint32_t id, const char* text, size_t bytes, int location,
+                                                        unsigned char delimiter, int has_header, int recursive,
+                                                        size_t* rows, sparkalog_load_error* error);
+
+/* The catalog's values in id order, into host memory (Database::query's
+ * decode, database.rs:179-213): kinds[i] 0 U32, 1 String, 2 Symbol;
+ * numbers[i] a U32's value; a String's or Symbol's text is
+ * bytes[offsets[i] .. offsets[i + 1]) (a String without its quotes and
+ * with '""' undone). kinds, numbers and offsets (size + 1 entries) and
+ * bytes may be null; *bytes_used is always set, so a first call with a null
+ * `bytes` sizes the buffer. */
+SPARKALOG_API int sparkalog_catalog_export(sparkalog_catalog* catalog, uint32_t* kinds, uint32_t* numbers,
+                                           uint64_t* offsets, unsigned char* bytes, size_t bytes_capacity,
+                                           size_t* bytes_used);
+
 SPARKALOG_API int sparkalog_executor_stats(sparkalog_executor* executor, sparkalog_kernel_stats* out, int reset);
 
 /* Per-round trace of an executor (the operator cardinalities of each round,

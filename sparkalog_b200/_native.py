@@ -50,6 +50,8 @@ TIER_B = [
     "sparkalog_store_join",
     "sparkalog_store_load_binary_u32",
     "sparkalog_store_load_delimited_u32",
+    "sparkalog_store_load_delimited_values",
+    "sparkalog_catalog_export",
     "sparkalog_catalog_create",
     "sparkalog_catalog_destroy",
     "sparkalog_catalog_intern_u32",
@@ -244,6 +246,11 @@ def load() -> ctypes.CDLL:
     L.sparkalog_store_load_delimited_u32.argtypes = [vp, ctypes.c_uint32, vp, ctypes.c_size_t, i, ctypes.c_ubyte, i,
                                                      i, c_sizep, ctypes.POINTER(LoadErrorC)]
     L.sparkalog_store_load_delimited_u32.restype = i
+    L.sparkalog_store_load_delimited_values.argtypes = [vp, vp, ctypes.c_uint32, vp, ctypes.c_size_t, i,
+                                                        ctypes.c_ubyte, i, i, c_sizep, ctypes.POINTER(LoadErrorC)]
+    L.sparkalog_store_load_delimited_values.restype = i
+    L.sparkalog_catalog_export.argtypes = [vp, c_u32p, c_u32p, c_u64p, vp, ctypes.c_size_t, c_sizep]
+    L.sparkalog_catalog_export.restype = i
     L.sparkalog_catalog_create.argtypes = [vp, ctypes.POINTER(vp)]
     L.sparkalog_catalog_create.restype = i
     L.sparkalog_catalog_destroy.argtypes = [vp]

@@ -1462,14 +1462,26 @@ int sparkalog_reserve_device_memory(size_t bytes, void* stream) {
 struct sparkalog_catalog {
     cudaStream_t stream = nullptr;
     sparkalog_executor ex;          // radix-sort scratch and look-back epochs (no rules)
-    DevArray keys, keys_spare;      // (value << 32 | id), sorted by value
-    DevArray dict;                  // id -> value
+    DevArray keys, keys_spare;      // U32 values: (value << 32 | id), sorted by value
+    DevArray dict;                  // id -> U32 value, or a String/Symbol's string index
     DevArray a, b, list_a, list_b;  // sort buffers
     DevArray staging, ids;          // host input / output staging, ids of a batch
     DevArray words;                 // u64 new-value count, then the u32 error word
     DevArray splits;                // merge diagonals
-    u64 size = 0;
+    u64 size = 0;                   // values (ids 0 .. size - 1)
+    u64 u32_count = 0;              // U32 values (entries of `keys`)
     u64* host = nullptr;            // pinned 64 bytes
+    // String and Symbol values (spk::StringTable), present once one is interned.
+    DevArray kinds;                 // u32 per id: 0 U32, 1 String, 2 Symbol
+    DevArray arena;                 // raw bytes of every string
+    DevArray str_offset, str_length;
+    DevArray skeys, sids, sidx;     // lookup index sorted by key
+    DevArray skeys_spare, sids_spare, sidx_spare;
+    u64 str_count = 0;
+    u64 arena_used = 0;
+    // Scratch of a mixed batch.
+    DevArray tokens, v_keys, v_pos, v_sorted, v_pairs, v_pairs_b, g_head, g_id, g_si, g_new, joint, joint_b,
+        str_src, nk, nid, nsi;
 };
 
 namespace {
@@ -1486,6 +1498,199 @@ int catalog_sort(sparkalog_catalog* c, DevArray& x, DevArray& y, u64 n, u32* err
              "cudaMemcpyAsync");
     SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
     *sorted = *sel ? &y : &x;
+    return 0;
+}
+
+}  // namespace
+
+namespace {
+
+// Interns n tokens (spk_ingest.cuh: U32 values and String/Symbol spans of
+// `text`, all on the device) in order, as ValueCatalog::intern applied to
+// each in turn would (catalog.rs:108-117): ids[p] receives token p's id.
+int catalog_intern_tokens(sparkalog_catalog* c, const u64* tokens, u64 n, const unsigned char* text, u64 text_bytes,
+                          u32* ids) {
+    cudaStream_t s = c->stream;
+    if (n == 0) return 0;
+    if (n > (1ull << 31)) return fail(SPARKALOG_E_TOO_MANY_ROWS, "more than 2^31 values in one batch");
+    u32* err = reinterpret_cast<u32*>(c->words.as<u64>() + 1);
+    auto* counts = reinterpret_cast<unsigned long long*>(c->words.as<u64>() + 2);  // [0] U32, [1] strings, [2] new
+    SPK_CUDA(cudaMemsetAsync(c->words.ptr, 0, 64, s), "cudaMemsetAsync");
+    SPK_CUDA(c->v_keys.ensure(n * 8, s), "cudaMallocAsync");      // U32 (value << 32 | pos)
+    SPK_CUDA(c->a.ensure(n * 8, s), "cudaMallocAsync");           // string keys
+    SPK_CUDA(c->v_pos.ensure(n * 4, s), "cudaMallocAsync");
+    spk::classify_tokens_kernel<<<simple_grid(n), 256, 0, s>>>(tokens, n, text, c->v_keys.as<u64>(), counts,
+                                                               c->a.as<u64>(), c->v_pos.as<u32>(), counts + 1);
+    SPK_CUDA(cudaGetLastError(), "classify_tokens_kernel");
+    SPK_CUDA(cudaMemcpyAsync(c->host, counts, 16, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+    SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    const u64 nu = c->host[0], ns = c->host[1];
+
+    // U32 values: the batch sorted by (value, position); heads the catalog lacks.
+    DevArray* usorted = nullptr;
+    u64 mu = 0;
+    if (nu) {
+        SPK_CUDA(c->b.ensure(nu * 8, s), "cudaMallocAsync");
+        int rc = catalog_sort(c, c->v_keys, c->b, nu, err, &usorted);
+        if (rc) return rc;
+        // Keep the sorted U32 keys in v_keys: `b` is reused below.
+        if (usorted == &c->b) swap_arrays(c->v_keys, c->b);
+        usorted = &c->v_keys;
+        SPK_CUDA(c->list_a.ensure(nu * 8, s), "cudaMallocAsync");
+        spk::new_value_heads_kernel<<<simple_grid(nu), 256, 0, s>>>(usorted->as<u64>(), nu, c->keys.as<u64>(),
+                                                                    c->u32_count, c->list_a.as<u64>(), counts + 2);
+        SPK_CUDA(cudaGetLastError(), "new_value_heads_kernel");
+        SPK_CUDA(cudaMemcpyAsync(c->host, counts + 2, 8, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+        SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+        mu = c->host[0];
+        SPK_CUDA(cudaMemsetAsync(counts + 2, 0, 8, s), "cudaMemsetAsync");
+    }
+
+    // Strings and Symbols: keys sorted, values grouped by key in position
+    // order, heads looked up in the catalog.
+    DevArray* ksorted = nullptr;
+    DevArray* psorted = nullptr;
+    u64 ms = 0;
+    if (ns) {
+        SPK_CUDA(c->v_sorted.ensure(ns * 8, s), "cudaMallocAsync");
+        SPK_CUDA(cudaMemcpyAsync(c->v_sorted.ptr, c->a.ptr, ns * 8, cudaMemcpyDeviceToDevice, s), "cudaMemcpyAsync");
+        SPK_CUDA(c->b.ensure(ns * 8, s), "cudaMallocAsync");
+        int rc = catalog_sort(c, c->v_sorted, c->b, ns, err, &ksorted);
+        if (rc) return rc;
+        SPK_CUDA(c->v_pairs.ensure(ns * 8, s), "cudaMallocAsync");
+        SPK_CUDA(c->v_pairs_b.ensure(ns * 8, s), "cudaMallocAsync");
+        spk::group_pairs_kernel<<<simple_grid(ns), 256, 0, s>>>(c->a.as<u64>(), c->v_pos.as<u32>(), ns,
+                                                                ksorted->as<u64>(), c->v_pairs.as<u64>());
+        SPK_CUDA(cudaGetLastError(), "group_pairs_kernel");
+        // The sorted keys must survive the next sort: keep them apart.
+        if (ksorted == &c->b) swap_arrays(c->v_sorted, c->b);
+        rc = catalog_sort(c, c->v_pairs, c->v_pairs_b, ns, err, &psorted);
+        if (rc) return rc;
+        for (DevArray* d : {&c->g_head, &c->g_id, &c->g_si, &c->g_new}) SPK_CUDA(d->ensure(ns * 4, s), "cudaMallocAsync");
+        SPK_CUDA(cudaMemsetAsync(c->g_new.ptr, 0, ns * 4, s), "cudaMemsetAsync");
+        SPK_CUDA(c->list_b.ensure(ns * 8, s), "cudaMallocAsync");
+        spk::StringTable cat{c->arena.as<unsigned char>(), c->str_offset.as<u64>(), c->str_length.as<u32>(),
+                             c->skeys.as<u64>(), c->sids.as<u32>(), c->sidx.as<u32>(), c->str_count};
+        spk::string_heads_kernel<<<simple_grid(ns), 256, 0, s>>>(
+            psorted->as<u64>(), ns, c->v_sorted.as<u64>(), tokens, text, cat, c->g_head.as<u32>(), c->g_id.as<u32>(),
+            c->g_new.as<u32>(), c->list_b.as<u64>(), counts + 2, err);
+        SPK_CUDA(cudaGetLastError(), "string_heads_kernel");
+        spk::verify_groups_kernel<<<simple_grid(ns), 256, 0, s>>>(psorted->as<u64>(), ns, c->g_head.as<u32>(), tokens,
+                                                                  text, err);
+        SPK_CUDA(cudaGetLastError(), "verify_groups_kernel");
+        SPK_CUDA(cudaMemcpyAsync(c->host, counts + 2, 8, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+        SPK_CUDA(cudaMemcpyAsync(c->host + 1, err, 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+        SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+        ms = c->host[0];
+        const u32 bits = static_cast<u32>(c->host[1] & 0xffffffffu);
+        if (bits & spk::kErrHashCollision)
+            return fail(SPARKALOG_E_DEVICE_FAULT, "two different values share a 62-bit value key");
+        if (bits) return fail(SPARKALOG_E_DEVICE_FAULT, "device error bits " + std::to_string(bits));
+    }
+    const u64 m = mu + ms;
+    if (c->size + m > kMaxRelationRows) return fail(SPARKALOG_E_TOO_MANY_ROWS, "more than 2^32 - 1 values");
+
+    if (m) {
+        // New values of both sorts, numbered together by first position.
+        SPK_CUDA(c->joint.ensure(m * 8, s), "cudaMallocAsync");
+        SPK_CUDA(c->joint_b.ensure(m * 8, s), "cudaMallocAsync");
+        spk::joint_entries_kernel<<<simple_grid(m), 256, 0, s>>>(c->list_a.as<u64>(), mu, c->list_b.as<u64>(), ms,
+                                                                 c->joint.as<u64>());
+        SPK_CUDA(cudaGetLastError(), "joint_entries_kernel");
+        DevArray* jsorted = nullptr;
+        int rc = catalog_sort(c, c->joint, c->joint_b, m, err, &jsorted);
+        if (rc) return rc;
+        if (!c->kinds.ptr || c->kinds.bytes < (c->size + m) * 4) {
+            const bool fresh = !c->kinds.ptr;
+            SPK_CUDA(c->kinds.ensure((c->size + m) * 4, s, c->size * 4), "cudaMallocAsync");
+            if (fresh && c->size) SPK_CUDA(cudaMemsetAsync(c->kinds.ptr, 0, c->size * 4, s), "cudaMemsetAsync");
+        }
+        SPK_CUDA(c->dict.ensure((c->size + m) * 4, s, c->size * 4), "cudaMallocAsync");
+        SPK_CUDA(c->list_a.ensure(std::max<u64>(mu, 1) * 8, s), "cudaMallocAsync");  // new U32 pairs (in place)
+        SPK_CUDA(c->str_offset.ensure((c->str_count + ms + 1) * 8, s, c->str_count * 8), "cudaMallocAsync");
+        SPK_CUDA(c->str_length.ensure((c->str_count + ms + 1) * 4, s, c->str_count * 4), "cudaMallocAsync");
+        SPK_CUDA(c->str_src.ensure((ms + 1) * 4, s), "cudaMallocAsync");
+        // New strings are distinct spans of this text, so they fit in its size.
+        SPK_CUDA(c->arena.ensure(c->arena_used + text_bytes + 16, s, c->arena_used), "cudaMallocAsync");
+        c->host[0] = c->arena_used;
+        SPK_CUDA(cudaMemcpyAsync(counts + 3, c->host, 8, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
+        SPK_CUDA(cudaMemsetAsync(counts, 0, 16, s), "cudaMemsetAsync");
+        spk::assign_joint_ids_kernel<<<simple_grid(m), 256, 0, s>>>(
+            jsorted->as<u64>(), m, c->size, c->str_count, c->dict.as<u32>(), c->kinds.as<u32>(), c->list_a.as<u64>(),
+            counts, c->g_id.as<u32>(), c->g_si.as<u32>(), c->g_head.as<u32>(), tokens, c->str_offset.as<u64>(),
+            c->str_length.as<u32>(), counts + 3, c->str_src.as<u32>(), counts + 1);
+        SPK_CUDA(cudaGetLastError(), "assign_joint_ids_kernel");
+        if (ms) {
+            spk::copy_strings_kernel<<<simple_grid(ms * 32), 256, 0, s>>>(c->str_src.as<u32>(), ms, c->str_count,
+                                                                          tokens, text, c->str_offset.as<u64>(),
+                                                                          c->arena.as<unsigned char>());
+            SPK_CUDA(cudaGetLastError(), "copy_strings_kernel");
+            // The new keys (group order is key order) into the catalog's index.
+            for (DevArray* d : {&c->nk}) SPK_CUDA(d->ensure(ms * 8, s), "cudaMallocAsync");
+            for (DevArray* d : {&c->nid, &c->nsi}) SPK_CUDA(d->ensure(ms * 4, s), "cudaMallocAsync");
+            SPK_CUDA(cudaMemsetAsync(counts + 2, 0, 8, s), "cudaMemsetAsync");
+            spk::new_string_keys_kernel<<<simple_grid(ns), 256, 0, s>>>(
+                c->v_sorted.as<u64>(), ns, c->g_id.as<u32>(), c->g_si.as<u32>(), c->g_new.as<u32>(), c->nk.as<u64>(),
+                c->nid.as<u32>(), c->nsi.as<u32>(), counts + 2);
+            SPK_CUDA(cudaGetLastError(), "new_string_keys_kernel");
+            // Atomic order: sort the new keys, then fetch each one's payload
+            // back through its group (the keys are distinct).
+            DevArray* nsorted = nullptr;
+            SPK_CUDA(c->b.ensure(ms * 8, s), "cudaMallocAsync");
+            rc = catalog_sort(c, c->nk, c->b, ms, err, &nsorted);
+            if (rc) return rc;
+            DevArray& other = nsorted == &c->nk ? c->b : c->nk;
+            SPK_CUDA(other.ensure(ms * 8, s), "cudaMallocAsync");
+            spk::keyed_payload_kernel<<<simple_grid(ms), 256, 0, s>>>(nsorted->as<u64>(), ms, c->v_sorted.as<u64>(),
+                                                                      ns, c->g_id.as<u32>(), c->g_si.as<u32>(),
+                                                                      c->nid.as<u32>(), c->nsi.as<u32>());
+            SPK_CUDA(cudaGetLastError(), "keyed_payload_kernel");
+            const u64 total = c->str_count + ms;
+            SPK_CUDA(c->skeys_spare.ensure(total * 8, s), "cudaMallocAsync");
+            SPK_CUDA(c->sids_spare.ensure(total * 4, s), "cudaMallocAsync");
+            SPK_CUDA(c->sidx_spare.ensure(total * 4, s), "cudaMallocAsync");
+            spk::merge_keyed_kernel<<<simple_grid(total), 256, 0, s>>>(
+                c->skeys.as<u64>(), c->sids.as<u32>(), c->sidx.as<u32>(), c->str_count, nsorted->as<u64>(),
+                c->nid.as<u32>(), c->nsi.as<u32>(), ms, c->skeys_spare.as<u64>(), c->sids_spare.as<u32>(),
+                c->sidx_spare.as<u32>());
+            SPK_CUDA(cudaGetLastError(), "merge_keyed_kernel");
+            swap_arrays(c->skeys, c->skeys_spare);
+            swap_arrays(c->sids, c->sids_spare);
+            swap_arrays(c->sidx, c->sidx_spare);
+            SPK_CUDA(cudaMemcpyAsync(c->host, counts + 3, 8, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+            SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+            c->arena_used = c->host[0];
+        }
+        if (mu) {
+            // The new U32 values into the U32 index.
+            DevArray* pairs_sorted = nullptr;
+            SPK_CUDA(c->list_b.ensure(mu * 8, s), "cudaMallocAsync");
+            rc = catalog_sort(c, c->list_a, c->list_b, mu, err, &pairs_sorted);
+            if (rc) return rc;
+            SPK_CUDA(c->keys_spare.ensure((c->u32_count + mu) * 8, s), "cudaMallocAsync");
+            SPK_CUDA(launch_merge(c->keys.as<u64>(), c->u32_count, pairs_sorted->as<u64>(), mu,
+                                  c->keys_spare.as<u64>(), c->splits, s, 11, err),
+                     "merge_bulk_kernel");
+            swap_arrays(c->keys, c->keys_spare);
+        }
+        c->size += m;
+        c->u32_count += mu;
+        c->str_count += ms;
+    }
+    // Every token's id.
+    if (nu) {
+        spk::lookup_ids_kernel<8><<<simple_grid((nu + 7) / 8), 256, 0, s>>>(usorted->as<u64>(), nu,
+                                                                           c->keys.as<u64>(), c->u32_count, ids, err);
+        SPK_CUDA(cudaGetLastError(), "lookup_ids_kernel");
+    }
+    if (ns) {
+        spk::string_ids_kernel<<<simple_grid(ns), 256, 0, s>>>(psorted->as<u64>(), ns, c->g_id.as<u32>(), ids);
+        SPK_CUDA(cudaGetLastError(), "string_ids_kernel");
+    }
+    SPK_CUDA(cudaMemcpyAsync(c->host + 1, err, 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+    SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    const u32 bits = static_cast<u32>(c->host[1] & 0xffffffffu);
+    if (bits) return fail(SPARKALOG_E_DEVICE_FAULT, "device error bits " + std::to_string(bits));
     return 0;
 }
 
@@ -1511,7 +1716,11 @@ void sparkalog_catalog_destroy(sparkalog_catalog* c) {
     if (!c) return;
     cudaStream_t s = c->stream;
     for (DevArray* d : {&c->keys, &c->keys_spare, &c->dict, &c->a, &c->b, &c->list_a, &c->list_b, &c->staging,
-                        &c->ids, &c->words, &c->splits, &c->ex.index_sort.plan, &c->ex.index_sort.status})
+                        &c->ids, &c->words, &c->splits, &c->ex.index_sort.plan, &c->ex.index_sort.status, &c->kinds,
+                        &c->arena, &c->str_offset, &c->str_length, &c->skeys, &c->sids, &c->sidx, &c->skeys_spare,
+                        &c->sids_spare, &c->sidx_spare, &c->tokens, &c->v_keys, &c->v_pos, &c->v_sorted, &c->v_pairs,
+                        &c->v_pairs_b, &c->g_head, &c->g_id, &c->g_si, &c->g_new, &c->joint, &c->joint_b, &c->str_src,
+                        &c->nk, &c->nid, &c->nsi})
         d->release(s);
     cudaStreamSynchronize(s);
     pinned_put(c->host, 64);
@@ -1549,8 +1758,8 @@ int sparkalog_catalog_intern_u32(sparkalog_catalog* c, const u32* values, size_t
         // Values the catalog lacks, with their first positions.
         SPK_CUDA(c->list_a.ensure(n * 8, s), "cudaMallocAsync");
         SPK_CUDA(c->list_b.ensure(n * 8, s), "cudaMallocAsync");
-        spk::new_value_heads_kernel<<<simple_grid(n), 256, 0, s>>>(sorted->as<u64>(), n, c->keys.as<u64>(), c->size,
-                                                                   c->list_a.as<u64>(), new_count);
+        spk::new_value_heads_kernel<<<simple_grid(n), 256, 0, s>>>(sorted->as<u64>(), n, c->keys.as<u64>(),
+                                                                   c->u32_count, c->list_a.as<u64>(), new_count);
         SPK_CUDA(cudaGetLastError(), "new_value_heads_kernel");
         SPK_CUDA(cudaMemcpyAsync(c->host, new_count, 8, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
         SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
@@ -1562,6 +1771,10 @@ int sparkalog_catalog_intern_u32(sparkalog_catalog* c, const u32* values, size_t
             if (rc) return rc;
             DevArray& pairs = by_position == &c->list_a ? c->list_b : c->list_a;
             SPK_CUDA(c->dict.ensure((c->size + m) * 4, s, c->size * 4), "cudaMallocAsync");
+            if (c->kinds.ptr) {
+                SPK_CUDA(c->kinds.ensure((c->size + m) * 4, s, c->size * 4), "cudaMallocAsync");
+                SPK_CUDA(cudaMemsetAsync(c->kinds.as<u32>() + c->size, 0, m * 4, s), "cudaMemsetAsync");
+            }
             spk::assign_new_ids_kernel<<<simple_grid(m), 256, 0, s>>>(by_position->as<u64>(), m, c->size,
                                                                       pairs.as<u64>(), c->dict.as<u32>());
             SPK_CUDA(cudaGetLastError(), "assign_new_ids_kernel");
@@ -1569,12 +1782,13 @@ int sparkalog_catalog_intern_u32(sparkalog_catalog* c, const u32* values, size_t
             DevArray* sorted_pairs = nullptr;
             rc = catalog_sort(c, pairs, other, m, err, &sorted_pairs);
             if (rc) return rc;
-            SPK_CUDA(c->keys_spare.ensure((c->size + m) * 8, s), "cudaMallocAsync");
-            SPK_CUDA(launch_merge(c->keys.as<u64>(), c->size, sorted_pairs->as<u64>(), m, c->keys_spare.as<u64>(),
-                                  c->splits, s, 11, err),
+            SPK_CUDA(c->keys_spare.ensure((c->u32_count + m) * 8, s), "cudaMallocAsync");
+            SPK_CUDA(launch_merge(c->keys.as<u64>(), c->u32_count, sorted_pairs->as<u64>(), m,
+                                  c->keys_spare.as<u64>(), c->splits, s, 11, err),
                      "merge_bulk_kernel");
             swap_arrays(c->keys, c->keys_spare);
             c->size += m;
+            c->u32_count += m;
         }
         u32* dids = ids;
         if (location == SPARKALOG_HOST) {
@@ -1582,7 +1796,7 @@ int sparkalog_catalog_intern_u32(sparkalog_catalog* c, const u32* values, size_t
             dids = c->ids.as<u32>();
         }
         spk::lookup_ids_kernel<8><<<simple_grid((n + 7) / 8), 256, 0, s>>>(sorted->as<u64>(), n, c->keys.as<u64>(),
-                                                                          c->size, dids, err);
+                                                                          c->u32_count, dids, err);
         SPK_CUDA(cudaGetLastError(), "lookup_ids_kernel");
         if (location == SPARKALOG_HOST)
             SPK_CUDA(cudaMemcpyAsync(ids, dids, n * 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
@@ -1610,7 +1824,9 @@ int sparkalog_catalog_decode_u32(sparkalog_catalog* c, const u32* ids, size_t n,
         dids = c->staging.as<u32>();
         dvalues = c->ids.as<u32>();
     }
-    spk::decode_ids_kernel<<<simple_grid(n), 256, 0, s>>>(dids, n, c->dict.as<u32>(), c->size, dvalues, err);
+    spk::decode_ids_kernel<<<simple_grid(n), 256, 0, s>>>(dids, n, c->dict.as<u32>(),
+                                                          c->kinds.ptr ? c->kinds.as<u32>() : nullptr, c->size,
+                                                          dvalues, err);
     SPK_CUDA(cudaGetLastError(), "decode_ids_kernel");
     if (location == SPARKALOG_HOST)
         SPK_CUDA(cudaMemcpyAsync(values, dvalues, n * 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
@@ -2034,6 +2250,170 @@ int load_text_u32(sparkalog_store* st, u32 id, const char* text, size_t bytes, i
 }
 
 }  // namespace
+
+int sparkalog_store_load_delimited_values(sparkalog_store* st, sparkalog_catalog* c, u32 id, const char* text,
+                                          size_t bytes, int location, unsigned char delimiter, int has_header,
+                                          int recursive, size_t* rows, sparkalog_load_error* error) {
+    if (!st || !c || !rows || (bytes && !text)) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null argument");
+    // parse_delimited_parallel refuses whitespace delimiters other than tab (ingest.rs:24-30).
+    if (delimiter == ' ' || delimiter == '\n' || delimiter == '\f' || delimiter == '\r')
+        return fail(SPARKALOG_E_INVALID_ARGUMENT, "delimiter must be a visible ASCII byte or tab");
+    if (st->find(id)) return fail(SPARKALOG_E_DUPLICATE, "relation " + std::to_string(id) + " is already registered");
+    if (error) *error = sparkalog_load_error{};
+    *rows = 0;
+    cudaStream_t s = st->stream;
+    StoreOps* ops_ptr = store_ops(st);
+    if (!ops_ptr) return static_cast<int>(cudaErrorMemoryAllocation);
+    StoreOps& ops = *ops_ptr;
+    u32* err = ops.counters.as<u32>() + 32;
+    const unsigned char* dtext = reinterpret_cast<const unsigned char*>(text);
+    if (location == SPARKALOG_HOST && bytes) {
+        SPK_CUDA(c->staging.ensure(bytes + 16, s), "cudaMallocAsync");
+        SPK_CUDA(cudaMemcpyAsync(c->staging.ptr, text, bytes, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
+        dtext = c->staging.as<unsigned char>();
+    }
+    unsigned long long* dcount = reinterpret_cast<unsigned long long*>(ops.counts.as<u64>());
+    SPK_CUDA(cudaMemsetAsync(ops.counts.ptr, 0, 64, s), "cudaMemsetAsync");
+    if (bytes) {
+        spk::count_newlines_kernel<<<simple_grid(bytes), 256, 0, s>>>(dtext, bytes, dcount);
+        SPK_CUDA(cudaGetLastError(), "count_newlines_kernel");
+    }
+    SPK_CUDA(cudaMemcpyAsync(ops.host, dcount, 8, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+    SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    const u64 newlines = ops.host[0];
+    unsigned char last = 0;
+    if (bytes) {
+        SPK_CUDA(cudaMemcpyAsync(&last, dtext + bytes - 1, 1, cudaMemcpyDefault, s), "cudaMemcpyAsync");
+        SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    }
+    const u64 lines = newlines + ((bytes && last != '\n') ? 1 : 0);
+    constexpr int kByteItems = 16, kLineItems = 8;
+    const u64 byte_tiles = (bytes + kThreads * kByteItems - 1) / (kThreads * kByteItems);
+    const u64 line_tiles = (lines + kThreads * kLineItems - 1) / (kThreads * kLineItems);
+    SPK_CUDA(ops.a.ensure(std::max<u64>(newlines, 1) * 8, s), "cudaMallocAsync");
+    SPK_CUDA(ops.status.ensure_zeroed((std::max(byte_tiles, line_tiles) + 1) * 8, s), "cudaMallocAsync");
+    SPK_CUDA(c->tokens.ensure(std::max<u64>(lines, 1) * 16, s), "cudaMallocAsync");
+    SPK_CUDA(cudaMemsetAsync(ops.counters.ptr, 0, 33 * 4, s), "cudaMemsetAsync");
+    SPK_CUDA(cudaMemsetAsync(ops.counts.as<u64>() + 2, 0xff, 24, s), "cudaMemsetAsync");
+    u64* ends_n = ops.counts.as<u64>() + 1;
+    unsigned long long* first_error = reinterpret_cast<unsigned long long*>(ops.counts.as<u64>() + 2);
+    u64* out_n = ops.counts.as<u64>() + 5;
+    {
+        auto kernel = spk::line_ends_kernel<kThreads, kByteItems>;
+        kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, std::max<u64>(byte_tiles, 1)), kThreads, 0,
+                 s>>>(dtext, bytes, ops.a.as<u64>(), ends_n, ops.status.as<u64>(), ops.counters.as<u32>(),
+                      ops.ex.epoch++, err);
+        SPK_CUDA(cudaGetLastError(), "line_ends_kernel");
+        auto parse = spk::parse_value_lines_kernel<kThreads, kLineItems>;
+        parse<<<grid_for(reinterpret_cast<const void*>(parse), kThreads, std::max<u64>(line_tiles, 1)), kThreads, 0,
+                s>>>(dtext, bytes, ops.a.as<u64>(), ends_n, lines, delimiter, has_header != 0, c->tokens.as<u64>(),
+                     out_n, first_error, ops.status.as<u64>(), ops.counters.as<u32>() + 1, ops.ex.epoch++, err);
+        SPK_CUDA(cudaGetLastError(), "parse_value_lines_kernel");
+    }
+    SPK_CUDA(cudaMemcpyAsync(ops.host, ops.counts.as<u64>() + 2, 32, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+    SPK_CUDA(cudaMemcpyAsync(ops.host + 4, err, 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+    SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    const u64 syntax_line = ops.host[0], arity_line = ops.host[1], long_line = ops.host[2], parsed = ops.host[3];
+    const u32 bits = static_cast<u32>(ops.host[4] & 0xffffffffu);
+    if (bits) return fail(SPARKALOG_E_DEVICE_FAULT, "device error bits " + std::to_string(bits));
+    if (syntax_line != spk::kNoLine || arity_line != spk::kNoLine) {
+        // A syntax error anywhere comes first (parse_delimited_parallel fails
+        // before any row is inserted); then the first row that does not hold
+        // two values (Database::insert's arity check).
+        const u64 index = syntax_line != spk::kNoLine ? syntax_line : arity_line;
+        u64 bounds[2] = {0, bytes};
+        if (index > 0)
+            SPK_CUDA(cudaMemcpyAsync(&bounds[0], ops.a.as<u64>() + index - 1, 8, cudaMemcpyDeviceToHost, s),
+                     "cudaMemcpyAsync");
+        if (index < newlines)
+            SPK_CUDA(cudaMemcpyAsync(&bounds[1], ops.a.as<u64>() + index, 8, cudaMemcpyDeviceToHost, s),
+                     "cudaMemcpyAsync");
+        SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+        if (index > 0) bounds[0] += 1;
+        std::vector<unsigned char> line(bounds[1] - bounds[0]);
+        if (!line.empty())
+            SPK_CUDA(cudaMemcpy(line.data(), dtext + bounds[0], line.size(), cudaMemcpyDefault), "cudaMemcpy");
+        if (index < newlines && !line.empty() && line.back() == '\r') line.pop_back();
+        sparkalog_load_error e{};
+        e.line = index + 1;
+        describe_delimited_error(line.data(), bounds[0], line.size(), delimiter, &e);
+        if (e.kind == SPARKALOG_LOAD_NOT_U32) e.kind = SPARKALOG_LOAD_ARITY;  // any value kind is taken here
+        if (error) *error = e;
+        return fail(SPARKALOG_E_LOAD, "line " + std::to_string(e.line) + ", column " + std::to_string(e.column) +
+                                          ": " + delimited_message(e.kind));
+    }
+    if (long_line != spk::kNoLine)
+        return fail(SPARKALOG_E_INVALID_ARGUMENT, "line " + std::to_string(long_line + 1) +
+                                                      " holds a value longer than 16 MiB - 1 bytes");
+    if (parsed > kMaxRelationRows) return fail(SPARKALOG_E_TOO_MANY_ROWS, "too many rows for u32 row ids");
+    // The catalog works on its own stream: wait for the parse first.
+    if (c->stream != s) SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    SPK_CUDA(c->ids.ensure(std::max<u64>(parsed, 1) * 8, c->stream), "cudaMallocAsync");
+    int rc = catalog_intern_tokens(c, c->tokens.as<u64>(), parsed * 2, dtext, bytes, c->ids.as<u32>());
+    if (rc) return rc;
+    SPK_CUDA(st->scratch_u32[0].ensure(std::max<u64>(parsed, 1) * 4, c->stream), "cudaMallocAsync");
+    SPK_CUDA(st->scratch_u32[1].ensure(std::max<u64>(parsed, 1) * 4, c->stream), "cudaMallocAsync");
+    if (parsed) {
+        spk::split_rows_kernel<<<simple_grid(parsed), 256, 0, c->stream>>>(
+            c->ids.as<u32>(), parsed, st->scratch_u32[0].as<u32>(), st->scratch_u32[1].as<u32>());
+        SPK_CUDA(cudaGetLastError(), "split_rows_kernel");
+    }
+    if (c->stream != s) SPK_CUDA(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+    *rows = parsed;
+    const u32* c0 = st->scratch_u32[0].as<u32>();
+    const u32* c1 = st->scratch_u32[1].as<u32>();
+    return recursive ? sparkalog_store_insert_recursive(st, id, c0, c1, parsed, c0, c1, parsed, SPARKALOG_DEVICE)
+                     : sparkalog_store_insert_static(st, id, c0, c1, parsed, SPARKALOG_DEVICE);
+}
+
+int sparkalog_catalog_export(sparkalog_catalog* c, uint32_t* kinds, uint32_t* numbers, uint64_t* offsets,
+                             unsigned char* bytes, size_t bytes_capacity, size_t* bytes_used) {
+    if (!c || !bytes_used) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null argument");
+    cudaStream_t s = c->stream;
+    const u64 n = c->size;
+    std::vector<u32> dict(n), kind(n, 0);
+    std::vector<u64> soff(c->str_count);
+    std::vector<u32> slen(c->str_count);
+    std::vector<unsigned char> arena(c->arena_used);
+    if (n) SPK_CUDA(cudaMemcpyAsync(dict.data(), c->dict.ptr, n * 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+    if (n && c->kinds.ptr)
+        SPK_CUDA(cudaMemcpyAsync(kind.data(), c->kinds.ptr, n * 4, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+    if (c->str_count) {
+        SPK_CUDA(cudaMemcpyAsync(soff.data(), c->str_offset.ptr, c->str_count * 8, cudaMemcpyDeviceToHost, s),
+                 "cudaMemcpyAsync");
+        SPK_CUDA(cudaMemcpyAsync(slen.data(), c->str_length.ptr, c->str_count * 4, cudaMemcpyDeviceToHost, s),
+                 "cudaMemcpyAsync");
+    }
+    if (c->arena_used)
+        SPK_CUDA(cudaMemcpyAsync(arena.data(), c->arena.ptr, c->arena_used, cudaMemcpyDeviceToHost, s),
+                 "cudaMemcpyAsync");
+    SPK_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    // A String's raw span is its quoted text: drop the quotes and undo the
+    // doubled quotes (parse_record, ingest.rs:43-120); a Symbol is its span.
+    size_t used = 0;
+    for (u64 i = 0; i < n; ++i) {
+        if (kinds) kinds[i] = kind[i];
+        if (numbers) numbers[i] = kind[i] == 0 ? dict[i] : 0;
+        if (offsets) offsets[i] = used;
+        if (kind[i] == 0) continue;
+        const unsigned char* raw = arena.data() + soff[dict[i]];
+        const u32 len = slen[dict[i]];
+        u32 b = 0, e = len;
+        if (kind[i] == 1 && len >= 2) {
+            b = 1;
+            e = len - 1;
+        }
+        for (u32 k = b; k < e; ++k) {
+            if (kind[i] == 1 && raw[k] == '"' && k + 1 < e && raw[k + 1] == '"') ++k;
+            if (bytes && used < bytes_capacity) bytes[used] = raw[k];
+            ++used;
+        }
+    }
+    if (offsets) offsets[n] = used;
+    *bytes_used = used;
+    if (bytes && used > bytes_capacity) return fail(SPARKALOG_E_INVALID_ARGUMENT, "byte buffer too small");
+    return 0;
+}
 
 int sparkalog_store_rows(sparkalog_store* st, u32 id, int version, size_t* rows) {
     if (!st || !rows) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null argument");

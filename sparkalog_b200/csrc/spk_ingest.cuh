@@ -241,7 +241,142 @@ struct DelimitedLineParser {
     }
 };
 
+// ---------------------------------------------------------------------------
+// Records of mixed values (InternedValue, crates/sparkalog-datalog/src/
+// catalog.rs:10-14: U32, String, Symbol), as parse_record (ingest.rs:43-120)
+// yields them. A value is one 64-bit token: bits 63-62 the kind (0 U32, 1
+// String, 2 Symbol); a U32 keeps its value in the low 32 bits; a String or
+// Symbol keeps the byte offset (bits 61-24) and length (bits 23-0) of its
+// raw text: a String's quoted span including its quotes (the only escape is a
+// doubled quote, so equal raw spans are exactly equal strings), a Symbol's
+// trimmed span.
+// ---------------------------------------------------------------------------
+constexpr u64 kTokenMaxLength = (1ull << 24) - 1;
+constexpr u64 kTokenMaxOffset = (1ull << 38) - 1;
+
+__device__ __forceinline__ u64 make_token(u32 kind, u64 offset, u64 length) {
+    return (static_cast<u64>(kind) << 62) | (offset << 24) | length;
+}
+__device__ __forceinline__ u32 token_kind(u64 t) { return static_cast<u32>(t >> 62); }
+__device__ __forceinline__ u64 token_offset(u64 t) { return (t >> 24) & kTokenMaxOffset; }
+__device__ __forceinline__ u32 token_length(u64 t) { return static_cast<u32>(t & kTokenMaxLength); }
+
+// 1: two values in *t0, *t1; 2: a syntax error; 3: not two values; 4: a
+// String or Symbol longer than kTokenMaxLength bytes.
+__device__ __forceinline__ int parse_value_record(const unsigned char* t, u64 b, u64 e, unsigned char delim, u64* t0,
+                                                  u64* t1) {
+    u64 pos = b;
+    int fields = 0;
+    bool too_long = false;
+    for (;;) {
+        u64 token = 0;
+        if (pos < e && t[pos] == '"') {
+            const u64 start = pos;
+            ++pos;
+            bool closed = false;
+            while (pos < e) {
+                if (t[pos] == '"') {
+                    if (pos + 1 < e && t[pos + 1] == '"') {
+                        pos += 2;
+                    } else {
+                        ++pos;
+                        closed = true;
+                        break;
+                    }
+                } else {
+                    ++pos;  // UTF-8 continuation bytes are never '"'
+                }
+            }
+            if (!closed) return 2;
+            if (pos < e && t[pos] != delim) return 2;
+            if (pos - start > kTokenMaxLength) too_long = true;
+            token = make_token(1, start, (pos - start) & kTokenMaxLength);
+        } else {
+            const u64 start = pos;
+            while (pos < e && t[pos] != delim) ++pos;
+            u64 fb = start, fe = pos;
+            unicode_trim(t, &fb, &fe);
+            if (fb == fe) return 2;
+            u32 v = 0;
+            if (parse_u32_field(t + fb, fe - fb, &v)) {
+                token = v;
+            } else {
+                if (fe - fb > kTokenMaxLength) too_long = true;
+                token = make_token(2, fb, (fe - fb) & kTokenMaxLength);
+            }
+        }
+        if (fields == 0) *t0 = token;
+        if (fields == 1) *t1 = token;
+        ++fields;
+        if (pos == e) break;
+        ++pos;
+        if (pos == e) return 2;
+    }
+    if (fields != 2) return 3;
+    return too_long ? 4 : 1;
+}
+
 // Line i spans [i == 0 ? 0 : ends[i - 1] + 1, i < ends_n ? ends[i] : bytes).
+// Every kept line leaves two tokens at out[2 row], out[2 row + 1] (rows in
+// line order); first_error[0] / [1] / [2] = smallest line with a syntax
+// error / not two values / a too-long value.
+template <int THREADS, int ITEMS>
+__global__ void __launch_bounds__(THREADS) parse_value_lines_kernel(const unsigned char* text, u64 bytes,
+                                                                    const u64* ends, const u64* ends_n_ptr, u64 lines,
+                                                                    unsigned char delim, bool header, u64* out,
+                                                                    u64* out_count, unsigned long long* first_error,
+                                                                    u64* status, u32* tile_counter, u32 epoch,
+                                                                    u32* err) {
+    constexpr int kTile = THREADS * ITEMS;
+    __shared__ CompactShared<THREADS> cs;
+    __shared__ u64 stage[2 * kTile];
+    const u64 ends_n = *ends_n_ptr;
+    const u64 num_tiles = (lines + kTile - 1) / kTile;
+    if (num_tiles == 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) *out_count = 0;
+        return;
+    }
+    for (;;) {
+        if (threadIdx.x == 0) cs.tile = atomicAdd(tile_counter, 1u);
+        __syncthreads();
+        const u64 tile = cs.tile;
+        if (tile >= num_tiles) break;
+        const u64 base = tile * kTile + static_cast<u64>(threadIdx.x) * ITEMS;
+        u32 keep = 0;
+        u64 a[ITEMS], c[ITEMS];
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i) {
+            a[i] = c[i] = 0;
+            const u64 line = base + i;
+            if (line >= lines) continue;
+            if (header && line == 0) continue;
+            const u64 b = line == 0 ? 0 : ends[line - 1] + 1;
+            u64 e = line < ends_n ? ends[line] : bytes;
+            if (line < ends_n && e > b && text[e - 1] == '\r') --e;
+            u64 tb = b, te = e;
+            unicode_trim(text, &tb, &te);
+            if (tb == te) continue;
+            const int kind = parse_value_record(text, b, e, delim, &a[i], &c[i]);
+            if (kind == 1) keep |= 1u << i;
+            else atomicMin(first_error + (kind == 2 ? 0 : (kind == 3 ? 1 : 2)), static_cast<unsigned long long>(line));
+        }
+        u32 excl, total;
+        const u64 off = compact_offsets<THREADS>(__popc(keep), &excl, &total, tile, status, epoch, err, cs);
+        u32 w = excl;
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i)
+            if (keep & (1u << i)) {
+                stage[2 * w] = a[i];
+                stage[2 * w + 1] = c[i];
+                ++w;
+            }
+        __syncthreads();
+        for (u32 j = threadIdx.x; j < 2 * total; j += THREADS) out[2 * off + j] = stage[j];
+        if (tile == num_tiles - 1 && threadIdx.x == 0) *out_count = off + total;
+        __syncthreads();
+    }
+}
+
 // first_error[0] = smallest line index whose parser returned 2,
 // first_error[1] = smallest line index whose parser returned 3.
 template <int THREADS, int ITEMS, class Parser>
@@ -373,17 +508,286 @@ __global__ void lookup_ids_kernel(const u64* sorted, u64 n, const u64* keys, u64
     }
 }
 
-// values[i] = dict[ids[i]]; an id outside the catalog sets kErrIndexRange.
-static __global__ void decode_ids_kernel(const u32* ids, u64 n, const u32* dict, u64 size, u32* values, u32* err) {
+// values[i] = dict[ids[i]]; an id outside the catalog, or one of a String
+// or Symbol value (kinds[id] != 0, when the catalog holds any), sets
+// kErrIndexRange.
+static __global__ void decode_ids_kernel(const u32* ids, u64 n, const u32* dict, const u32* kinds, u64 size,
+                                         u32* values, u32* err) {
     const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
     for (u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
         const u32 id = ids[i];
-        if (id < size) {
+        if (id < size && (!kinds || kinds[id] == 0)) {
             values[i] = dict[id];
         } else {
             values[i] = 0;
             atomicOr(err, kErrIndexRange);
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Interning of mixed values. U32 values take the path above. A String or
+// Symbol is keyed by (kind << 62 | a 62-bit hash of its raw bytes); values
+// with equal keys are grouped by sorting (group index << 32 | position), and
+// every value's bytes are compared with its group's first value and with the
+// catalog's stored value of that key, so a hash collision between different
+// values is detected (kErrHashCollision) instead of merging them. New values
+// of both sorts are then numbered together by first position.
+// ---------------------------------------------------------------------------
+constexpr u32 kErrHashCollision = 1u << 5;
+constexpr u32 kNewValue = 0xffffffffu;
+
+__device__ __forceinline__ u64 mix64(u64 x) {
+    // The splitmix64 finaliser (Steele, Lea, Flood 2014).
+    x ^= x >> 30;
+    x *= 0xBF58476D1CE4E5B9ull;
+    x ^= x >> 27;
+    x *= 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+__device__ __forceinline__ u64 value_key(const unsigned char* p, u32 len, u32 kind) {
+    u64 h = mix64(0x9E3779B97F4A7C15ull ^ (static_cast<u64>(kind) << 56) ^ len);
+    u32 i = 0;
+    for (; i + 8 <= len; i += 8) {
+        u64 w = 0;
+        for (int b = 0; b < 8; ++b) w |= static_cast<u64>(p[i + b]) << (8 * b);
+        h = mix64(h ^ w);
+    }
+    u64 w = 0;
+    for (u32 b = 0; i + b < len; ++b) w |= static_cast<u64>(p[i + b]) << (8 * b);
+    h = mix64(h ^ w ^ 0x5555555555555555ull);
+    return (static_cast<u64>(kind) << 62) | (h >> 2);
+}
+
+__device__ __forceinline__ bool same_bytes(const unsigned char* a, const unsigned char* b, u32 len) {
+    for (u32 i = 0; i < len; ++i)
+        if (a[i] != b[i]) return false;
+    return true;
+}
+
+// U32 tokens to ukeys (value << 32 | position), String/Symbol tokens to
+// (skeys, spos); each list compacted by an atomic counter (its order does
+// not matter: both are sorted next).
+static __global__ void classify_tokens_kernel(const u64* tokens, u64 n, const unsigned char* text, u64* ukeys,
+                                              unsigned long long* ucount, u64* skeys, u32* spos,
+                                              unsigned long long* scount) {
+    const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+    for (u64 p = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; p < n; p += stride) {
+        const u64 t = tokens[p];
+        const u32 kind = token_kind(t);
+        if (kind == 0) {
+            ukeys[atomicAdd(ucount, 1ull)] = (static_cast<u64>(static_cast<u32>(t)) << 32) | p;
+        } else {
+            const unsigned long long k = atomicAdd(scount, 1ull);
+            skeys[k] = value_key(text + token_offset(t), token_length(t), kind);
+            spos[k] = static_cast<u32>(p);
+        }
+    }
+}
+
+__device__ __forceinline__ u64 lower_bound_u64(const u64* a, u64 n, u64 key) {
+    u64 lo = 0, hi = n;
+    while (lo < hi) {
+        const u64 mid = (lo + hi) >> 1;
+        if (a[mid] < key) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// pairs[k] = (group << 32 | position), group = first index of the key in
+// the sorted keys (one per distinct key).
+static __global__ void group_pairs_kernel(const u64* skeys, const u32* spos, u64 ns, const u64* sorted_keys,
+                                          u64* pairs) {
+    const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+    for (u64 k = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; k < ns; k += stride)
+        pairs[k] = (lower_bound_u64(sorted_keys, ns, skeys[k]) << 32) | spos[k];
+}
+
+// The catalog's String/Symbol values: raw bytes in an arena, one
+// (offset, length) per string index, and the lookup index sorted by key
+// (keys, the value id, the string index).
+struct StringTable {
+    const unsigned char* arena;
+    const u64* offset;
+    const u32* length;
+    const u64* keys;
+    const u32* ids;
+    const u32* index;
+    u64 count;
+};
+
+// Group heads (the first position of each distinct key): head[g], the
+// catalog id of the value (or kNewValue, then (position << 32 | g) joins
+// the new list), with the bytes checked against the catalog's value.
+static __global__ void string_heads_kernel(const u64* sorted_pairs, u64 ns, const u64* sorted_keys, const u64* tokens,
+                                           const unsigned char* text, StringTable cat, u32* head, u32* id_of,
+                                           u32* is_new, u64* new_list, unsigned long long* new_count, u32* err) {
+    const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+    for (u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; i < ns; i += stride) {
+        const u32 g = static_cast<u32>(sorted_pairs[i] >> 32);
+        if (i > 0 && static_cast<u32>(sorted_pairs[i - 1] >> 32) == g) continue;
+        const u32 pos = static_cast<u32>(sorted_pairs[i]);
+        head[g] = pos;
+        const u64 key = sorted_keys[g];
+        const u64 c = lower_bound_u64(cat.keys, cat.count, key);
+        if (c < cat.count && cat.keys[c] == key) {
+            const u64 t = tokens[pos];
+            const u32 si = cat.index[c];
+            if (cat.length[si] != token_length(t) ||
+                !same_bytes(cat.arena + cat.offset[si], text + token_offset(t), token_length(t)))
+                atomicOr(err, kErrHashCollision);
+            id_of[g] = cat.ids[c];
+        } else {
+            id_of[g] = kNewValue;
+            is_new[g] = 1;
+            new_list[atomicAdd(new_count, 1ull)] = (static_cast<u64>(pos) << 32) | g;
+        }
+    }
+}
+
+// The joint list of new values: U32 heads (position << 32 | value) and
+// string heads (position << 32 | group) as (position << 33 | sort << 32 |
+// payload), which sorts by first position.
+static __global__ void joint_entries_kernel(const u64* ulist, u64 mu, const u64* slist, u64 ms, u64* out) {
+    const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+    for (u64 k = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; k < mu + ms; k += stride) {
+        const u64 e = k < mu ? ulist[k] : slist[k - mu];
+        const u64 pos = e >> 32;
+        out[k] = (pos << 33) | (static_cast<u64>(k < mu ? 0 : 1) << 32) | static_cast<u32>(e);
+    }
+}
+
+// ids[k], index[k] of each sorted new key, fetched through its group (the
+// first index of the key among the batch's sorted keys).
+static __global__ void keyed_payload_kernel(const u64* keys, u64 m, const u64* sorted_keys, u64 ns, const u32* id_of,
+                                            const u32* si_of, u32* ids, u32* index) {
+    const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+    for (u64 k = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; k < m; k += stride) {
+        const u64 g = lower_bound_u64(sorted_keys, ns, keys[k]);
+        ids[k] = id_of[g];
+        index[k] = si_of[g];
+    }
+}
+
+// Every grouped value has its head's bytes (else two different values share
+// a key).
+static __global__ void verify_groups_kernel(const u64* sorted_pairs, u64 ns, const u32* head, const u64* tokens,
+                                            const unsigned char* text, u32* err) {
+    const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+    for (u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; i < ns; i += stride) {
+        const u32 g = static_cast<u32>(sorted_pairs[i] >> 32);
+        const u32 pos = static_cast<u32>(sorted_pairs[i]);
+        const u32 h = head[g];
+        if (h == pos) continue;
+        const u64 a = tokens[pos], b = tokens[h];
+        if (token_length(a) != token_length(b) ||
+            !same_bytes(text + token_offset(a), text + token_offset(b), token_length(a)))
+            atomicOr(err, kErrHashCollision);
+    }
+}
+
+// New values of both sorts in first-position order: entry (position << 33 |
+// sort << 32 | payload), payload the U32 value (sort 0) or the group (sort
+// 1). Rank r gets id base + r. A U32 joins (value << 32 | id) for the U32
+// index; a string gets string index str_base + (its rank among strings,
+// counted by atomics) and its raw bytes are reserved in the arena.
+static __global__ void assign_joint_ids_kernel(const u64* sorted, u64 m, u64 base, u64 str_base, u32* dict,
+                                               u32* kinds, u64* upairs, unsigned long long* ucount, u32* id_of,
+                                               u32* si_of, const u32* head, const u64* tokens, u64* str_offset,
+                                               u32* str_length, unsigned long long* arena_used, u32* str_src,
+                                               unsigned long long* scount) {
+    const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+    for (u64 r = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; r < m; r += stride) {
+        const u64 e = sorted[r];
+        const u32 payload = static_cast<u32>(e);
+        const u32 id = static_cast<u32>(base + r);
+        if (((e >> 32) & 1u) == 0) {
+            upairs[atomicAdd(ucount, 1ull)] = (static_cast<u64>(payload) << 32) | id;
+            dict[id] = payload;
+            kinds[id] = 0;
+        } else {
+            const u32 g = payload;
+            const u64 t = tokens[head[g]];
+            const u64 si = str_base + atomicAdd(scount, 1ull);
+            id_of[g] = id;
+            si_of[g] = static_cast<u32>(si);
+            dict[id] = static_cast<u32>(si);
+            kinds[id] = token_kind(t);
+            str_length[si] = token_length(t);
+            str_offset[si] = atomicAdd(arena_used, static_cast<unsigned long long>(token_length(t)));
+            str_src[si - str_base] = head[g];
+        }
+    }
+}
+
+// One warp per new string: its raw bytes from the text into the arena.
+static __global__ void copy_strings_kernel(const u32* str_src, u64 count, u64 str_base, const u64* tokens,
+                                           const unsigned char* text, const u64* str_offset, unsigned char* arena) {
+    const u64 warps = static_cast<u64>(gridDim.x) * (blockDim.x / kWarp);
+    for (u64 k = (static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x) / kWarp; k < count; k += warps) {
+        const u64 t = tokens[str_src[k]];
+        const unsigned char* src = text + token_offset(t);
+        unsigned char* dst = arena + str_offset[str_base + k];
+        for (u32 b = lane_id(); b < token_length(t); b += kWarp) dst[b] = src[b];
+    }
+}
+
+// The new strings' keys (in group order, which is key order) for the
+// catalog's index, with their ids and string indices.
+static __global__ void new_string_keys_kernel(const u64* sorted_keys, u64 ns, const u32* id_of, const u32* si_of,
+                                              const u32* group_is_new, u64* keys, u32* ids, u32* index,
+                                              unsigned long long* count) {
+    const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+    for (u64 g = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; g < ns; g += stride) {
+        if (!group_is_new[g]) continue;
+        const unsigned long long k = atomicAdd(count, 1ull);
+        keys[k] = sorted_keys[g];
+        ids[k] = id_of[g];
+        index[k] = si_of[g];
+    }
+}
+
+// Merge of two key-sorted (key, id, index) lists with distinct keys: each
+// element's output position is its own index plus its rank in the other list.
+static __global__ void merge_keyed_kernel(const u64* ak, const u32* ai, const u32* ax, u64 na, const u64* bk,
+                                          const u32* bi, const u32* bx, u64 nb, u64* ok, u32* oi, u32* ox) {
+    const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+    for (u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; i < na + nb; i += stride) {
+        u64 key, o;
+        u32 id, x;
+        if (i < na) {
+            key = ak[i];
+            id = ai[i];
+            x = ax[i];
+            o = i + lower_bound_u64(bk, nb, key);
+        } else {
+            const u64 j = i - na;
+            key = bk[j];
+            id = bi[j];
+            x = bx[j];
+            o = j + lower_bound_u64(ak, na, key);
+        }
+        ok[o] = key;
+        oi[o] = id;
+        ox[o] = x;
+    }
+}
+
+// ids[position] of every String/Symbol value from its group.
+static __global__ void string_ids_kernel(const u64* sorted_pairs, u64 ns, const u32* id_of, u32* ids) {
+    const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+    for (u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; i < ns; i += stride)
+        ids[static_cast<u32>(sorted_pairs[i])] = id_of[static_cast<u32>(sorted_pairs[i] >> 32)];
+}
+
+// Row r of the relation: (ids[2r], ids[2r + 1]).
+static __global__ void split_rows_kernel(const u32* ids, u64 rows, u32* c0, u32* c1) {
+    const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+    for (u64 r = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; r < rows; r += stride) {
+        c0[r] = ids[2 * r];
+        c1[r] = ids[2 * r + 1];
     }
 }
 

@@ -165,6 +165,34 @@ class ValueCatalog:
         return self._call(lambda p, n, loc, o: self._check(L.sparkalog_catalog_decode_u32(self._h, p, n, loc, o)),
                           ids)
 
+    @property
+    def handle(self):
+        return self._h
+
+    def values(self) -> list[tuple]:
+        """Every interned value in id order, as ("u32", n), ("string", s) or
+        ("symbol", s) (InternedValue, catalog.rs:10-14), read from the device."""
+        ctypes, L = self._ctypes, self._native.load()
+        n = len(self)
+        used = ctypes.c_size_t(0)
+        self._check(L.sparkalog_catalog_export(self._h, None, None, None, None, 0, ctypes.byref(used)))
+        kinds = np.zeros(max(n, 1), dtype=np.uint32)
+        numbers = np.zeros(max(n, 1), dtype=np.uint32)
+        offsets = np.zeros(n + 1, dtype=np.uint64)
+        raw = np.zeros(max(used.value, 1), dtype=np.uint8)
+        self._check(L.sparkalog_catalog_export(self._h, kinds.ctypes.data_as(self._native.c_u32p),
+                                               numbers.ctypes.data_as(self._native.c_u32p),
+                                               offsets.ctypes.data_as(self._native.c_u64p), raw.ctypes.data,
+                                               len(raw), ctypes.byref(used)))
+        out = []
+        for i in range(n):
+            if kinds[i] == 0:
+                out.append(("u32", int(numbers[i])))
+            else:
+                text = bytes(raw[int(offsets[i]):int(offsets[i + 1])]).decode()
+                out.append(("string" if kinds[i] == 1 else "symbol", text))
+        return out
+
     def __len__(self) -> int:
         size = self._ctypes.c_size_t(0)
         self._check(self._native.load().sparkalog_catalog_size(self._h, self._ctypes.byref(size)))

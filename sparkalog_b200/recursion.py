@@ -259,6 +259,34 @@ class RelationStore:
         _check(code)
         return int(rows.value)
 
+    def load_delimited(self, rid: RelationId | int, text, catalog, delimiter: str = ",", has_header: bool = False,
+                       recursive: bool = False) -> int:
+        """Database::load_delimited (database.rs:165-177) for a binary relation of any
+        values (U32, String, Symbol), parsed and interned into ``catalog`` (a
+        datalog.ValueCatalog) on the GPU; the relation holds value ids. Returns the
+        number of rows read; errors raise LoadError as load_delimited_u32."""
+        L = _native.load()
+        if isinstance(text, str):
+            text = text.encode()
+        if isinstance(text, torch.Tensor):
+            ptr, nbytes, loc = text.data_ptr(), int(text.numel()), DEVICE
+        else:
+            host = text if isinstance(text, np.ndarray) else np.frombuffer(text, dtype=np.uint8)
+            host = np.ascontiguousarray(host.view(np.uint8).reshape(-1))
+            ptr, nbytes, loc = host.ctypes.data if len(host) else None, len(host), HOST
+        d = delimiter.encode()
+        if len(d) != 1:
+            raise ValueError("the delimiter is one byte")
+        rows = ctypes.c_size_t(0)
+        err = _native.LoadErrorC()
+        code = L.sparkalog_store_load_delimited_values(self._h, catalog.handle, int(getattr(rid, "value", rid)), ptr,
+                                                       nbytes, loc, d[0], 1 if has_header else 0,
+                                                       1 if recursive else 0, ctypes.byref(rows), ctypes.byref(err))
+        if code == -23:
+            raise LoadError(code, _native.last_error(), err.kind, int(err.line), int(err.column), None)
+        _check(code)
+        return int(rows.value)
+
     def append(self, rid: RelationId | int, relation) -> None:
         """FULL u= rows (and DELTA u= the genuinely new rows of a recursive relation),
         so a resident fixpoint continues from them."""
