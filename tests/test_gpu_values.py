@@ -101,7 +101,7 @@ def test_errors(cuda):
 
     with pytest.raises(LoadError) as e:
         load('1,2\n"a",b,c\n')
-    assert e.value.kind == 8 and e.value.line == 2  # SPARKALOG_LOAD_ARITY
+    assert e.value.kind == "Arity" and e.value.line == 2
     for text in ['1,"open\n', '1,"a"b\n', "1,,2\n", "1,2,\n"]:
         with pytest.raises(oracle.OracleDelimitedError) as want:
             oracle.parse_delimited(text)
