@@ -16,7 +16,8 @@
 //      loads, ranked stably per digit with match.any warp multi-split, its
 //      global offsets come from a per-digit decoupled look-back, the tile is
 //      reordered in shared memory and written out so that keys of one digit
-//      go to consecutive addresses (coalesced stores).
+//      go to consecutive addresses (coalesced stores, two keys of one digit
+//      per 128-bit store where the destination is aligned).
 // Buffer ping-pong is decided on the device (RadixPlan::src_sel/final_sel),
 // because skipped passes are only known after the histogram.
 #pragma once
@@ -212,11 +213,26 @@ __global__ void __launch_bounds__(THREADS) radix_pass(u64* buf_a, u64* buf_b, co
         }
         __syncthreads();
 
-        // Write out: consecutive positions of one digit are consecutive addresses.
-        for (u32 j = threadIdx.x; j < valid_count; j += THREADS) {
-            const u64 k = sh.keys[j];
-            const u32 d = static_cast<u32>((k >> shift) & (kRadix - 1));
-            dst[sh.global_base[d] + (j - sh.tile_start[d])] = k;
+        // Write out: consecutive positions of one digit are consecutive
+        // addresses. Each thread takes two neighbouring positions; when both
+        // hold the same digit and the first lands on a 16-byte boundary they
+        // leave as one 128-bit store (a warp then writes 512 contiguous
+        // bytes), otherwise as two 64-bit stores.
+        const bool dst16 = (reinterpret_cast<uintptr_t>(dst) & 15) == 0;
+        for (u32 j = 2 * threadIdx.x; j < valid_count; j += 2 * THREADS) {
+            const u64 k0 = sh.keys[j];
+            const u32 d0 = static_cast<u32>((k0 >> shift) & (kRadix - 1));
+            const u64 o0 = sh.global_base[d0] + (j - sh.tile_start[d0]);
+            if (j + 1 < valid_count) {
+                const u64 k1 = sh.keys[j + 1];
+                const u32 d1 = static_cast<u32>((k1 >> shift) & (kRadix - 1));
+                if (d1 == d0 && dst16 && (o0 & 1) == 0) {
+                    *reinterpret_cast<ulonglong2*>(dst + o0) = make_ulonglong2(k0, k1);
+                    continue;
+                }
+                dst[sh.global_base[d1] + (j + 1 - sh.tile_start[d1])] = k1;
+            }
+            dst[o0] = k0;
         }
         __syncthreads();
     }
