@@ -407,6 +407,8 @@ typedef struct sparkalog_tuning {
     uint32_t merge_items;         /* rows per thread of a merge tile: 7, 11 or 15 */
     uint32_t level_ratio;         /* a FULL level merges down past 1/ratio of the next (2-64) */
     uint32_t levels;              /* sorted runs that hold a recursive FULL (2-4) */
+    uint32_t bloom_bits;          /* bits per FULL row of the anti-join's Bloom filter; 0: no filter (0, 4-32) */
+    uint32_t reserved;            /* 0 */
 } sparkalog_tuning;
 
 /* The built-in defaults (measured on a B200). */

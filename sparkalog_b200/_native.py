@@ -126,10 +126,12 @@ class TuningC(ctypes.Structure):
         ("merge_items", ctypes.c_uint32),
         ("level_ratio", ctypes.c_uint32),
         ("levels", ctypes.c_uint32),
+        ("bloom_bits", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
     ]
 
     def as_dict(self) -> dict:
-        return {name: int(getattr(self, name)) for name, _ in self._fields_}
+        return {name: int(getattr(self, name)) for name, _ in self._fields_ if name != "reserved"}
 
 
 class SelectC(ctypes.Structure):

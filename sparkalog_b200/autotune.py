@@ -49,6 +49,7 @@ SPACE: dict[str, list[int]] = {
     "level_ratio": [3, 4, 6, 8],
     "levels": [3, 4],
     "merge_items": [7, 11, 15],
+    "bloom_bits": [0, 8, 12, 16],
 }
 
 

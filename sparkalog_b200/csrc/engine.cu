@@ -29,6 +29,7 @@
 #include "spk_fused.cuh"
 #include "spk_member.cuh"
 #include "spk_ingest.cuh"
+#include "spk_bloom.cuh"
 #include "spk_loop.cuh"
 #include "spk_setops.cuh"
 
@@ -201,6 +202,8 @@ sparkalog_tuning default_tuning() {
     t.merge_items = 11;
     t.level_ratio = 4;
     t.levels = 3;
+    t.bloom_bits = 0;
+    t.reserved = 0;
     return t;
 }
 
@@ -208,7 +211,8 @@ bool tuning_valid(const sparkalog_tuning& t) {
     const bool lanes = t.group_lanes == 4 || t.group_lanes == 8 || t.group_lanes == 16;
     return t.dir_rows_log2 <= 10 && lanes && t.fused_rows_cap >= 64 && t.fused_rows_cap <= 768 &&
            (t.merge_items == 7 || t.merge_items == 11 || t.merge_items == 15) && t.level_ratio >= 2 && t.level_ratio <= 64 && t.levels >= 2 &&
-           t.levels <= static_cast<u32>(spk::kMaxLevels) && t.group_candidates <= t.sparse_candidates;
+           t.levels <= static_cast<u32>(spk::kMaxLevels) && t.group_candidates <= t.sparse_candidates &&
+           (t.bloom_bits == 0 || (t.bloom_bits >= 4 && t.bloom_bits <= 32)) && t.reserved == 0;
 }
 
 // A stream-ordered device allocation that only grows.
@@ -286,6 +290,13 @@ struct RelState {
     u64 member_groups = 0;   // power of two
     u64 member_count = 0;    // rows inserted
     bool member_valid = false;
+    // FULL's blocked Bloom filter (spk_bloom.cuh), when the tuning asks for
+    // one: built from the levels, kept in step by the anti-join, dropped when
+    // FULL changes otherwise.
+    DevArray bloom;
+    u64 bloom_blocks = 0;
+    u64 bloom_capacity = 0;  // rows the filter was sized for
+    bool bloom_valid = false;
 
     u64 full_rows() const {
         u64 n = 0;
@@ -573,6 +584,36 @@ int member_add(RelState& r, const u64* rows, u64 n, u32* err, cudaStream_t s, u6
     if (launches) *launches += 1;
     r.member_count += n;
     return 0;
+}
+
+// FULL's Bloom filter: 2^k blocks of 256 bits, about `bits` bits per row
+// for 8 times the rows FULL holds when it is built (a recursive relation
+// grows several-fold), rebuilt larger once FULL outgrows that.
+spk::Bloom bloom_of(RelState& r) { return spk::Bloom{r.bloom.as<u32>(), r.bloom_blocks - 1}; }
+
+int bloom_build(RelState& r, u32 bits, cudaStream_t s, u64* launches) {
+    const u64 rows = std::max<u64>(r.full_rows(), 1);
+    u64 blocks = 4096;
+    while (blocks * 256 < 8 * rows * bits) blocks <<= 1;
+    SPK_CUDA(r.bloom.ensure(blocks * 32, s), "cudaMallocAsync");
+    SPK_CUDA(cudaMemsetAsync(r.bloom.ptr, 0, blocks * 32, s), "cudaMemsetAsync");
+    r.bloom_blocks = blocks;
+    r.bloom_capacity = blocks * 256 / bits;
+    const spk::Bloom bf = bloom_of(r);
+    for (int l = 0; l < spk::kMaxLevels; ++l) {
+        if (r.level_n[l] == 0) continue;
+        spk::bloom_insert_kernel<<<simple_grid(r.level_n[l]), 256, 0, s>>>(r.level[l].as<u64>(), r.level_n[l], bf);
+        SPK_CUDA(cudaGetLastError(), "bloom_insert_kernel");
+        if (launches) *launches += 1;
+    }
+    r.bloom_valid = true;
+    return 0;
+}
+
+// A valid filter for FULL before its anti-join (built, or rebuilt larger).
+int bloom_ready(RelState& r, u32 bits, cudaStream_t s, u64* launches) {
+    if (r.bloom_valid && r.full_rows() <= r.bloom_capacity) return 0;
+    return bloom_build(r, bits, s, launches);
 }
 
 struct SortScratch {
@@ -1076,6 +1117,7 @@ struct LoopGraph {
     u64 bound = 0;
     u32 lanes = 0, items = 0;
     bool segments = false;
+    bool bloom = false;                   // the anti-join probes FULL's Bloom filter
     std::mutex use;
     spk::LoopDesc* desc = nullptr;        // device
     spk::LoopDesc* host_desc = nullptr;   // pinned
@@ -1093,7 +1135,7 @@ std::mutex g_loop_mu;
 std::vector<LoopGraph*> g_loops;  // kept for the life of the process
 
 struct LoopGrids {
-    unsigned fused, anti, merge, split, segment;
+    unsigned fused, anti, anti_bloom, merge, split, segment;
 };
 
 // Shared-memory opt-ins and persistent grid sizes of the loop's kernels.
@@ -1112,6 +1154,11 @@ cudaError_t prepare_loop_kernels(const LoopGraph& g, LoopGrids* grids) {
     const u64 anti_tiles = (g.bound + (kWideThreads / G) - 1) / (kWideThreads / G);
     grids->fused = spk::persistent_grid(reinterpret_cast<const void*>(fused), kFusedThreads, FL::kBytes, fused_tiles);
     grids->anti = spk::persistent_grid(reinterpret_cast<const void*>(anti), kWideThreads, 0, anti_tiles);
+    {
+        auto bloom = spk::loop_anti_join_bloom_kernel<kSparseThreads, kSparseItems>;
+        grids->anti_bloom = spk::persistent_grid(reinterpret_cast<const void*>(bloom), kSparseThreads, 0,
+                                                 (g.bound + kSparseTile - 1) / kSparseTile);
+    }
     grids->merge = spk::persistent_grid(reinterpret_cast<const void*>(merge), kThreads, ML::kBytes, ~0ull >> 1);
     grids->split = static_cast<unsigned>(spk::device_sm_count()) * 4;
     grids->segment = simple_grid(g.bound);
@@ -1184,7 +1231,11 @@ cudaError_t build_loop_graph_shape(LoopGraph& g) {
         e = add_kernel_node(body, &last,
                             reinterpret_cast<const void*>(spk::loop_fused_kernel<kFusedThreads, kFusedCap, kFusedRowCap>),
                             gr.fused, kFusedThreads, FL::kBytes, desc_args);
-    if (e == cudaSuccess)
+    if (e == cudaSuccess && g.bloom)
+        e = add_kernel_node(body, &last,
+                            reinterpret_cast<const void*>(spk::loop_anti_join_bloom_kernel<kSparseThreads, kSparseItems>),
+                            gr.anti_bloom, kSparseThreads, 0, desc_args);
+    else if (e == cudaSuccess)
         e = add_kernel_node(body, &last, reinterpret_cast<const void*>(spk::loop_anti_join_kernel<kWideThreads, G>),
                             gr.anti, kWideThreads, 0, desc_args);
     if (e == cudaSuccess)
@@ -1217,14 +1268,15 @@ cudaError_t build_loop_graph(LoopGraph& g) {
 }
 
 // The cached graph for this shape (built on first use).
-cudaError_t loop_graph(cudaStream_t s, u64 bound, u32 lanes, u32 items, bool segments, LoopGraph** out) {
+cudaError_t loop_graph(cudaStream_t s, u64 bound, u32 lanes, u32 items, bool segments, bool bloom,
+                       LoopGraph** out) {
     int device = 0;
     cudaError_t e = cudaGetDevice(&device);
     if (e != cudaSuccess) return e;
     std::lock_guard<std::mutex> lock(g_loop_mu);
     for (LoopGraph* g : g_loops) {
         if (g->device == device && g->stream == s && g->bound == bound && g->lanes == lanes && g->items == items &&
-            g->segments == segments) {
+            g->segments == segments && g->bloom == bloom) {
             *out = g;
             return cudaSuccess;
         }
@@ -1236,6 +1288,7 @@ cudaError_t loop_graph(cudaStream_t s, u64 bound, u32 lanes, u32 items, bool seg
     g->lanes = lanes;
     g->items = items;
     g->segments = segments;
+    g->bloom = bloom;
     g->fused_status_words = (bound + kLoopMinFusedRows - 1) / kLoopMinFusedRows + 2;
     g->anti_status_words = (bound + (kWideThreads / lanes) - 1) / (kWideThreads / lanes) + 2;
     e = cudaMalloc(reinterpret_cast<void**>(&g->desc), sizeof(spk::LoopDesc));
@@ -1308,9 +1361,19 @@ int run_device_loop(sparkalog_executor* ex, sparkalog_store* st, size_t ti, u64 
     }
     int rc = refresh_directories(st, tr, s, nullptr);
     if (rc) return rc;
+    const bool use_bloom = ex->tuning.bloom_bits != 0;
+    if (use_bloom) {
+        // Sized for the largest FULL the loop may reach (it stops at a cascade).
+        if (!tr.bloom_valid || tr.full_rows() + upper_n / ratio + bound > tr.bloom_capacity) {
+            rc = bloom_build(tr, ex->tuning.bloom_bits, s, nullptr);
+            if (rc) return rc;
+        }
+    } else {
+        tr.bloom_valid = false;
+    }
 
     LoopGraph* g = nullptr;
-    SPK_CUDA(loop_graph(s, bound, ex->tuning.group_lanes, st->merge_items, ex->seg_count != 0, &g),
+    SPK_CUDA(loop_graph(s, bound, ex->tuning.group_lanes, st->merge_items, ex->seg_count != 0, use_bloom, &g),
              "device loop graph");
     std::lock_guard<std::mutex> use(g->use);
     spk::LoopDesc& d = *g->host_desc;
@@ -1383,6 +1446,7 @@ int run_device_loop(sparkalog_executor* ex, sparkalog_store* st, size_t ti, u64 
     d.seg_seen = ex->seg_seen.as<u32>();
     d.seg_new = ex->seg_new.as<unsigned long long>();
     d.trace = g->trace;
+    d.bloom = use_bloom ? bloom_of(tr) : spk::Bloom{nullptr, 0};
     SPK_CUDA(cudaMemcpyAsync(g->desc, &d, sizeof(d), cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
     SPK_CUDA(cudaGraphLaunch(g->exec, s), "cudaGraphLaunch");
     SPK_CUDA(cudaMemcpyAsync(&d, g->desc, sizeof(d), cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
@@ -2706,6 +2770,11 @@ int sparkalog_store_append(sparkalog_store* st, u32 id, const u32* first, const 
         r->dir_valid[l] = false;
         rc = member_add(*r, fresh.as<u64>(), fresh_n, ops.counters.as<u32>() + 33, s, nullptr);
         if (rc) return rc;
+        if (r->bloom_valid && fresh_n) {
+            // FULL's Bloom filter takes the new rows too.
+            spk::bloom_insert_kernel<<<simple_grid(fresh_n), 256, 0, s>>>(fresh.as<u64>(), fresh_n, bloom_of(*r));
+            SPK_CUDA(cudaGetLastError(), "bloom_insert_kernel");
+        }
         if (r->recursive) {
             // DELTA u= fresh rows (DELTA is part of FULL, so they are disjoint).
             if (!r->delta_sorted) {
@@ -3355,6 +3424,13 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                 RelState& tr = *st->find(t.id);
                 u64 dir_launches = 0;
                 bool use_member = false;
+                const bool use_bloom = ex->tuning.bloom_bits != 0 && tr.recursive && !ex->member_enabled;
+                if (use_bloom) {
+                    int rc = bloom_ready(tr, ex->tuning.bloom_bits, s, &dir_launches);
+                    if (rc) return rc;
+                } else {
+                    tr.bloom_valid = false;  // this round's NEWT will not reach the filter
+                }
                 if (ex->member_enabled && tr.recursive) {
                     if (!tr.member_valid) {
                         int rc = member_build(tr, member_err, s, &dir_launches);
@@ -3435,7 +3511,17 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                     cand_bound += ex->host_rule_delta[k] * static_cast<u64>(std::max<u32>(ex->index[k].max_degree, 1));
                 // Distinct join rows of the target (round trace).
                 unsigned long long* unique_word = reinterpret_cast<unsigned long long*>(tc + t.rules.size() + 2);
-                if (use_member) {
+                if (use_bloom) {
+                    // The filter rules out most candidates with one sector each;
+                    // the rest are searched in the levels.
+                    auto kernel = spk::anti_join_bloom_kernel<kSparseThreads, kSparseItems>;
+                    const size_t tiles = (cand_bound + kSparseTile - 1) / kSparseTile;
+                    kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kSparseThreads, std::max<size_t>(tiles, 1)),
+                             kSparseThreads, 0, s>>>(cand, t.j_b.as<u64>(), cand_sel, jn, lv, bloom_of(tr),
+                                                     tr.newt.as<u64>(), tc + t.rules.size() + 1, ex->status.as<u64>(),
+                                                     counters + counter_slot++, ex->epoch++, err, unique_word);
+                    SPK_CUDA(cudaGetLastError(), "anti_join_bloom_kernel");
+                } else if (use_member) {
                     auto kernel = spk::anti_join_member_kernel<kThreads, kSetItems>;
                     const size_t tiles = (t.j_cap + kSetTile - 1) / kSetTile;
                     kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kThreads, std::max<size_t>(tiles, 1)),

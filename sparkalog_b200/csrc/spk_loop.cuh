@@ -23,6 +23,7 @@
 //     is not applied, and the host redoes it with the general kernels).
 #pragma once
 
+#include "spk_bloom.cuh"
 #include "spk_common.cuh"
 #include "spk_engine_kernels.cuh"
 #include "spk_fused.cuh"
@@ -75,6 +76,7 @@ struct LoopDesc {
     u32* seg_seen;
     unsigned long long* seg_new;
     LoopTrace* trace;      // one record per applied round (capacity >= limit)
+    Bloom bloom;           // FULL's Bloom filter (the Bloom variant of the anti-join)
 };
 
 template <int THREADS, int CAP, int ROWCAP>
@@ -88,6 +90,14 @@ __global__ void __launch_bounds__(THREADS) loop_anti_join_kernel(const LoopDesc*
     const u64* cand = d->fused.out;
     anti_join_group<THREADS, G>(cand, cand, nullptr, d->counts + 1, d->lv, d->newt, d->counts + 2, d->anti_status,
                                 d->counters + 1, 1u, d->err, reinterpret_cast<unsigned long long*>(d->counts + 3));
+}
+
+template <int THREADS, int ITEMS>
+__global__ void __launch_bounds__(THREADS) loop_anti_join_bloom_kernel(const LoopDesc* d) {
+    const u64* cand = d->fused.out;
+    anti_join_bloom<THREADS, ITEMS>(cand, cand, nullptr, d->counts + 1, d->lv, d->bloom, d->newt, d->counts + 2,
+                                    d->anti_status, d->counters + 1, 1u, d->err,
+                                    reinterpret_cast<unsigned long long*>(d->counts + 3));
 }
 
 static __global__ void loop_split_kernel(const LoopDesc* d, u32 tile) {

@@ -431,6 +431,8 @@ TUNINGS = [
     {"merge_items": 7, "levels": 4, "dir_rows_log2": 2, "group_lanes": 4},
     {"merge_items": 15, "levels": 2, "dir_rows_log2": 0, "group_lanes": 16, "group_candidates": 1 << 21},
     {"level_ratio": 2, "sparse_candidates": 1 << 22, "group_candidates": 1 << 12, "fused_rows_cap": 128},
+    {"bloom_bits": 8},
+    {"bloom_bits": 4, "levels": 4, "group_candidates": 1 << 12},
 ]
 
 
