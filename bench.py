@@ -348,6 +348,8 @@ def run_ours(args):
         if profile:
             ex.set_profiling(True)
         summary = ex.run(store)
+        # FULL as one sorted run, as the reference leaves it after every round.
+        store.compact(1)
         stats = ex.stats()
         stats["trace"] = ex.trace() if profile else []
         ex.close()

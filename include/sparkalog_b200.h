@@ -253,6 +253,13 @@ SPARKALOG_API int sparkalog_store_anti_join(sparkalog_store* store, uint32_t lef
  * BTreeSet GeneralCpu builds) and fails with SPARKALOG_E_DUPLICATE when
  * out_id exists. */
 
+/* Merges the levels of relation id's FULL into one sorted run on the device
+ * (the single sorted FULL that TargetRuntime::apply keeps after every round,
+ * crates/sparkalog-recursion/src/generic.rs:360-397; here FULL is kept as
+ * disjoint sorted levels and merged on demand). Reads merge implicitly; this
+ * call does it ahead of them. Synchronises the store's stream. */
+SPARKALOG_API int sparkalog_store_compact(sparkalog_store* store, uint32_t id);
+
 /* Removes relation id from the store and frees its device memory (stream-
  * ordered). */
 SPARKALOG_API int sparkalog_store_drop(sparkalog_store* store, uint32_t id);

@@ -46,6 +46,7 @@ TIER_B = [
     "sparkalog_store_read",
     "sparkalog_store_anti_join",
     "sparkalog_store_drop",
+    "sparkalog_store_compact",
     "sparkalog_store_select",
     "sparkalog_store_join",
     "sparkalog_store_load_binary_u32",
@@ -237,6 +238,8 @@ def load() -> ctypes.CDLL:
     L.sparkalog_store_anti_join.restype = i
     L.sparkalog_store_drop.argtypes = [vp, ctypes.c_uint32]
     L.sparkalog_store_drop.restype = i
+    L.sparkalog_store_compact.argtypes = [vp, ctypes.c_uint32]
+    L.sparkalog_store_compact.restype = i
     L.sparkalog_store_select.argtypes = [vp, ctypes.c_uint32, ctypes.POINTER(SelectC), ctypes.c_uint32, c_sizep]
     L.sparkalog_store_select.restype = i
     L.sparkalog_store_join.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,

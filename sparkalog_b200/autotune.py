@@ -12,7 +12,8 @@ launch shape and threshold of the fixpoint (``sparkalog_tuning`` in
 * the search is coordinate descent: each value in turn is swept over its
   candidates with the others held at the best found so far, for a fixed
   number of passes; a trial's cost is the median device time of a few runs
-  (fresh store + compile + run, CUDA events on the run's stream);
+  (fresh store + compile + run + FULL merged into one sorted run, CUDA
+  events on the run's stream);
 * the choice is saved per device (name and SM count) as JSON. The executor
   applies a saved choice when it is compiled: first the file named by
   ``$SPARKALOG_TUNING``, then the user's cache
@@ -152,7 +153,9 @@ def calibration_measure(nodes: int = 1 << 22, degree: float = 0.875, seed: int =
     dev = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).cuda()
     e0, e1 = dev(src), dev(dst)
     stream = torch.cuda.current_stream()
-    reserve_device_memory(4 << 30, stream)
+    # The pool the fixpoint needs (about 1.5 KB per node), so no trial pays
+    # for growing it.
+    reserve_device_memory(max(4 << 30, nodes * 1536), stream)
     plan = transitive_closure_scc(RelationId(1), RelationId(0))
 
     def once(tuning: dict) -> float:
@@ -166,6 +169,7 @@ def calibration_measure(nodes: int = 1 << 22, degree: float = 0.875, seed: int =
             b = torch.cuda.Event(enable_timing=True)
             a.record(stream)
             ex.run(store)
+            store.compact(1)
             b.record(stream)
             b.synchronize()
             ex.close()

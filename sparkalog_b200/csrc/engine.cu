@@ -416,19 +416,28 @@ int check_store_fault(sparkalog_store* st) {
 }
 
 // Collapses all levels of a relation into level[0] (a single sorted run).
+// Levels are disjoint sorted runs, larger towards level 0, so the smallest
+// merge first: each level merges into the nearest non-empty level below it,
+// from the top down, and level 0 is rewritten once.
 int materialize(sparkalog_store* st, RelState& r) {
     cudaStream_t s = st->stream;
-    for (int l = 1; l < spk::kMaxLevels; ++l) {
+    for (int l = spk::kMaxLevels - 1; l >= 1; --l) {
         if (r.level_n[l] == 0) continue;
-        const u64 total = r.level_n[0] + r.level_n[l];
-        SPK_CUDA(r.spare.ensure(total * 8, s), "cudaMallocAsync");
-        SPK_CUDA(store_merge(st, r.level[0].as<u64>(), r.level_n[0], r.level[l].as<u64>(), r.level_n[l],
-                             r.spare.as<u64>()),
-                 "merge_bulk_kernel");
-        swap_arrays(r.level[0], r.spare);
-        r.level_n[0] = total;
+        int t = l - 1;
+        while (t > 0 && r.level_n[t] == 0) --t;
+        if (r.level_n[t] == 0) {
+            swap_arrays(r.level[t], r.level[l]);
+        } else {
+            const u64 total = r.level_n[t] + r.level_n[l];
+            SPK_CUDA(r.spare.ensure(total * 8, s), "cudaMallocAsync");
+            SPK_CUDA(store_merge(st, r.level[t].as<u64>(), r.level_n[t], r.level[l].as<u64>(), r.level_n[l],
+                                 r.spare.as<u64>()),
+                     "merge_bulk_kernel");
+            swap_arrays(r.level[t], r.spare);
+        }
+        r.level_n[t] += r.level_n[l];
         r.level_n[l] = 0;
-        r.dir_valid[0] = r.dir_valid[l] = false;
+        r.dir_valid[t] = r.dir_valid[l] = false;
     }
     return 0;
 }
@@ -2477,6 +2486,15 @@ int sparkalog_catalog_export(sparkalog_catalog* c, uint32_t* kinds, uint32_t* nu
     *bytes_used = used;
     if (bytes && used > bytes_capacity) return fail(SPARKALOG_E_INVALID_ARGUMENT, "byte buffer too small");
     return 0;
+}
+
+int sparkalog_store_compact(sparkalog_store* st, u32 id) {
+    if (!st) return fail(SPARKALOG_E_INVALID_ARGUMENT, "null store");
+    RelState* r = st->find(id);
+    if (!r) return fail(SPARKALOG_E_MISSING, "relation " + std::to_string(id) + " is not registered");
+    int rc = materialize(st, *r);
+    if (rc) return rc;
+    return check_store_fault(st);
 }
 
 int sparkalog_store_rows(sparkalog_store* st, u32 id, int version, size_t* rows) {

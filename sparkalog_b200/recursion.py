@@ -158,6 +158,11 @@ class RelationStore:
         _check(_native.load().sparkalog_store_anti_join(self._h, *ids))
         return self.rows(ids[2])
 
+    def compact(self, rid: RelationId | int) -> None:
+        """Merges FULL's levels into one sorted run on the device (the single
+        sorted FULL the reference's TargetRuntime::apply keeps, generic.rs:360-397)."""
+        _check(_native.load().sparkalog_store_compact(self._h, int(getattr(rid, "value", rid))))
+
     def drop(self, rid: RelationId | int) -> None:
         """Removes a relation and frees its device memory."""
         _check(_native.load().sparkalog_store_drop(self._h, int(getattr(rid, "value", rid))))

@@ -475,3 +475,27 @@ def test_device_loop_respects_step_limits(cuda):
     full, iterations, derived, _, loop = _run_tc(src, dst, None, device_loop=True, steps=3)
     assert iterations == it and derived == new
     assert np.array_equal(full[0], w0) and np.array_equal(full[1], w1)
+
+
+@pytest.mark.parametrize("levels", [2, 3, 4])
+def test_compact_merges_full_into_one_sorted_run(cuda, levels):
+    # store.compact merges FULL's levels (smallest first) into one sorted run:
+    # the rows, and what a later read returns, are the oracle's fixpoint.
+    src, dst = generators.er_edges(300_000, 262_500, 6)
+    (w0, w1), it, new = oracle.transitive_closure(src, dst, threads=8)
+    R = rec()
+    e0, e1 = oracle.btree_pairs(src, dst)
+    store = R.RelationStore()
+    store.insert_static(0, (e0, e1))
+    store.insert_recursive(1, (e0, e1), (e0, e1))
+    ex = R.RecursiveExecutor.compile(R.transitive_closure_scc(_rid(1), _rid(0)), store)
+    ex.set_tuning({"levels": levels})
+    summary = ex.run(store)
+    assert summary.iterations == it and summary.total_new_rows == new
+    store.compact(1)
+    assert store.rows(1) == len(w0)
+    store.compact(1)  # already one run: nothing to merge
+    f0, f1 = store.full(1)
+    assert np.array_equal(f0, w0) and np.array_equal(f1, w1)
+    ex.close()
+    store.close()
