@@ -415,7 +415,8 @@ typedef struct sparkalog_tuning {
     uint32_t level_ratio;         /* a FULL level merges down past 1/ratio of the next (2-64) */
     uint32_t levels;              /* sorted runs that hold a recursive FULL (2-4) */
     uint32_t bloom_bits;          /* bits per FULL row of the anti-join's Bloom filter; 0: no filter (0, 4-32) */
-    uint32_t reserved;            /* 0 */
+    uint32_t merge_anti_ratio;    /* the merge-form anti-join runs while FULL rows <= ratio x the round's
+                                     estimated candidates; 0: never (0-1024) */
 } sparkalog_tuning;
 
 /* The built-in defaults (measured on a B200). */

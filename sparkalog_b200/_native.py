@@ -128,11 +128,11 @@ class TuningC(ctypes.Structure):
         ("level_ratio", ctypes.c_uint32),
         ("levels", ctypes.c_uint32),
         ("bloom_bits", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32),
+        ("merge_anti_ratio", ctypes.c_uint32),
     ]
 
     def as_dict(self) -> dict:
-        return {name: int(getattr(self, name)) for name, _ in self._fields_ if name != "reserved"}
+        return {name: int(getattr(self, name)) for name, _ in self._fields_}
 
 
 class SelectC(ctypes.Structure):

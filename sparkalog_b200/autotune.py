@@ -51,6 +51,7 @@ SPACE: dict[str, list[int]] = {
     "levels": [3, 4],
     "merge_items": [7, 11, 15],
     "bloom_bits": [0, 8, 12, 16],
+    "merge_anti_ratio": [0, 8, 16, 32, 64, 128],
 }
 
 

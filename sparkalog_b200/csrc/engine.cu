@@ -29,6 +29,7 @@
 #include "spk_fused.cuh"
 #include "spk_member.cuh"
 #include "spk_ingest.cuh"
+#include "spk_anti_merge.cuh"
 #include "spk_bloom.cuh"
 #include "spk_loop.cuh"
 #include "spk_setops.cuh"
@@ -183,6 +184,10 @@ constexpr int kLevelStage = 2048;  // level rows per shared-memory chunk of the 
 constexpr int kSparseThreads = 256;  // anti-join of small candidate sets
 constexpr int kSparseItems = 4;
 constexpr int kSparseTile = kSparseThreads * kSparseItems;
+constexpr int kAntiMergeThreads = 256;  // merge-form anti-join: 11 merged rows per thread,
+constexpr int kAntiMergeItems = 11;     // 1,024 rows of side slices per stage
+constexpr int kAntiMergeSide = 1024;
+constexpr int kAntiMergeTile = kAntiMergeThreads * kAntiMergeItems;
 constexpr int kWideThreads = 256;    // group-searched anti-join (lanes per candidate: tuning.group_lanes)
 constexpr int kSortThreads = spk::RadixSortConfig::kThreads;
 constexpr int kSortItems = spk::RadixSortConfig::kItems;
@@ -203,7 +208,7 @@ sparkalog_tuning default_tuning() {
     t.level_ratio = 4;
     t.levels = 3;
     t.bloom_bits = 0;
-    t.reserved = 0;
+    t.merge_anti_ratio = 32;
     return t;
 }
 
@@ -212,7 +217,7 @@ bool tuning_valid(const sparkalog_tuning& t) {
     return t.dir_rows_log2 <= 10 && lanes && t.fused_rows_cap >= 64 && t.fused_rows_cap <= 768 &&
            (t.merge_items == 7 || t.merge_items == 11 || t.merge_items == 15) && t.level_ratio >= 2 && t.level_ratio <= 64 && t.levels >= 2 &&
            t.levels <= static_cast<u32>(spk::kMaxLevels) && t.group_candidates <= t.sparse_candidates &&
-           (t.bloom_bits == 0 || (t.bloom_bits >= 4 && t.bloom_bits <= 32)) && t.reserved == 0;
+           (t.bloom_bits == 0 || (t.bloom_bits >= 4 && t.bloom_bits <= 32)) && t.merge_anti_ratio <= 1024;
 }
 
 // A stream-ordered device allocation that only grows.
@@ -660,6 +665,8 @@ struct TargetRT {
     u32 fused_rows_cap = 672;  // its ceiling, halved whenever a tile overflows
     bool force_generic = false;  // redo the current round with the general kernels
     bool fused_last = false;     // the round just applied ran the fused kernel
+    DevArray anti_plan;          // merge-form anti-join tiles (spk::AntiTile)
+    double unique_per_delta = -1.0;  // last round's distinct candidates per DELTA row
 };
 
 }  // namespace
@@ -3356,6 +3363,10 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                 const u64 wide = std::min<u64>(t.j_cap, ex->tuning.group_candidates);
                 const u64 wide_tile = kWideThreads / ex->tuning.group_lanes;
                 max_status_words = std::max<size_t>(max_status_words, (wide + wide_tile - 1) / wide_tile + 1);
+                // ...or the merge-form kernel's, over FULL and the candidates...
+                if (ex->tuning.merge_anti_ratio)
+                    max_status_words = std::max<size_t>(
+                        max_status_words, (st->find(t.id)->full_rows() + t.j_cap + kAntiMergeTile - 1) / kAntiMergeTile + 1);
                 // ...and per fused tile, which are DELTA-row tiles.
                 u64 delta_rows = 0;
                 for (size_t k : t.rules) delta_rows += ex->host_rule_delta[k];
@@ -3433,6 +3444,7 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
             ex->end(join_timing, s, 0.0, join_launches);
             std::vector<int> hist_t(ex->targets.size(), -1), pass_t(ex->targets.size(), -1),
                 anti_t(ex->targets.size(), -1), fused_t(ex->targets.size(), -1);
+            std::vector<u64> anti_full(ex->targets.size(), 0);  // FULL rows a merge-form anti-join read
             // Distinct (radix sort) + unique/anti-join per target. The sort
             // reads the clamped candidate count from the device.
             for (size_t ti = 0; ti < ex->targets.size(); ++ti) {
@@ -3529,7 +3541,57 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                     cand_bound += ex->host_rule_delta[k] * static_cast<u64>(std::max<u32>(ex->index[k].max_degree, 1));
                 // Distinct join rows of the target (round trace).
                 unsigned long long* unique_word = reinterpret_cast<unsigned long long*>(tc + t.rules.size() + 2);
-                if (use_bloom) {
+                // Merge form while FULL is within merge_anti_ratio times the
+                // round's candidates (estimated from the last round's distinct
+                // rows per DELTA row): reading FULL once then costs less than a
+                // search per candidate.
+                u64 full_rows = 0;
+                int partner = 0;
+                for (int l = 0; l < lv.n; ++l) {
+                    full_rows += lv.count[l];
+                    if (lv.count[l] > lv.count[partner]) partner = l;
+                }
+                u64 delta_rows = 0;
+                for (size_t k : t.rules) delta_rows += ex->host_rule_delta[k];
+                const double cand_estimate = t.unique_per_delta >= 0.0
+                                                 ? t.unique_per_delta * static_cast<double>(delta_rows)
+                                                 : static_cast<double>(cand_bound);
+                const bool use_merge_form = ex->tuning.merge_anti_ratio != 0 && !use_bloom && !use_member && lv.n > 0 &&
+                                            static_cast<double>(full_rows) <=
+                                                static_cast<double>(ex->tuning.merge_anti_ratio) * cand_estimate;
+                if (use_merge_form) {
+                    const u64 tiles = (full_rows + t.j_cap + kAntiMergeTile - 1) / kAntiMergeTile;
+                    SPK_CUDA(t.anti_plan.ensure(std::max<u64>(tiles, 1) * sizeof(spk::AntiTile), s), "cudaMallocAsync");
+                    spk::AntiTile* plan = t.anti_plan.as<spk::AntiTile>();
+                    {
+                        const u64 blocks = std::min<u64>((tiles + 7) / 8, static_cast<u64>(spk::device_sm_count()) * 16);
+                        spk::anti_merge_plan_kernel<kAntiMergeTile><<<static_cast<unsigned>(std::max<u64>(blocks, 1)), 256,
+                                                                      0, s>>>(cand, t.j_b.as<u64>(), cand_sel, jn, lv,
+                                                                              partner, plan);
+                        SPK_CUDA(cudaGetLastError(), "anti_merge_plan_kernel");
+                    }
+                    using AL = spk::AntiMergeLayout<kAntiMergeThreads, kAntiMergeItems, kAntiMergeSide>;
+                    auto kernel = spk::anti_merge_kernel<kAntiMergeThreads, kAntiMergeItems, kAntiMergeSide>;
+                    static std::atomic<u64> configured{0};
+                    int device = 0;
+                    SPK_CUDA(cudaGetDevice(&device), "cudaGetDevice");
+                    const u64 bit = 1ull << (device & 63);
+                    if (!(configured.load() & bit)) {
+                        SPK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                      static_cast<int>(AL::kBytes)),
+                                 "cudaFuncSetAttribute");
+                        configured.fetch_or(bit);
+                    }
+                    const unsigned grid = spk::persistent_grid(reinterpret_cast<const void*>(kernel), kAntiMergeThreads,
+                                                               AL::kBytes, std::max<u64>(tiles, 1));
+                    kernel<<<grid, kAntiMergeThreads, AL::kBytes, s>>>(
+                        cand, t.j_b.as<u64>(), cand_sel, jn, lv, partner, plan, tr.newt.as<u64>(),
+                        tc + t.rules.size() + 1, ex->status.as<u64>(), counters + counter_slot++, ex->epoch++, err,
+                        unique_word);
+                    SPK_CUDA(cudaGetLastError(), "anti_merge_kernel");
+                    anti_full[ti] = full_rows;
+                    ex->stats.total_launches += 1;
+                } else if (use_bloom) {
                     // The filter rules out most candidates with one sector each;
                     // the rest are searched in the levels.
                     auto kernel = spk::anti_join_bloom_kernel<kSparseThreads, kSparseItems>;
@@ -3579,7 +3641,7 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                                                ex->epoch++, err, unique_word);
                     SPK_CUDA(cudaGetLastError(), "anti_join_levels_kernel");
                 }
-                ex->end(anti_t[ti], s, 0.0, 1);
+                ex->end(anti_t[ti], s, 0.0, use_merge_form ? 2 : 1);
                 ex->stats.total_launches += 1 + dir_launches;
                 if (!fused[ti])
                     SPK_CUDA(cudaMemcpyAsync(ex->host_active + ti * spk::kMaxPasses,
@@ -3613,7 +3675,9 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                         ex->timings[pass_t[ti]].bytes = 16.0 * jn * static_cast<double>(active);
                         ex->timings[pass_t[ti]].launches = active;
                     }
-                    if (anti_t[ti] >= 0) ex->timings[anti_t[ti]].bytes = 8.0 * jn + 8.0 * nn;
+                    // The merge form reads FULL once as well.
+                    if (anti_t[ti] >= 0)
+                        ex->timings[anti_t[ti]].bytes = 8.0 * jn + 8.0 * nn + 8.0 * static_cast<double>(anti_full[ti]);
                     if (fused_t[ti] >= 0) {
                         // DELTA rows and their index entries, the joined right
                         // rows, the distinct candidates out.
@@ -3743,6 +3807,7 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                                    static_cast<double>(delta_rows);
             const double rows = kFusedCap / (1.5 * std::max(per_row, 1e-3));
             t.fused_rows = static_cast<u32>(std::max(64.0, std::min<double>(t.fused_rows_cap, rows)));
+            t.unique_per_delta = static_cast<double>(c[t.rules.size() + 2]) / static_cast<double>(delta_rows);
         }
     }
     u32* member_err_host = reinterpret_cast<u32*>(ex->host_counts + ex->counts_words + 30);

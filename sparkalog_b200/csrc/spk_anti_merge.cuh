@@ -1,0 +1,354 @@
+// Merge-form anti-join for the rounds whose candidates are dense in FULL's
+// key space: NEWT = unique(sorted candidates) - FULL, FULL the union of the
+// levels, replacing SortedBinaryAntiJoin (crates/sparkalog-execution/native/
+// column_ops.cu:167-227, 551-641) with the reference's own merge formulation.
+//
+// The candidates and FULL's largest level (the partner) are cut into tiles
+// of THREADS * ITEMS rows of their merged order (merge-path diagonals, the
+// partner's row first on equal keys), so every tile holds a bounded number
+// of rows whatever the ratio of candidates to FULL. For the other levels
+// (the sides) a tile needs only their rows inside the tile's key range,
+// which the plan kernel finds through their directories. A tile's partner
+// slice, candidate slice and side slices arrive in shared memory by bulk
+// copies on one mbarrier while the previous tile is processed (two stages);
+// side slices that do not fit the stage are searched in global memory
+// instead. Each thread takes ITEMS consecutive candidates, keeps the first of
+// each run of equal ones (BinaryDistinct), and drops those found in a slice:
+// a candidate equal to a partner row either finds it in the tile's partner
+// slice or, when the row ends the previous tile, in the one partner row
+// loaded ahead of the slice. Kept rows are compacted in tile order with a
+// decoupled look-back (tiles are claimed in order, so the look-back only
+// waits on tiles already claimed), staged in place, and stored coalesced.
+#pragma once
+
+#include "spk_common.cuh"
+#include "spk_engine_kernels.cuh"
+#include "spk_setops.cuh"
+
+namespace spk {
+
+constexpr int kAntiSides = kMaxLevels - 1;
+
+// One tile of the plan: partner rows [i0, i1), candidates [j0, j1), and
+// each side level's rows [side_lo, side_hi) with keys in the tile's range.
+struct AntiTile {
+    u64 i0, i1, j0, j1;
+    u64 side_lo[kAntiSides], side_hi[kAntiSides];
+};
+
+// Merge-path split: the number of partner rows among the first d rows of the
+// merged order (partner first on equal keys): the smallest i with
+// L[i] > C[d - 1 - i].
+__device__ __forceinline__ u64 anti_split(const u64* L, u64 nL, const u64* C, u64 nC, u64 d) {
+    u64 lo = d > nC ? d - nC : 0, hi = d < nL ? d : nL;
+    while (lo < hi) {
+        const u64 mid = (lo + hi) >> 1;
+        if (C[d - 1 - mid] >= L[mid]) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// The side levels of a plan: every level but the partner, in level order.
+__device__ __forceinline__ int anti_side_level(int partner, int s) { return s < partner ? s : s + 1; }
+
+// One warp per tile: lanes 0 and 1 find the tile's two diagonals and its
+// first and last merged keys, then two lanes per side level bound that
+// level's rows in [first, last] through its directory.
+template <int TILE>
+__global__ void anti_merge_plan_kernel(const u64* buf_a, const u64* buf_b, const u32* final_sel, const u64* n_ptr,
+                                       Levels levels, int partner, AntiTile* plan) {
+    const u64* C = (final_sel && *final_sel) ? buf_b : buf_a;
+    const u64 nC = *n_ptr;
+    const u64* L = levels.keys[partner];
+    const u64 nL = levels.count[partner];
+    const u64 total = nL + nC;
+    const u64 tiles = (total + TILE - 1) / TILE;
+    const u32 lane = lane_id();
+    const u64 warps = static_cast<u64>(gridDim.x) * (blockDim.x / kWarp);
+    for (u64 t = static_cast<u64>(blockIdx.x) * (blockDim.x / kWarp) + warp_id(); t < tiles; t += warps) {
+        u64 i = 0, j = 0, key = 0;
+        if (lane < 2) {
+            const u64 d = (t + lane) * TILE < total ? (t + lane) * TILE : total;
+            i = anti_split(L, nL, C, nC, d);
+            j = d - i;
+            if (lane == 0) {
+                // First merged row of the tile (the tile is not empty).
+                key = (i < nL && (j >= nC || L[i] <= C[j])) ? L[i] : C[j];
+            } else {
+                // Last merged row of the tile: the larger of the rows before d.
+                const u64 a = i > 0 ? L[i - 1] : 0, c = j > 0 ? C[j - 1] : 0;
+                key = i == 0 ? c : (j == 0 ? a : (a > c ? a : c));
+            }
+        }
+        const u64 first = __shfl_sync(0xffffffffu, key, 0);
+        const u64 last = __shfl_sync(0xffffffffu, key, 1);
+        AntiTile& p = plan[t];
+        if (lane == 0) {
+            p.i0 = i;
+            p.j0 = j;
+        } else if (lane == 1) {
+            p.i1 = i;
+            p.j1 = j;
+        } else if (lane < 2 + 2 * kAntiSides) {
+            const int s = static_cast<int>(lane - 2) >> 1;
+            const bool hi_side = ((lane - 2) & 1) != 0;
+            const int l = anti_side_level(partner, s);
+            u64 v = 0;
+            if (l < levels.n && levels.count[l] > 0) {
+                if (!hi_side) v = dir_lower_bound(levels, l, first);
+                else v = last == ~0ull ? levels.count[l] : dir_lower_bound(levels, l, last + 1);
+            }
+            if (!hi_side) p.side_lo[s] = v;
+            else p.side_hi[s] = v;
+        }
+    }
+}
+
+// Shared memory of anti_merge_kernel: two stages, each holding the partner
+// and candidate slices (with one row ahead of each and 16-byte alignment
+// slack) and up to SIDE_ROWS rows of side slices; per-stage bookkeeping;
+// the stages' barriers.
+template <int THREADS, int ITEMS, int SIDE_ROWS>
+struct AntiMergeLayout {
+    static constexpr int kTile = THREADS * ITEMS;
+    static constexpr int kMainRows = kTile + 8;
+    static constexpr int kSideRows = SIDE_ROWS + 2 * kAntiSides;
+    static constexpr int kStageRows = kMainRows + kSideRows;
+    static constexpr size_t kStage = static_cast<size_t>(kStageRows) * sizeof(u64);
+    static constexpr int kMetaWords = 16;
+    static constexpr size_t kMeta = 2 * kStage;
+    static constexpr size_t kBars = kMeta + 2 * kMetaWords * sizeof(u64);
+    static constexpr size_t kBytes = kBars + 2 * sizeof(unsigned long long);
+    static_assert(kTile % 2 == 0 && kMainRows % 2 == 0, "16-byte aligned regions");
+};
+
+// Per-stage bookkeeping words.
+enum : int {
+    kAmTile = 0,      // tile index
+    kAmLOff = 1,      // stage row of partner row i0
+    kAmLCount = 2,    // i1 - i0
+    kAmCOff = 3,      // stage row of candidate j0
+    kAmCCount = 4,    // j1 - j0
+    kAmI0 = 5,
+    kAmJ0 = 6,
+    kAmSideOff = 7,   // + s: stage row of the side slice, or ~0: search it in global memory
+    kAmSideCount = 7 + kAntiSides,
+    kAmSideLo = 7 + 2 * kAntiSides,  // + s: the slice's first row in its level
+};
+static_assert(kAmSideLo + kAntiSides <= 16, "bookkeeping fits 16 words");
+
+template <int THREADS, int ITEMS, int SIDE_ROWS>
+__global__ void __launch_bounds__(THREADS) anti_merge_kernel(const u64* buf_a, const u64* buf_b, const u32* final_sel,
+                                                             const u64* n_ptr, Levels levels, int partner,
+                                                             const AntiTile* plan, u64* out, u64* out_count,
+                                                             u64* status, u32* tile_counter, u32 epoch, u32* err,
+                                                             unsigned long long* unique_count) {
+    using Lay = AntiMergeLayout<THREADS, ITEMS, SIDE_ROWS>;
+    constexpr int kTile = Lay::kTile;
+    extern __shared__ __align__(16) unsigned char smem[];
+    auto stage = [&](int st) { return reinterpret_cast<u64*>(smem + st * Lay::kStage); };
+    u64* meta = reinterpret_cast<u64*>(smem + Lay::kMeta);
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem + Lay::kBars);
+    __shared__ CompactShared<THREADS> cs;
+    __shared__ int failed;
+
+    const u64* C = (final_sel && *final_sel) ? buf_b : buf_a;
+    const u64 nC = *n_ptr;
+    const u64* L = levels.keys[partner];
+    const u64 nL = levels.count[partner];
+    const u64 num_tiles = (nL + nC + kTile - 1) / kTile;
+    if (nC == 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) *out_count = 0;
+        return;
+    }
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_fence_init();
+        failed = 0;
+    }
+    __syncthreads();
+
+    // Thread 0: claims the next tile and issues its copies into stage st
+    // (meta[kAmTile] = num_tiles when none is left).
+    auto claim_and_issue = [&](int st) -> bool {
+        u64* m = meta + st * Lay::kMetaWords;
+        const u64 t = atomicAdd(tile_counter, 1u);
+        m[kAmTile] = t;
+        if (t >= num_tiles) return false;
+        const AntiTile& p = plan[t];
+        const u64 i0 = p.i0, i1 = p.i1, j0 = p.j0, j1 = p.j1;
+        u64* base = stage(st);
+        u32 bytes = 0;
+        // Partner slice from row i0 - 1 (the row that may equal this tile's
+        // first candidate), starting on a 16-byte boundary.
+        const u64 ls = i0 > 0 ? i0 - 1 : 0;
+        const u64 l_lead = (reinterpret_cast<uintptr_t>(L + ls) >> 3) & 1;
+        const u32 l_rows = i1 > ls ? static_cast<u32>((l_lead + i1 - ls + 1) & ~1ull) : 0u;
+        // Candidates from row j0 - 1 (the unique step compares with it).
+        const u64 cs0 = j0 > 0 ? j0 - 1 : 0;
+        const u64 c_lead = (reinterpret_cast<uintptr_t>(C + cs0) >> 3) & 1;
+        const u32 c_rows = j1 > cs0 ? static_cast<u32>((c_lead + j1 - cs0 + 1) & ~1ull) : 0u;
+        m[kAmLOff] = l_lead + (i0 - ls);
+        m[kAmLCount] = i1 - i0;
+        m[kAmCOff] = l_rows + c_lead + (j0 - cs0);
+        m[kAmCCount] = j1 - j0;
+        m[kAmI0] = i0;
+        m[kAmJ0] = j0;
+        bytes += (l_rows + c_rows) * 8u;
+        u32 side_used = 0;
+        u32 side_rows[kAntiSides];
+        u64 side_src[kAntiSides];
+#pragma unroll
+        for (int s = 0; s < kAntiSides; ++s) {
+            const int l = anti_side_level(partner, s);
+            const u64 lo = p.side_lo[s], hi = p.side_hi[s];
+            const u64 cnt = (l < levels.n && hi > lo) ? hi - lo : 0;
+            m[kAmSideLo + s] = lo;
+            m[kAmSideCount + s] = cnt;
+            side_rows[s] = 0;
+            side_src[s] = 0;
+            if (cnt == 0) {
+                m[kAmSideOff + s] = 0;
+                continue;
+            }
+            const u64* src = levels.keys[l] + lo;
+            const u64 lead = (reinterpret_cast<uintptr_t>(src) >> 3) & 1;
+            const u64 rows = (lead + cnt + 1) & ~1ull;
+            if (side_used + rows <= static_cast<u64>(Lay::kSideRows)) {
+                m[kAmSideOff + s] = Lay::kMainRows + side_used + lead;
+                side_rows[s] = static_cast<u32>(rows);
+                side_src[s] = reinterpret_cast<u64>(src - lead);
+                side_used += static_cast<u32>(rows);
+                bytes += static_cast<u32>(rows) * 8u;
+            } else {
+                m[kAmSideOff + s] = ~0ull;
+            }
+        }
+        mbar_arrive_expect_tx(&bars[st], bytes);
+        if (l_rows) bulk_load(base, L + (ls - l_lead), l_rows * 8u, &bars[st]);
+        if (c_rows) bulk_load(base + l_rows, C + (cs0 - c_lead), c_rows * 8u, &bars[st]);
+        u32 at = Lay::kMainRows;
+#pragma unroll
+        for (int s = 0; s < kAntiSides; ++s) {
+            if (side_rows[s]) {
+                bulk_load(base + at, reinterpret_cast<const u64*>(side_src[s]), side_rows[s] * 8u, &bars[st]);
+                at += side_rows[s];
+            }
+        }
+        return true;
+    };
+
+    u32 parity = 0, pending = 0;
+    if (threadIdx.x == 0 && claim_and_issue(0)) pending |= 1u;
+    __syncthreads();
+    for (int k = 0;; ++k) {
+        const int st = k & 1;
+        const u64* m = meta + st * Lay::kMetaWords;
+        const u64 tile = m[kAmTile];
+        if (tile >= num_tiles) break;
+        // The next tile's copies go out while this one is processed.
+        if (threadIdx.x == 0 && claim_and_issue(st ^ 1)) pending |= 1u << (st ^ 1);
+        if (mbar_wait(&bars[st], (parity >> st) & 1u)) {
+            parity ^= 1u << st;
+            pending &= ~(1u << st);
+        } else {
+            atomicOr(err, kErrBarrierTimeout);
+            failed = 1;
+        }
+        const u64* S = stage(st);
+        const u32 nLs = static_cast<u32>(m[kAmLCount]), nCs = static_cast<u32>(m[kAmCCount]);
+        const u64* Ls = S + m[kAmLOff];
+        const u64* Cs = S + m[kAmCOff];
+        const bool has_l_prev = m[kAmI0] > 0, has_c_prev = m[kAmJ0] > 0;
+
+        const u32 p0 = threadIdx.x * ITEMS;
+        u64 v[ITEMS];
+        u32 keep = 0;
+        {
+            u64 prev = (p0 > 0 && p0 - 1 < nCs) ? Cs[p0 - 1] : (has_c_prev ? Cs[-1] : 0);
+            const bool prev_ok = p0 > 0 || has_c_prev;
+#pragma unroll
+            for (int i = 0; i < ITEMS; ++i) {
+                const u32 p = p0 + i;
+                v[i] = 0;
+                if (p < nCs) {
+                    const u64 key = Cs[p];
+                    v[i] = key;
+                    if ((i > 0 || prev_ok) ? key != prev : true) keep |= 1u << i;
+                    prev = key;
+                }
+            }
+        }
+        count_unique(keep, unique_count);
+        if (keep) {
+            // Partner slice: one search for the first kept candidate, then
+            // galloping forward (the candidates are sorted).
+            const SmemKeys lk{Ls};
+            u64 cur = 0;
+            bool started = false;
+#pragma unroll
+            for (int i = 0; i < ITEMS; ++i) {
+                if (keep & (1u << i)) {
+                    cur = started ? gallop_lower_bound(lk, cur, nLs, v[i]) : lower_bound_keys(lk, 0, nLs, v[i]);
+                    started = true;
+                    if ((cur < nLs && Ls[cur] == v[i]) || (p0 + i == 0 && has_l_prev && Ls[-1] == v[i]))
+                        keep &= ~(1u << i);
+                }
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < kAntiSides; ++s) {
+            const u64 cnt = m[kAmSideCount + s];
+            if (!keep || cnt == 0) continue;
+            const u64 off = m[kAmSideOff + s];
+            if (off != ~0ull) {
+                const u64* ss = S + off;
+                const SmemKeys sk{ss};
+                u64 cur = 0;
+#pragma unroll
+                for (int i = 0; i < ITEMS; ++i) {
+                    if (keep & (1u << i)) {
+                        cur = gallop_lower_bound(sk, cur, cnt, v[i]);
+                        if (cur < cnt && ss[cur] == v[i]) keep &= ~(1u << i);
+                    }
+                }
+            } else {
+                const u64 lo = m[kAmSideLo + s];
+                const PackedKeys gk{levels.keys[anti_side_level(partner, s)]};
+                u64 cur = lo;
+#pragma unroll
+                for (int i = 0; i < ITEMS; ++i) {
+                    if (keep & (1u << i)) {
+                        cur = gallop_lower_bound(gk, cur, lo + cnt, v[i]);
+                        if (cur < lo + cnt && gk(cur) == v[i]) keep &= ~(1u << i);
+                    }
+                }
+            }
+        }
+        u32 excl, total;
+        const u64 off = compact_offsets<THREADS>(__popc(keep), &excl, &total, tile, status, epoch, err, cs);
+        // Every read of the stage is done (compact_offsets synchronises):
+        // stage the kept rows in place, then store them coalesced.
+        u64* outs = const_cast<u64*>(Cs);
+        u32 wpos = excl;
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i)
+            if (keep & (1u << i)) outs[wpos++] = v[i];
+        __syncthreads();
+        for (u32 j = threadIdx.x; j < total; j += THREADS) out[off + j] = outs[j];
+        if (tile == num_tiles - 1 && threadIdx.x == 0) *out_count = off + total;
+        // The stage's generic accesses come before the bulk copies that refill it.
+        fence_async_shared();
+        __syncthreads();
+        if (failed) break;
+    }
+    if (threadIdx.x == 0) {
+        // After a timeout, copies may still be in flight into shared memory.
+        for (int st = 0; st < 2; ++st)
+            if ((pending >> st) & 1u) mbar_wait(&bars[st], (parity >> st) & 1u);
+    }
+}
+
+}  // namespace spk

@@ -491,7 +491,7 @@ class RecursiveExecutor:
         t = _native.TuningC()
         _check(_native.load().sparkalog_executor_get_tuning(self._h, ctypes.byref(t)))
         for name, value in tuning.items():
-            if name not in dict(_native.TuningC._fields_) or name == "reserved":
+            if name not in dict(_native.TuningC._fields_):
                 raise KeyError(f"unknown tuning value {name!r}")
             setattr(t, name, int(value))
         _check(_native.load().sparkalog_executor_set_tuning(self._h, ctypes.byref(t)))

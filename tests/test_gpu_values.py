@@ -23,7 +23,7 @@ def load(text, catalog=None, **kw):
     from sparkalog_b200.datalog import ValueCatalog
     from sparkalog_b200.recursion import RelationStore
 
-    catalog = catalog or ValueCatalog()
+    catalog = catalog if catalog is not None else ValueCatalog()
     store = RelationStore()
     n = store.load_delimited(0, text, catalog, **kw)
     return store, catalog, n
