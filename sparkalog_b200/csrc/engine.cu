@@ -208,7 +208,7 @@ sparkalog_tuning default_tuning() {
     t.level_ratio = 4;
     t.levels = 3;
     t.bloom_bits = 0;
-    t.merge_anti_ratio = 32;
+    t.merge_anti_ratio = 0;
     return t;
 }
 
@@ -350,6 +350,10 @@ unsigned simple_grid(size_t n) {
 // the diagonal splits (one warp per diagonal), then the bulk-copy merge with
 // `items` rows per thread (7, 11 or 15). Returns the number of kernels
 // launched through *launches. Errors of the merge's barrier waits go to *err.
+// Merges of at least this many tiles find their diagonals one per thread
+// (merge_split_thread_kernel); smaller ones one per warp.
+constexpr u64 kThreadSplitTiles = 8192;
+
 template <int ITEMS>
 cudaError_t launch_merge_items(const u64* a, u64 na, const u64* b, u64 nb, u64* out, DevArray& splits,
                                cudaStream_t s, u32* err, spk::MergeDirectory md) {
@@ -361,10 +365,16 @@ cudaError_t launch_merge_items(const u64* a, u64 na, const u64* b, u64 nb, u64* 
     cudaError_t st = splits.ensure((tiles + 1) * 8, s);
     if (st != cudaSuccess) return st;
     {
-        const u64 warps = tiles + 1;
-        const u64 blocks = std::min<u64>((warps + 7) / 8, static_cast<u64>(spk::device_sm_count()) * 8);
-        spk::merge_split_kernel<<<static_cast<unsigned>(std::max<u64>(blocks, 1)), 256, 0, s>>>(
-            a, na, b, nb, kTile, tiles, splits.as<u64>());
+        if (tiles >= kThreadSplitTiles) {
+            const u64 blocks = std::min<u64>((tiles + 1 + 127) / 128, static_cast<u64>(spk::device_sm_count()) * 16);
+            spk::merge_split_thread_kernel<<<static_cast<unsigned>(blocks), 128, 0, s>>>(a, na, b, nb, kTile, tiles,
+                                                                                       splits.as<u64>());
+        } else {
+            const u64 warps = tiles + 1;
+            const u64 blocks = std::min<u64>((warps + 7) / 8, static_cast<u64>(spk::device_sm_count()) * 8);
+            spk::merge_split_kernel<<<static_cast<unsigned>(std::max<u64>(blocks, 1)), 256, 0, s>>>(
+                a, na, b, nb, kTile, tiles, splits.as<u64>());
+        }
         st = cudaGetLastError();
         if (st != cudaSuccess) return st;
     }
@@ -518,8 +528,16 @@ int merge_buffers(sparkalog_store* st, RelState& r, int l, u64 n, cudaStream_t s
     return 0;
 }
 
+// Merges of at least this many rows leave the merged level's directory to
+// level_directory_kernel: written inside the merge it doubled the merge's
+// time (an 84M-row merge: 0.24 ms without, 0.46 ms with), while the
+// directory kernel's per-bucket searches over the merged level take a
+// fraction of that; below it one launch less wins.
+constexpr u64 kMergeDirectoryRows = 1ull << 22;
+
 // Merges two disjoint sorted runs into level l of r (through r.spare) and
-// writes the merged level's directory on the way when the merge runs a kernel.
+// writes the merged level's directory: on the way when the merge is small
+// and runs a kernel, else by a directory pass after it.
 int merge_into_level(sparkalog_store* st, RelState& r, int l, const u64* a, u64 na, const u64* b, u64 nb,
                      cudaStream_t s, u64* launches) {
     const u64 n = na + nb;
@@ -529,12 +547,21 @@ int merge_into_level(sparkalog_store* st, RelState& r, int l, const u64* a, u64 
     directory_shape(st, n, &shift, &buckets);
     SPK_CUDA(r.dir[l].ensure((buckets + 1) * 4, s), "cudaMallocAsync");
     u64 launched = 0;
+    const bool inline_dir = n < kMergeDirectoryRows;
     SPK_CUDA(store_merge(st, a, na, b, nb, r.spare.as<u64>(), &launched,
-                         spk::MergeDirectory{r.dir[l].as<u32>(), shift, buckets}),
+                         inline_dir ? spk::MergeDirectory{r.dir[l].as<u32>(), shift, buckets}
+                                    : spk::MergeDirectory{nullptr, 0, 0}),
              "merge_bulk_kernel");
+    if (!inline_dir && n > 0) {
+        spk::level_directory_kernel<<<simple_grid(buckets + 1), 256, 0, s>>>(r.spare.as<u64>(), n, shift, buckets,
+                                                                            r.dir[l].as<u32>());
+        SPK_CUDA(cudaGetLastError(), "level_directory_kernel");
+        launched += 1;
+    }
     swap_arrays(r.level[l], r.spare);
     r.level_n[l] = n;
-    r.dir_valid[l] = launched > 0;  // a plain copy (one side empty) wrote no directory
+    // A plain copy (one side empty) of a small merge wrote no directory.
+    r.dir_valid[l] = !inline_dir || launched > 0;
     r.dir_shift[l] = shift;
     r.dir_buckets[l] = buckets;
     if (launches) *launches += launched;
@@ -666,6 +693,8 @@ struct TargetRT {
     bool force_generic = false;  // redo the current round with the general kernels
     bool fused_last = false;     // the round just applied ran the fused kernel
     DevArray anti_plan;          // merge-form anti-join tiles (spk::AntiTile)
+    DevArray anti_scratch;       // ... each tile's kept run, at its first candidate index
+    DevArray anti_counts;        // ... and its length (u32 per tile)
     double unique_per_delta = -1.0;  // last round's distinct candidates per DELTA row
 };
 
@@ -3044,6 +3073,9 @@ void sparkalog_executor_destroy(sparkalog_executor* ex) {
         t.j_b.release(s);
         t.sort.plan.release(s);
         t.sort.status.release(s);
+        t.anti_plan.release(s);
+        t.anti_scratch.release(s);
+        t.anti_counts.release(s);
     }
     for (auto& ic : ex->index) {
         ic.offsets.release(s);
@@ -3584,13 +3616,24 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                     }
                     const unsigned grid = spk::persistent_grid(reinterpret_cast<const void*>(kernel), kAntiMergeThreads,
                                                                AL::kBytes, std::max<u64>(tiles, 1));
-                    kernel<<<grid, kAntiMergeThreads, AL::kBytes, s>>>(
-                        cand, t.j_b.as<u64>(), cand_sel, jn, lv, partner, plan, tr.newt.as<u64>(),
-                        tc + t.rules.size() + 1, ex->status.as<u64>(), counters + counter_slot++, ex->epoch++, err,
-                        unique_word);
+                    SPK_CUDA(t.anti_scratch.ensure(t.j_cap * 8, s), "cudaMallocAsync");
+                    SPK_CUDA(t.anti_counts.ensure((tiles + 1) * 4, s), "cudaMallocAsync");
+                    kernel<<<grid, kAntiMergeThreads, AL::kBytes, s>>>(cand, t.j_b.as<u64>(), cand_sel, jn, lv, partner,
+                                                                       plan, t.anti_scratch.as<u64>(),
+                                                                       t.anti_counts.as<u32>(), err, unique_word);
                     SPK_CUDA(cudaGetLastError(), "anti_merge_kernel");
+                    spk::anti_merge_scan_kernel<1024, kAntiMergeTile><<<1, 1024, 0, s>>>(
+                        jn, lv, partner, t.anti_counts.as<u32>(), tc + t.rules.size() + 1);
+                    SPK_CUDA(cudaGetLastError(), "anti_merge_scan_kernel");
+                    {
+                        const u64 blocks = std::min<u64>((tiles + 7) / 8 + 1, static_cast<u64>(spk::device_sm_count()) * 8);
+                        spk::anti_merge_copy_kernel<<<static_cast<unsigned>(blocks), 256, 0, s>>>(
+                            jn, lv, partner, kAntiMergeTile, plan, t.anti_scratch.as<u64>(), t.anti_counts.as<u32>(),
+                            tr.newt.as<u64>());
+                        SPK_CUDA(cudaGetLastError(), "anti_merge_copy_kernel");
+                    }
                     anti_full[ti] = full_rows;
-                    ex->stats.total_launches += 1;
+                    ex->stats.total_launches += 3;
                 } else if (use_bloom) {
                     // The filter rules out most candidates with one sector each;
                     // the rest are searched in the levels.
@@ -3641,7 +3684,7 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                                                ex->epoch++, err, unique_word);
                     SPK_CUDA(cudaGetLastError(), "anti_join_levels_kernel");
                 }
-                ex->end(anti_t[ti], s, 0.0, use_merge_form ? 2 : 1);
+                ex->end(anti_t[ti], s, 0.0, use_merge_form ? 4 : 1);
                 ex->stats.total_launches += 1 + dir_launches;
                 if (!fused[ti])
                     SPK_CUDA(cudaMemcpyAsync(ex->host_active + ti * spk::kMaxPasses,

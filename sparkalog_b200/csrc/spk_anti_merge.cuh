@@ -138,19 +138,24 @@ enum : int {
 };
 static_assert(kAmSideLo + kAntiSides <= 16, "bookkeeping fits 16 words");
 
+// Pass 1 over the tiles, statically assigned (tile blockIdx.x + k *
+// gridDim.x), with the next tile's copies always in flight: each tile's kept
+// candidates go to scratch[j0 ..] (a tile keeps at most its j1 - j0
+// candidates) and their number to counts[tile]. No tile waits on another, so
+// nothing serialises the tiles; anti_merge_scan_kernel and
+// anti_merge_copy_kernel then pack the kept runs in tile order.
 template <int THREADS, int ITEMS, int SIDE_ROWS>
 __global__ void __launch_bounds__(THREADS) anti_merge_kernel(const u64* buf_a, const u64* buf_b, const u32* final_sel,
                                                              const u64* n_ptr, Levels levels, int partner,
-                                                             const AntiTile* plan, u64* out, u64* out_count,
-                                                             u64* status, u32* tile_counter, u32 epoch, u32* err,
-                                                             unsigned long long* unique_count) {
+                                                             const AntiTile* plan, u64* scratch, u32* counts,
+                                                             u32* err, unsigned long long* unique_count) {
     using Lay = AntiMergeLayout<THREADS, ITEMS, SIDE_ROWS>;
     constexpr int kTile = Lay::kTile;
     extern __shared__ __align__(16) unsigned char smem[];
     auto stage = [&](int st) { return reinterpret_cast<u64*>(smem + st * Lay::kStage); };
     u64* meta = reinterpret_cast<u64*>(smem + Lay::kMeta);
     unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem + Lay::kBars);
-    __shared__ CompactShared<THREADS> cs;
+    __shared__ u32 scan_scratch[THREADS / kWarp + 1];
     __shared__ int failed;
 
     const u64* C = (final_sel && *final_sel) ? buf_b : buf_a;
@@ -158,10 +163,8 @@ __global__ void __launch_bounds__(THREADS) anti_merge_kernel(const u64* buf_a, c
     const u64* L = levels.keys[partner];
     const u64 nL = levels.count[partner];
     const u64 num_tiles = (nL + nC + kTile - 1) / kTile;
-    if (nC == 0) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) *out_count = 0;
-        return;
-    }
+    const u64 first_tile = blockIdx.x;
+    if (nC == 0 || first_tile >= num_tiles) return;
     if (threadIdx.x == 0) {
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
@@ -170,14 +173,9 @@ __global__ void __launch_bounds__(THREADS) anti_merge_kernel(const u64* buf_a, c
     }
     __syncthreads();
 
-    // Thread 0: claims the next tile and issues its copies into stage st
-    // (meta[kAmTile] = num_tiles when none is left).
-    auto claim_and_issue = [&](int st) -> bool {
+    // Thread 0: the copies of tile t (plan entry p) into stage st.
+    auto issue = [&](u64 t, const AntiTile& p, int st) {
         u64* m = meta + st * Lay::kMetaWords;
-        const u64 t = atomicAdd(tile_counter, 1u);
-        m[kAmTile] = t;
-        if (t >= num_tiles) return false;
-        const AntiTile& p = plan[t];
         const u64 i0 = p.i0, i1 = p.i1, j0 = p.j0, j1 = p.j1;
         u64* base = stage(st);
         u32 bytes = 0;
@@ -190,6 +188,7 @@ __global__ void __launch_bounds__(THREADS) anti_merge_kernel(const u64* buf_a, c
         const u64 cs0 = j0 > 0 ? j0 - 1 : 0;
         const u64 c_lead = (reinterpret_cast<uintptr_t>(C + cs0) >> 3) & 1;
         const u32 c_rows = j1 > cs0 ? static_cast<u32>((c_lead + j1 - cs0 + 1) & ~1ull) : 0u;
+        m[kAmTile] = t;
         m[kAmLOff] = l_lead + (i0 - ls);
         m[kAmLCount] = i1 - i0;
         m[kAmCOff] = l_rows + c_lead + (j0 - cs0);
@@ -199,7 +198,7 @@ __global__ void __launch_bounds__(THREADS) anti_merge_kernel(const u64* buf_a, c
         bytes += (l_rows + c_rows) * 8u;
         u32 side_used = 0;
         u32 side_rows[kAntiSides];
-        u64 side_src[kAntiSides];
+        const u64* side_src[kAntiSides];
 #pragma unroll
         for (int s = 0; s < kAntiSides; ++s) {
             const int l = anti_side_level(partner, s);
@@ -208,18 +207,16 @@ __global__ void __launch_bounds__(THREADS) anti_merge_kernel(const u64* buf_a, c
             m[kAmSideLo + s] = lo;
             m[kAmSideCount + s] = cnt;
             side_rows[s] = 0;
-            side_src[s] = 0;
-            if (cnt == 0) {
-                m[kAmSideOff + s] = 0;
-                continue;
-            }
+            side_src[s] = nullptr;
+            m[kAmSideOff + s] = 0;
+            if (cnt == 0) continue;
             const u64* src = levels.keys[l] + lo;
             const u64 lead = (reinterpret_cast<uintptr_t>(src) >> 3) & 1;
             const u64 rows = (lead + cnt + 1) & ~1ull;
             if (side_used + rows <= static_cast<u64>(Lay::kSideRows)) {
                 m[kAmSideOff + s] = Lay::kMainRows + side_used + lead;
                 side_rows[s] = static_cast<u32>(rows);
-                side_src[s] = reinterpret_cast<u64>(src - lead);
+                side_src[s] = src - lead;
                 side_used += static_cast<u32>(rows);
                 bytes += static_cast<u32>(rows) * 8u;
             } else {
@@ -233,23 +230,30 @@ __global__ void __launch_bounds__(THREADS) anti_merge_kernel(const u64* buf_a, c
 #pragma unroll
         for (int s = 0; s < kAntiSides; ++s) {
             if (side_rows[s]) {
-                bulk_load(base + at, reinterpret_cast<const u64*>(side_src[s]), side_rows[s] * 8u, &bars[st]);
+                bulk_load(base + at, side_src[s], side_rows[s] * 8u, &bars[st]);
                 at += side_rows[s];
             }
         }
-        return true;
     };
 
-    u32 parity = 0, pending = 0;
-    if (threadIdx.x == 0 && claim_and_issue(0)) pending |= 1u;
-    __syncthreads();
-    for (int k = 0;; ++k) {
+    // Thread 0 keeps the plan entry of the tile after next in registers, so
+    // the issue of the next tile never waits on a plan load.
+    const u64 stride = gridDim.x;
+    AntiTile ahead{};
+    if (threadIdx.x == 0) {
+        issue(first_tile, plan[first_tile], 0);
+        if (first_tile + stride < num_tiles) ahead = plan[first_tile + stride];
+    }
+    u32 parity = 0, pending = 1;
+    int k = 0;
+    u32 unique_tally = 0;
+    for (u64 tile = first_tile; tile < num_tiles; tile += stride, ++k) {
         const int st = k & 1;
-        const u64* m = meta + st * Lay::kMetaWords;
-        const u64 tile = m[kAmTile];
-        if (tile >= num_tiles) break;
-        // The next tile's copies go out while this one is processed.
-        if (threadIdx.x == 0 && claim_and_issue(st ^ 1)) pending |= 1u << (st ^ 1);
+        if (threadIdx.x == 0 && tile + stride < num_tiles) {
+            issue(tile + stride, ahead, st ^ 1);
+            pending |= 1u << (st ^ 1);
+            if (tile + 2 * stride < num_tiles) ahead = plan[tile + 2 * stride];
+        }
         if (mbar_wait(&bars[st], (parity >> st) & 1u)) {
             parity ^= 1u << st;
             pending &= ~(1u << st);
@@ -257,11 +261,13 @@ __global__ void __launch_bounds__(THREADS) anti_merge_kernel(const u64* buf_a, c
             atomicOr(err, kErrBarrierTimeout);
             failed = 1;
         }
+        const u64* m = meta + st * Lay::kMetaWords;
         const u64* S = stage(st);
         const u32 nLs = static_cast<u32>(m[kAmLCount]), nCs = static_cast<u32>(m[kAmCCount]);
         const u64* Ls = S + m[kAmLOff];
         const u64* Cs = S + m[kAmCOff];
         const bool has_l_prev = m[kAmI0] > 0, has_c_prev = m[kAmJ0] > 0;
+        const u64 j0 = m[kAmJ0];
 
         const u32 p0 = threadIdx.x * ITEMS;
         u64 v[ITEMS];
@@ -281,7 +287,7 @@ __global__ void __launch_bounds__(THREADS) anti_merge_kernel(const u64* buf_a, c
                 }
             }
         }
-        count_unique(keep, unique_count);
+        unique_tally += __popc(keep);
         if (keep) {
             // Partner slice: one search for the first kept candidate, then
             // galloping forward (the candidates are sorted).
@@ -303,14 +309,17 @@ __global__ void __launch_bounds__(THREADS) anti_merge_kernel(const u64* buf_a, c
             const u64 cnt = m[kAmSideCount + s];
             if (!keep || cnt == 0) continue;
             const u64 off = m[kAmSideOff + s];
+            // One search for the first kept candidate, galloping after it.
             if (off != ~0ull) {
                 const u64* ss = S + off;
                 const SmemKeys sk{ss};
                 u64 cur = 0;
+                bool started = false;
 #pragma unroll
                 for (int i = 0; i < ITEMS; ++i) {
                     if (keep & (1u << i)) {
-                        cur = gallop_lower_bound(sk, cur, cnt, v[i]);
+                        cur = started ? gallop_lower_bound(sk, cur, cnt, v[i]) : lower_bound_keys(sk, 0, cnt, v[i]);
+                        started = true;
                         if (cur < cnt && ss[cur] == v[i]) keep &= ~(1u << i);
                     }
                 }
@@ -318,36 +327,83 @@ __global__ void __launch_bounds__(THREADS) anti_merge_kernel(const u64* buf_a, c
                 const u64 lo = m[kAmSideLo + s];
                 const PackedKeys gk{levels.keys[anti_side_level(partner, s)]};
                 u64 cur = lo;
+                bool started = false;
 #pragma unroll
                 for (int i = 0; i < ITEMS; ++i) {
                     if (keep & (1u << i)) {
-                        cur = gallop_lower_bound(gk, cur, lo + cnt, v[i]);
+                        cur = started ? gallop_lower_bound(gk, cur, lo + cnt, v[i])
+                                      : lower_bound_keys(gk, lo, lo + cnt, v[i]);
+                        started = true;
                         if (cur < lo + cnt && gk(cur) == v[i]) keep &= ~(1u << i);
                     }
                 }
             }
         }
-        u32 excl, total;
-        const u64 off = compact_offsets<THREADS>(__popc(keep), &excl, &total, tile, status, epoch, err, cs);
-        // Every read of the stage is done (compact_offsets synchronises):
-        // stage the kept rows in place, then store them coalesced.
+        u32 total;
+        const u32 excl = block_exclusive_scan<THREADS>(static_cast<u32>(__popc(keep)), scan_scratch, &total);
+        // The block scan synchronised: every read of the stage is done.
+        // Stage the kept rows in place, then store them coalesced.
         u64* outs = const_cast<u64*>(Cs);
         u32 wpos = excl;
 #pragma unroll
         for (int i = 0; i < ITEMS; ++i)
             if (keep & (1u << i)) outs[wpos++] = v[i];
         __syncthreads();
-        for (u32 j = threadIdx.x; j < total; j += THREADS) out[off + j] = outs[j];
-        if (tile == num_tiles - 1 && threadIdx.x == 0) *out_count = off + total;
+        for (u32 j = threadIdx.x; j < total; j += THREADS) scratch[j0 + j] = outs[j];
+        if (threadIdx.x == 0) counts[tile] = total;
         // The stage's generic accesses come before the bulk copies that refill it.
         fence_async_shared();
         __syncthreads();
         if (failed) break;
     }
+    flush_unique(unique_tally, unique_count);
     if (threadIdx.x == 0) {
         // After a timeout, copies may still be in flight into shared memory.
         for (int st = 0; st < 2; ++st)
             if ((pending >> st) & 1u) mbar_wait(&bars[st], (parity >> st) & 1u);
+    }
+}
+
+// Pass 2: the tiles' kept counts turned into NEWT offsets in place (an
+// exclusive scan; counts[num_tiles] receives the total, which is also NEWT's
+// size). One CTA: a fixpoint round has at most about a hundred thousand
+// tiles, and each thread sums a contiguous run of them.
+template <int THREADS, int TILE>
+__global__ void __launch_bounds__(THREADS) anti_merge_scan_kernel(const u64* n_ptr, Levels levels, int partner,
+                                                                  u32* counts, u64* out_count) {
+    __shared__ u32 scratch[THREADS / kWarp + 1];
+    const u64 nC = *n_ptr;
+    const u64 num_tiles = nC == 0 ? 0 : (levels.count[partner] + nC + TILE - 1) / TILE;
+    const u64 per = (num_tiles + THREADS - 1) / THREADS;
+    const u64 b = threadIdx.x * per;
+    const u64 e = b + per < num_tiles ? b + per : num_tiles;
+    u32 sum = 0;
+    for (u64 t = b; t < e; ++t) sum += counts[t];
+    u32 total;
+    u32 run = block_exclusive_scan<THREADS>(sum, scratch, &total);
+    for (u64 t = b; t < e; ++t) {
+        const u32 c = counts[t];
+        counts[t] = run;
+        run += c;
+    }
+    if (threadIdx.x == 0) {
+        counts[num_tiles] = total;
+        *out_count = total;
+    }
+}
+
+// Pass 3: each tile's kept run copied to its NEWT offset (a warp per tile).
+static __global__ void anti_merge_copy_kernel(const u64* n_ptr, Levels levels, int partner, u32 tile_rows,
+                                              const AntiTile* plan, const u64* scratch, const u32* offsets,
+                                              u64* out) {
+    const u64 nC = *n_ptr;
+    const u64 num_tiles = nC == 0 ? 0 : (levels.count[partner] + nC + tile_rows - 1) / tile_rows;
+    const u64 warps = static_cast<u64>(gridDim.x) * (blockDim.x / kWarp);
+    for (u64 t = static_cast<u64>(blockIdx.x) * (blockDim.x / kWarp) + warp_id(); t < num_tiles; t += warps) {
+        const u32 o = offsets[t], n = offsets[t + 1] - o;
+        const u64* src = scratch + plan[t].j0;
+        u64* dst = out + o;
+        for (u32 j = lane_id(); j < n; j += kWarp) dst[j] = src[j];
     }
 }
 

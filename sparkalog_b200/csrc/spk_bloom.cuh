@@ -94,6 +94,7 @@ __device__ __forceinline__ void anti_join_bloom(const u64* buf_a, const u64* buf
         if (blockIdx.x == 0 && threadIdx.x == 0) *out_count = 0;
         return;
     }
+    u32 unique_tally = 0;
     for (;;) {
         if (threadIdx.x == 0) cs.tile = atomicAdd(tile_counter, 1u);
         __syncthreads();
@@ -114,7 +115,7 @@ __device__ __forceinline__ void anti_join_bloom(const u64* buf_a, const u64* buf
                 prev = k;
             }
         }
-        count_unique(keep, unique_count);
+        unique_tally += __popc(keep);
         u32 maybe = 0;
 #pragma unroll
         for (int i = 0; i < ITEMS; ++i)
@@ -183,6 +184,7 @@ __device__ __forceinline__ void anti_join_bloom(const u64* buf_a, const u64* buf
         if (tile == num_tiles - 1 && threadIdx.x == 0) *out_count = off + total;
         __syncthreads();
     }
+    flush_unique(unique_tally, unique_count);
 }
 
 template <int THREADS, int ITEMS>

@@ -73,11 +73,14 @@ static __global__ void level_directory_kernel(const u64* keys, u64 n, u32 shift,
 // decoupled look-back, so NEWT stays sorted.
 constexpr u64 kStreamChunks = 2;
 
-// Adds the rows a warp keeps after the unique step (BinaryDistinct's output
-// size) to *unique_count, when given. Called by every thread.
-__device__ __forceinline__ void count_unique(u32 keep, unsigned long long* unique_count) {
+// The rows kept after the unique step (BinaryDistinct's output size): each
+// thread sums its own over all its tiles, and when the kernel ends every
+// warp adds its sum to *unique_count (when given) with one atomic. (One
+// atomic per warp per tile on the single counter serialised whole launches.)
+// Called by every thread.
+__device__ __forceinline__ void flush_unique(u32 tally, unsigned long long* unique_count) {
     if (!unique_count) return;
-    const u32 c = __reduce_add_sync(0xffffffffu, static_cast<u32>(__popc(keep)));
+    const u32 c = __reduce_add_sync(0xffffffffu, tally);
     if (lane_id() == 0 && c) atomicAdd(unique_count, static_cast<unsigned long long>(c));
 }
 
@@ -115,6 +118,7 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_kernel(const u64* bu
         if (blockIdx.x == 0 && threadIdx.x == 0) *out_count = 0;
         return;
     }
+    u32 unique_tally = 0;
     for (;;) {
         if (threadIdx.x == 0) cs.tile = atomicAdd(tile_counter, 1u);
         __syncthreads();
@@ -138,7 +142,7 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_kernel(const u64* bu
                 prev = k;
             }
         }
-        count_unique(keep, unique_count);
+        unique_tally += __popc(keep);
         __syncthreads();
         for (int l = 0; l < levels.n; ++l) {
             const u64 lo = range_lo[l];
@@ -229,6 +233,7 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_kernel(const u64* bu
         if (tile == num_tiles - 1 && threadIdx.x == 0) *out_count = off + total;
         __syncthreads();
     }
+    flush_unique(unique_tally, unique_count);
 }
 
 // The same anti-join for small candidate sets, whose keys lie far apart in
@@ -251,6 +256,7 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_sparse_kernel(const 
         if (blockIdx.x == 0 && threadIdx.x == 0) *out_count = 0;
         return;
     }
+    u32 unique_tally = 0;
     for (;;) {
         if (threadIdx.x == 0) cs.tile = atomicAdd(tile_counter, 1u);
         __syncthreads();
@@ -271,7 +277,7 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_sparse_kernel(const 
                 prev = k;
             }
         }
-        count_unique(keep, unique_count);
+        unique_tally += __popc(keep);
         u64 pos[kMaxLevels][ITEMS];
         u32 span[kMaxLevels][ITEMS], bucket[kMaxLevels][ITEMS];
         u32 max_span = 0;
@@ -327,6 +333,7 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_sparse_kernel(const 
         if (tile == num_tiles - 1 && threadIdx.x == 0) *out_count = off + total;
         __syncthreads();
     }
+    flush_unique(unique_tally, unique_count);
 }
 
 // The same anti-join for a handful of candidates (the last rounds of a
@@ -357,6 +364,7 @@ __device__ __forceinline__ void anti_join_group(const u64* buf_a, const u64* buf
     }
     const u32 lane = threadIdx.x % G;
     const u32 group_mask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << (lane_id() / G * G);
+    u32 unique_tally = 0;
     for (;;) {
         if (threadIdx.x == 0) cs.tile = atomicAdd(tile_counter, 1u);
         __syncthreads();
@@ -369,7 +377,7 @@ __device__ __forceinline__ void anti_join_group(const u64* buf_a, const u64* buf
             v = keys[idx];
             keep = idx == 0 || keys[idx - 1] != v;
         }
-        count_unique(lane == 0 && keep ? 1u : 0u, unique_count);
+        unique_tally += (lane == 0 && keep) ? 1u : 0u;
         // [lo, hi): the rows of v's bucket in each level; a row equal to v
         // can only lie there.
         u64 lo[kMaxLevels], hi[kMaxLevels];
@@ -424,6 +432,7 @@ __device__ __forceinline__ void anti_join_group(const u64* buf_a, const u64* buf
         if (tile == num_tiles - 1 && threadIdx.x == 0) *out_count = off + total;
         __syncthreads();
     }
+    flush_unique(unique_tally, unique_count);
 }
 
 template <int THREADS, int G>
@@ -675,6 +684,26 @@ static __global__ void merge_split_kernel(const u64* a, u64 na, const u64* b, u6
     merge_splits(a, na, b, nb, tile, tiles, splits);
 }
 
+// The same splits with one thread per diagonal and a plain binary search:
+// more dependent loads per diagonal than the warp search, but one sector per
+// step instead of 32, which wins once there are tens of thousands of
+// diagonals (a large merge) and the searches' sector traffic dominates.
+static __global__ void merge_split_thread_kernel(const u64* a, u64 na, const u64* b, u64 nb, u32 tile, u64 tiles,
+                                                 u64* splits) {
+    const u64 total = na + nb;
+    const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+    for (u64 t = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; t <= tiles; t += stride) {
+        const u64 d = t * tile < total ? t * tile : total;
+        u64 lo = d > nb ? d - nb : 0, hi = d < na ? d : na;
+        while (lo < hi) {
+            const u64 mid = (lo + hi) >> 1;
+            if (b[d - 1 - mid] >= a[mid]) lo = mid + 1;
+            else hi = mid;
+        }
+        splits[t] = lo;
+    }
+}
+
 // Shared-memory layout of merge_bulk_kernel: two input stages (a's slice,
 // then b's slice at the next 16-byte boundary, each with up to one leading
 // row of alignment slack), the output tile, per-stage slice bounds and the
@@ -757,7 +786,16 @@ __device__ __forceinline__ void merge_bulk(const u64* a, u64 na, const u64* b, u
         if (b_rows) bulk_load(in_s(st) + a_rows, b + (j0 - b_lead), b_rows * 8u, &bars[st]);
     };
 
-    if (threadIdx.x == 0) issue(t_begin, 0);
+    if (threadIdx.x == 0) {
+        issue(t_begin, 0);
+        // The row before the chunk's first output row (the directory needs
+        // its bucket); each later tile takes its predecessor's last row.
+        if (md.dir && t_begin > 0) {
+            const u64 i0 = splits[t_begin], j0 = t_begin * kTile - i0;
+            const u64 pa = i0 > 0 ? a[i0 - 1] : 0, pb = j0 > 0 ? b[j0 - 1] : 0;
+            before_tile = i0 == 0 ? pb : (j0 == 0 ? pa : (pa > pb ? pa : pb));
+        }
+    }
     u32 parity = 0;   // bit st: the phase parity stage st waits for next
     u32 pending = 1;  // bit st: stage st's copies were issued and not yet waited for
     for (u64 t = t_begin, k = 0; t < t_end; ++t, ++k) {
@@ -780,10 +818,6 @@ __device__ __forceinline__ void merge_bulk(const u64* a, u64 na, const u64* b, u
         const u64 i0 = m[0], j0 = m[2];
         const u32 sa_n = static_cast<u32>(m[1] - i0), sb_n = static_cast<u32>(m[3] - j0);
         const SmemKeys sa{in_s(st) + m[4]}, sb{in_s(st) + m[5] + m[6]};
-        if (md.dir && threadIdx.x == 0 && d0 > 0) {
-            const u64 pa = i0 > 0 ? a[i0 - 1] : 0, pb = j0 > 0 ? b[j0 - 1] : 0;
-            before_tile = i0 == 0 ? pb : (j0 == 0 ? pa : (pa > pb ? pa : pb));
-        }
         const u32 diag = threadIdx.x * ITEMS;
         u64 v[ITEMS];
         if (diag < len) {
@@ -816,18 +850,39 @@ __device__ __forceinline__ void merge_bulk(const u64* a, u64 na, const u64* b, u
         } else {
             for (u32 j = threadIdx.x; j < len; j += THREADS) out[d0 + j] = out_s[j];
         }
-        if (md.dir) {
-            for (u32 j = threadIdx.x; j < len; j += THREADS) {
-                const u64 o = d0 + j;
-                const u64 bucket = out_s[j] >> md.shift;
-                u64 from = 0;
-                if (o > 0) from = ((j > 0 ? out_s[j - 1] : before_tile) >> md.shift) + 1;
-                for (u64 e = from; e <= bucket && e <= md.buckets; ++e) md.dir[e] = static_cast<u32>(o);
-                if (o == total - 1)
-                    for (u64 e = bucket + 1; e <= md.buckets; ++e) md.dir[e] = static_cast<u32>(total);
+        if (md.dir && diag < len) {
+            // This thread's rows are v[0 .. ITEMS) at outputs d0 + diag + i,
+            // after the previous thread's last row (or the previous tile's).
+            // Usually no bucket starts among them: one comparison decides.
+            const u64 o0 = d0 + diag;
+            u64 last = v[0];
+            u32 cnt = 0;
+#pragma unroll
+            for (int i = 0; i < ITEMS; ++i)
+                if (diag + i < len) {
+                    last = v[i];
+                    cnt = i + 1;
+                }
+            const u64 prev0 = diag > 0 ? out_s[diag - 1] : before_tile;
+            const u64 first_bucket = o0 == 0 ? 0 : (prev0 >> md.shift) + 1;
+            if (first_bucket <= (last >> md.shift) || o0 + cnt == total) {
+                u64 prev = prev0;
+#pragma unroll
+                for (int i = 0; i < ITEMS; ++i) {
+                    if (diag + i < len) {
+                        const u64 o = o0 + i;
+                        const u64 bucket = v[i] >> md.shift;
+                        const u64 from = o > 0 ? (prev >> md.shift) + 1 : 0;
+                        for (u64 e = from; e <= bucket && e <= md.buckets; ++e) md.dir[e] = static_cast<u32>(o);
+                        if (o == total - 1)
+                            for (u64 e = bucket + 1; e <= md.buckets; ++e) md.dir[e] = static_cast<u32>(total);
+                        prev = v[i];
+                    }
+                }
             }
         }
         __syncthreads();
+        if (md.dir && threadIdx.x == 0) before_tile = out_s[len - 1];
         if (failed) break;
     }
     if (threadIdx.x == 0) {

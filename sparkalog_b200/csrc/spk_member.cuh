@@ -117,6 +117,7 @@ __global__ void __launch_bounds__(THREADS) anti_join_member_kernel(const u64* bu
         return;
     }
     const bool empty_key_member = *set.has_empty_key != 0;
+    u32 unique_tally = 0;
     for (;;) {
         if (threadIdx.x == 0) cs.tile = atomicAdd(tile_counter, 1u);
         __syncthreads();
@@ -137,7 +138,7 @@ __global__ void __launch_bounds__(THREADS) anti_join_member_kernel(const u64* bu
                 prev = k;
             }
         }
-        count_unique(keep, unique_count);
+        unique_tally += __popc(keep);
         ulonglong2 lo[ITEMS], hi[ITEMS];
         u64 group[ITEMS];
 #pragma unroll
@@ -174,6 +175,7 @@ __global__ void __launch_bounds__(THREADS) anti_join_member_kernel(const u64* bu
         if (tile == num_tiles - 1 && threadIdx.x == 0) *out_count = off + total;
         __syncthreads();
     }
+    flush_unique(unique_tally, unique_count);
 }
 
 }  // namespace spk

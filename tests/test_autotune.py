@@ -7,7 +7,7 @@ from sparkalog_b200 import autotune
 
 START = {"dir_rows_log2": 6, "group_lanes": 8, "group_candidates": 1 << 17, "sparse_candidates": 1 << 26,
          "fused_rows_cap": 672, "level_ratio": 4, "levels": 3, "merge_items": 11, "bloom_bits": 0,
-         "merge_anti_ratio": 32}
+         "merge_anti_ratio": 0}
 
 
 def bowl(target):
