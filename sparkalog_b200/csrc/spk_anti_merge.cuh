@@ -269,38 +269,43 @@ __global__ void __launch_bounds__(THREADS) anti_merge_kernel(const u64* buf_a, c
         const bool has_l_prev = m[kAmI0] > 0, has_c_prev = m[kAmJ0] > 0;
         const u64 j0 = m[kAmJ0];
 
-        const u32 p0 = threadIdx.x * ITEMS;
+        // Each thread walks ITEMS consecutive rows of the tile's merged order
+        // (partner rows first on equal keys), from its merge-path split. A
+        // candidate is a member of the partner level exactly when the last
+        // partner row before it equals it, and a repeat when the last
+        // candidate before it does; the rows just ahead of the tile (one of
+        // each, loaded with the slices) seed both for the first thread.
+        const u32 len = nLs + nCs;
+        const u32 diag = threadIdx.x * ITEMS;
         u64 v[ITEMS];
         u32 keep = 0;
-        {
-            u64 prev = (p0 > 0 && p0 - 1 < nCs) ? Cs[p0 - 1] : (has_c_prev ? Cs[-1] : 0);
-            const bool prev_ok = p0 > 0 || has_c_prev;
+        if (diag < len) {
+            const SmemKeys lk{Ls}, ck{Cs};
+            u32 ia = static_cast<u32>(merge_path(lk, nLs, ck, nCs, diag));
+            u32 ib = diag - ia;
+            bool l_ok = ia > 0 || has_l_prev, c_ok = ib > 0 || has_c_prev;
+            u64 last_l = l_ok ? Ls[static_cast<int>(ia) - 1] : 0;
+            u64 last_c = c_ok ? Cs[static_cast<int>(ib) - 1] : 0;
 #pragma unroll
             for (int i = 0; i < ITEMS; ++i) {
-                const u32 p = p0 + i;
                 v[i] = 0;
-                if (p < nCs) {
-                    const u64 key = Cs[p];
-                    v[i] = key;
-                    if ((i > 0 || prev_ok) ? key != prev : true) keep |= 1u << i;
-                    prev = key;
-                }
-            }
-        }
-        unique_tally += __popc(keep);
-        if (keep) {
-            // Partner slice: one search for the first kept candidate, then
-            // galloping forward (the candidates are sorted).
-            const SmemKeys lk{Ls};
-            u64 cur = 0;
-            bool started = false;
-#pragma unroll
-            for (int i = 0; i < ITEMS; ++i) {
-                if (keep & (1u << i)) {
-                    cur = started ? gallop_lower_bound(lk, cur, nLs, v[i]) : lower_bound_keys(lk, 0, nLs, v[i]);
-                    started = true;
-                    if ((cur < nLs && Ls[cur] == v[i]) || (p0 + i == 0 && has_l_prev && Ls[-1] == v[i]))
-                        keep &= ~(1u << i);
+                if (diag + i < len) {
+                    if (ib >= nCs || (ia < nLs && Ls[ia] <= Cs[ib])) {
+                        last_l = Ls[ia++];
+                        l_ok = true;
+                    } else {
+                        const u64 c = Cs[ib++];
+                        const bool repeat = c_ok && c == last_c;
+                        if (!repeat) {
+                            ++unique_tally;
+                            if (!(l_ok && c == last_l)) {
+                                keep |= 1u << i;
+                                v[i] = c;
+                            }
+                        }
+                        last_c = c;
+                        c_ok = true;
+                    }
                 }
             }
         }

@@ -217,6 +217,9 @@ __device__ __forceinline__ void fused_round(const FusedRoundArgs& a) {
         if (blockIdx.x == 0 && threadIdx.x == 0) *a.out_count = 0;
         return;
     }
+    // Join rows of this CTA's tiles (thread 0), added to the total once at
+    // the end: an atomic per tile on the one counter serialised the tiles.
+    unsigned long long join_tally = 0;
     for (;;) {
         if (threadIdx.x == 0) tile_shared = atomicAdd(a.tile_counter, 1u);
         __syncthreads();
@@ -327,7 +330,7 @@ __device__ __forceinline__ void fused_round(const FusedRoundArgs& a) {
         }
         if (threadIdx.x == 0) {
             run_off[runs < ROWCAP ? runs : ROWCAP] = total;
-            if (ok && total) atomicAdd(a.join_rows, static_cast<unsigned long long>(total));
+            if (ok) join_tally += total;
             if (!ok) atomicOr(a.fallback, 1u);
             // Publish the tile's output size now: successors resolve their
             // offsets while this tile still orders its rows.
@@ -398,6 +401,7 @@ __device__ __forceinline__ void fused_round(const FusedRoundArgs& a) {
         if (tile == num_tiles - 1 && threadIdx.x == 0) *a.out_count = base + total;
         __syncthreads();
     }
+    if (threadIdx.x == 0 && join_tally) atomicAdd(a.join_rows, join_tally);
 }
 
 template <int THREADS, int CAP, int ROWCAP>
