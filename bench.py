@@ -61,42 +61,40 @@ DIGEST_KEYS = {"er_16m_14_68m": "er_16m"}
 L2_NOTE = "inputs larger than L2 (FULL ~1 GB, candidates ~100 MB per round)"
 
 
-# DRAM traffic measured by ncu for one fixpoint of a smaller graph of the same
-# family (a summary table: kernel, launches, total ms, read GB, write GB, ...);
-# scaled to this run by derived tuples.
-TRAFFIC_PROFILE = ROOT / "profiles" / "traffic_tc_er4m.txt"
+# DRAM traffic of the fixpoint's kernels measured by ncu on launches of this
+# workload (a summary table: kernel, round, algorithmic MB, read MB, write MB),
+# turned into traffic per algorithmic byte for each kernel class.
+TRAFFIC_PROFILE = ROOT / "profiles" / "traffic_tc_er16m.txt"
 CLASS_KERNELS = {
-    "anti_join": ("anti_join_levels_kernel", "anti_join_levels_sparse_kernel", "anti_join_member_kernel"),
+    "anti_join": ("anti_join_levels_kernel", "anti_join_levels_sparse_kernel", "anti_join_levels_wide_kernel",
+                  "anti_join_member_kernel", "anti_join_bloom_kernel", "anti_merge_plan_kernel",
+                  "anti_merge_kernel", "anti_merge_scan_kernel", "anti_merge_copy_kernel"),
     "join_distinct": ("fused_join_distinct_kernel",),
-    "merge": ("merge_disjoint_kernel", "merge_partition_kernel"),
+    "merge": ("merge_bulk_kernel", "merge_split_kernel", "merge_split_thread_kernel", "level_directory_kernel"),
 }
 
 
-def profiled_traffic(kernel_class, new_rows):
-    """Per-launch DRAM bytes of a kernel class from the ncu summary, scaled by
-    derived tuples to this run; (None, reason) when there is no summary."""
-    import re
-
+def profiled_traffic(kernel_class, per_launch_bytes):
+    """DRAM bytes per launch of a kernel class: its measured traffic per
+    algorithmic byte (ncu summary) times this run's algorithmic bytes per
+    launch; (None, reason) when there is no summary for the class."""
     if not TRAFFIC_PROFILE.exists() or kernel_class not in CLASS_KERNELS:
         return None, "no ncu traffic summary for this kernel class"
-    text = TRAFFIC_PROFILE.read_text()
-    m = re.search(r"derived tuples: (\d+)", text)
-    if not m:
-        return None, "ncu traffic summary without a derived-tuple count"
-    launches, nbytes = 0, 0.0
-    for line in text.splitlines():
+    launches, algorithmic, traffic = 0, 0.0, 0.0
+    for line in TRAFFIC_PROFILE.read_text().splitlines():
         cells = [c.strip() for c in line.strip().strip("|").split("|")]
         if len(cells) < 5 or not cells[0].startswith("`"):
             continue
         name = cells[0].strip("`").split("<")[0]
         if name in CLASS_KERNELS[kernel_class]:
-            launches += int(cells[1])
-            nbytes += (float(cells[3]) + float(cells[4])) * 1e9
-    if launches == 0:
+            launches += 1
+            algorithmic += float(cells[2]) * 1e6
+            traffic += (float(cells[3]) + float(cells[4])) * 1e6
+    if launches == 0 or algorithmic <= 0:
         return None, "kernel class absent from the ncu traffic summary"
-    scale = new_rows / int(m.group(1))
-    return nbytes / launches * scale, (f"{TRAFFIC_PROFILE.relative_to(ROOT)}: {launches} launches, "
-                                       f"scaled x{scale:.2f} by derived tuples")
+    ratio = traffic / algorithmic
+    return ratio * per_launch_bytes, (f"{TRAFFIC_PROFILE.relative_to(ROOT)}: {launches} launches, "
+                                      f"{ratio:.2f} DRAM bytes per algorithmic byte")
 
 
 def pipeline_bytes(trace):
@@ -400,7 +398,7 @@ def run_ours(args):
     per_launch_ms = dom["ms"] / max(dom["launches"], 1)
     per_launch_bytes = dom["bytes"] / max(dom["launches"], 1)
     achieved = per_launch_bytes / (per_launch_ms / 1e3) / 1e9 if per_launch_ms > 0 else 0.0
-    traffic, traffic_source = profiled_traffic(dominant, float(new_rows) / max(world, 1))
+    traffic, traffic_source = profiled_traffic(dominant, per_launch_bytes)
     pipe = float(pipeline_bytes(pstats["trace"]))
     own_bytes = float(sum(v["bytes"] for v in classes.values()))
     own_gbs = own_bytes / (ms / args.steps / 1e3) / 1e9

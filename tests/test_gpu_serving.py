@@ -142,15 +142,17 @@ def test_large_pageable_reads_equal_pinned_reads(cuda):
     store.close()
 
 
-@pytest.mark.parametrize("readout,rounds", [("device", 1), ("host", 4), ("device", 8)])
-def test_laned_server_results_equal_alone(cuda, readout, rounds):
-    # Size lanes on their own streams and threads, several rounds per step
-    # (the device-driven loop), results in device or host memory: every
-    # request's rows and iteration count equal its run alone.
+@pytest.mark.parametrize("readout,rounds,batch_last", [("device", 1, False), ("host", 4, False), ("device", 8, False),
+                                                      ("device", 4, True)])
+def test_laned_server_results_equal_alone(cuda, readout, rounds, batch_last):
+    # Size lanes on their own streams and threads (the last one batched, or
+    # running its requests one at a time), several rounds per step (the
+    # device-driven loop), results in device or host memory: every request's
+    # rows and iteration count equal its run alone.
     from sparkalog_b200.serving import LanedServer, serve_laned, serve_one_at_a_time
 
     reqs = make_requests(40, 13, e_max=60_000)
-    server = LanedServer(bounds=(6_000,), readout=readout, rounds_per_step=rounds)
+    server = LanedServer(bounds=(6_000,), readout=readout, rounds_per_step=rounds, batch_last=batch_last)
     report = serve_laned(reqs, server, realtime=False)
     lanes = [len(lane.completions) for lane in server.lanes]
     server.close()

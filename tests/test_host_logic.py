@@ -92,7 +92,7 @@ def test_bench_baseline_helpers_on_cpu():
     assert g["status"] == "not run (extrapolated)" and g["seconds"] > 0.2
     trace = [{"delta_rows": 10, "join_rows": 8, "unique_rows": 8, "new_rows": 7, "full_rows": 17}]
     assert bench.pipeline_bytes(trace) > 0
-    traffic, source = bench.profiled_traffic("anti_join", 26_045_821)
+    traffic, source = bench.profiled_traffic("anti_join", 19.1e6)
     assert traffic is None or traffic > 0
 
 
