@@ -417,6 +417,7 @@ typedef struct sparkalog_tuning {
     uint32_t bloom_bits;          /* bits per FULL row of the anti-join's Bloom filter; 0: no filter (0, 4-32) */
     uint32_t merge_anti_ratio;    /* the merge-form anti-join runs while FULL rows <= ratio x the round's
                                      estimated candidates; 0: never (0-1024) */
+    uint32_t sparse_items;        /* candidates per thread of the per-thread search: 2, 3 or 4 */
 } sparkalog_tuning;
 
 /* The built-in defaults (measured on a B200). */

@@ -129,6 +129,7 @@ class TuningC(ctypes.Structure):
         ("levels", ctypes.c_uint32),
         ("bloom_bits", ctypes.c_uint32),
         ("merge_anti_ratio", ctypes.c_uint32),
+        ("sparse_items", ctypes.c_uint32),
     ]
 
     def as_dict(self) -> dict:

@@ -52,6 +52,7 @@ SPACE: dict[str, list[int]] = {
     "merge_items": [7, 11, 15],
     "bloom_bits": [0, 8, 12, 16],
     "merge_anti_ratio": [0, 8, 16, 32, 64, 128],
+    "sparse_items": [2, 3, 4],
 }
 
 

@@ -184,6 +184,7 @@ constexpr int kLevelStage = 2048;  // level rows per shared-memory chunk of the 
 constexpr int kSparseThreads = 256;  // anti-join of small candidate sets
 constexpr int kSparseItems = 4;
 constexpr int kSparseTile = kSparseThreads * kSparseItems;
+constexpr int kSparseMinTile = kSparseThreads * 2;  // the per-thread search's smallest tile (sparse_items 2)
 constexpr int kAntiMergeThreads = 256;  // merge-form anti-join: 11 merged rows per thread,
 constexpr int kAntiMergeItems = 11;     // 1,024 rows of side slices per stage
 constexpr int kAntiMergeSide = 1024;
@@ -209,6 +210,7 @@ sparkalog_tuning default_tuning() {
     t.levels = 3;
     t.bloom_bits = 0;
     t.merge_anti_ratio = 0;
+    t.sparse_items = 3;
     return t;
 }
 
@@ -217,7 +219,8 @@ bool tuning_valid(const sparkalog_tuning& t) {
     return t.dir_rows_log2 <= 10 && lanes && t.fused_rows_cap >= 64 && t.fused_rows_cap <= 768 &&
            (t.merge_items == 7 || t.merge_items == 11 || t.merge_items == 15) && t.level_ratio >= 2 && t.level_ratio <= 64 && t.levels >= 2 &&
            t.levels <= static_cast<u32>(spk::kMaxLevels) && t.group_candidates <= t.sparse_candidates &&
-           (t.bloom_bits == 0 || (t.bloom_bits >= 4 && t.bloom_bits <= 32)) && t.merge_anti_ratio <= 1024;
+           (t.bloom_bits == 0 || (t.bloom_bits >= 4 && t.bloom_bits <= 32)) && t.merge_anti_ratio <= 1024 &&
+           t.sparse_items >= 2 && t.sparse_items <= 4;
 }
 
 // A stream-ordered device allocation that only grows.
@@ -528,16 +531,8 @@ int merge_buffers(sparkalog_store* st, RelState& r, int l, u64 n, cudaStream_t s
     return 0;
 }
 
-// Merges of at least this many rows leave the merged level's directory to
-// level_directory_kernel: written inside the merge it doubled the merge's
-// time (an 84M-row merge: 0.24 ms without, 0.46 ms with), while the
-// directory kernel's per-bucket searches over the merged level take a
-// fraction of that; below it one launch less wins.
-constexpr u64 kMergeDirectoryRows = 1ull << 22;
-
 // Merges two disjoint sorted runs into level l of r (through r.spare) and
-// writes the merged level's directory: on the way when the merge is small
-// and runs a kernel, else by a directory pass after it.
+// writes the merged level's directory on the way when the merge runs a kernel.
 int merge_into_level(sparkalog_store* st, RelState& r, int l, const u64* a, u64 na, const u64* b, u64 nb,
                      cudaStream_t s, u64* launches) {
     const u64 n = na + nb;
@@ -547,21 +542,12 @@ int merge_into_level(sparkalog_store* st, RelState& r, int l, const u64* a, u64 
     directory_shape(st, n, &shift, &buckets);
     SPK_CUDA(r.dir[l].ensure((buckets + 1) * 4, s), "cudaMallocAsync");
     u64 launched = 0;
-    const bool inline_dir = n < kMergeDirectoryRows;
     SPK_CUDA(store_merge(st, a, na, b, nb, r.spare.as<u64>(), &launched,
-                         inline_dir ? spk::MergeDirectory{r.dir[l].as<u32>(), shift, buckets}
-                                    : spk::MergeDirectory{nullptr, 0, 0}),
+                         spk::MergeDirectory{r.dir[l].as<u32>(), shift, buckets}),
              "merge_bulk_kernel");
-    if (!inline_dir && n > 0) {
-        spk::level_directory_kernel<<<simple_grid(buckets + 1), 256, 0, s>>>(r.spare.as<u64>(), n, shift, buckets,
-                                                                            r.dir[l].as<u32>());
-        SPK_CUDA(cudaGetLastError(), "level_directory_kernel");
-        launched += 1;
-    }
     swap_arrays(r.level[l], r.spare);
     r.level_n[l] = n;
-    // A plain copy (one side empty) of a small merge wrote no directory.
-    r.dir_valid[l] = !inline_dir || launched > 0;
+    r.dir_valid[l] = launched > 0;  // a plain copy (one side empty) wrote no directory
     r.dir_shift[l] = shift;
     r.dir_buckets[l] = buckets;
     if (launches) *launches += launched;
@@ -3390,7 +3376,8 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                 SPK_CUDA(st->find(t.id)->newt.ensure(t.j_cap * 8, s), "cudaMallocAsync");
                 // One status word per anti-join tile (the sparse kernel's
                 // tiles are the smallest)...
-                max_status_words = std::max<size_t>(max_status_words, (t.j_cap + kSparseTile - 1) / kSparseTile + 1);
+                max_status_words =
+                    std::max<size_t>(max_status_words, (t.j_cap + kSparseMinTile - 1) / kSparseMinTile + 1);
                 // ...or the group-searched kernel's, over at most group_candidates.
                 const u64 wide = std::min<u64>(t.j_cap, ex->tuning.group_candidates);
                 const u64 wide_tile = kWideThreads / ex->tuning.group_lanes;
@@ -3668,8 +3655,18 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                 } else if (cand_bound <= ex->tuning.sparse_candidates) {
                     // Few candidates, far apart in every level: look each up
                     // in all levels at once.
-                    auto kernel = spk::anti_join_levels_sparse_kernel<kSparseThreads, kSparseItems>;
-                    const size_t tiles = (cand_bound + kSparseTile - 1) / kSparseTile;
+                    const u32 items = ex->tuning.sparse_items;
+                    const bool three = lv.n <= 3;
+                    auto kernel = three ? spk::anti_join_levels_sparse_kernel<kSparseThreads, 4, 3>
+                                        : spk::anti_join_levels_sparse_kernel<kSparseThreads, 4, 4>;
+                    if (items == 3)
+                        kernel = three ? spk::anti_join_levels_sparse_kernel<kSparseThreads, 3, 3>
+                                       : spk::anti_join_levels_sparse_kernel<kSparseThreads, 3, 4>;
+                    if (items == 2)
+                        kernel = three ? spk::anti_join_levels_sparse_kernel<kSparseThreads, 2, 3>
+                                       : spk::anti_join_levels_sparse_kernel<kSparseThreads, 2, 4>;
+                    const u64 tile_rows = static_cast<u64>(kSparseThreads) * items;
+                    const size_t tiles = (cand_bound + tile_rows - 1) / tile_rows;
                     kernel<<<grid_for(reinterpret_cast<const void*>(kernel), kSparseThreads, std::max<size_t>(tiles, 1)),
                              kSparseThreads, 0, s>>>(cand, t.j_b.as<u64>(), cand_sel, jn, lv, tr.newt.as<u64>(),
                                                      tc + t.rules.size() + 1, ex->status.as<u64>(),

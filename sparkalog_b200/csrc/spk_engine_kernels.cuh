@@ -239,8 +239,10 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_kernel(const u64* bu
 // The same anti-join for small candidate sets, whose keys lie far apart in
 // every level (the tail rounds of a fixpoint): each thread looks its ITEMS
 // candidates up in all levels at once, so a tile's dependent chain is one
-// bucket search long instead of one per level.
-template <int THREADS, int ITEMS>
+// bucket search long instead of one per level. LV (>= levels.n) sizes the
+// per-level search state: three levels instead of four, or fewer items per
+// thread, need fewer registers, so more CTAs share an SM.
+template <int THREADS, int ITEMS, int LV = kMaxLevels>
 __global__ void __launch_bounds__(THREADS) anti_join_levels_sparse_kernel(const u64* buf_a, const u64* buf_b,
                                                                           const u32* final_sel, const u64* n_ptr,
                                                                           Levels levels, u64* out, u64* out_count,
@@ -278,11 +280,11 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_sparse_kernel(const 
             }
         }
         unique_tally += __popc(keep);
-        u64 pos[kMaxLevels][ITEMS];
-        u32 span[kMaxLevels][ITEMS], bucket[kMaxLevels][ITEMS];
+        u64 pos[LV][ITEMS];
+        u32 span[LV][ITEMS], bucket[LV][ITEMS];
         u32 max_span = 0;
 #pragma unroll
-        for (int l = 0; l < kMaxLevels; ++l) {
+        for (int l = 0; l < LV; ++l) {
 #pragma unroll
             for (int i = 0; i < ITEMS; ++i) {
                 pos[l][i] = 0;
@@ -298,7 +300,7 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_sparse_kernel(const 
         }
         while (max_span > 1) {
 #pragma unroll
-            for (int l = 0; l < kMaxLevels; ++l) {
+            for (int l = 0; l < LV; ++l) {
 #pragma unroll
                 for (int i = 0; i < ITEMS; ++i) {
                     if (span[l][i] > 1) {
@@ -311,7 +313,7 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_sparse_kernel(const 
             max_span -= max_span >> 1;
         }
 #pragma unroll
-        for (int l = 0; l < kMaxLevels; ++l) {
+        for (int l = 0; l < LV; ++l) {
 #pragma unroll
             for (int i = 0; i < ITEMS; ++i) {
                 if (bucket[l][i] > 0) {
@@ -850,36 +852,18 @@ __device__ __forceinline__ void merge_bulk(const u64* a, u64 na, const u64* b, u
         } else {
             for (u32 j = threadIdx.x; j < len; j += THREADS) out[d0 + j] = out_s[j];
         }
-        if (md.dir && diag < len) {
-            // This thread's rows are v[0 .. ITEMS) at outputs d0 + diag + i,
-            // after the previous thread's last row (or the previous tile's).
-            // Usually no bucket starts among them: one comparison decides.
-            const u64 o0 = d0 + diag;
-            u64 last = v[0];
-            u32 cnt = 0;
-#pragma unroll
-            for (int i = 0; i < ITEMS; ++i)
-                if (diag + i < len) {
-                    last = v[i];
-                    cnt = i + 1;
-                }
-            const u64 prev0 = diag > 0 ? out_s[diag - 1] : before_tile;
-            const u64 first_bucket = o0 == 0 ? 0 : (prev0 >> md.shift) + 1;
-            if (first_bucket <= (last >> md.shift) || o0 + cnt == total) {
-                u64 prev = prev0;
-#pragma unroll
-                for (int i = 0; i < ITEMS; ++i) {
-                    if (diag + i < len) {
-                        const u64 o = o0 + i;
-                        const u64 bucket = v[i] >> md.shift;
-                        const u64 from = o > 0 ? (prev >> md.shift) + 1 : 0;
-                        for (u64 e = from; e <= bucket && e <= md.buckets; ++e) md.dir[e] = static_cast<u32>(o);
-                        if (o == total - 1)
-                            for (u64 e = bucket + 1; e <= md.buckets; ++e) md.dir[e] = static_cast<u32>(total);
-                        prev = v[i];
-                    }
-                }
-            }
+        if (md.dir) {
+            // The directory entries of the buckets that start in this tile:
+            // those after the previous row's bucket up to the last row's.
+            // Each is the tile position of the bucket's first key (a binary
+            // search in the staged tile), one bucket per thread.
+            const u64 b_lo = d0 == 0 ? 0 : (before_tile >> md.shift) + 1;
+            const u64 b_hi = out_s[len - 1] >> md.shift;
+            const SmemKeys ok{out_s};
+            for (u64 b = b_lo + threadIdx.x; b <= b_hi && b <= md.buckets; b += THREADS)
+                md.dir[b] = static_cast<u32>(d0 + lower_bound_keys(ok, 0, len, b << md.shift));
+            if (d0 + len == total)
+                for (u64 b = b_hi + 1 + threadIdx.x; b <= md.buckets; b += THREADS) md.dir[b] = static_cast<u32>(total);
         }
         __syncthreads();
         if (md.dir && threadIdx.x == 0) before_tile = out_s[len - 1];

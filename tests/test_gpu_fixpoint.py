@@ -433,7 +433,8 @@ TUNINGS = [
     {"level_ratio": 2, "sparse_candidates": 1 << 22, "group_candidates": 1 << 12, "fused_rows_cap": 128},
     {"bloom_bits": 8},
     {"bloom_bits": 4, "levels": 4, "group_candidates": 1 << 12},
-    {"merge_anti_ratio": 0},
+    {"merge_anti_ratio": 0, "sparse_items": 2, "levels": 4, "group_candidates": 1 << 10},
+    {"sparse_items": 3, "group_candidates": 1 << 10},
     {"merge_anti_ratio": 1024, "levels": 4, "level_ratio": 2},
     {"merge_anti_ratio": 1024, "levels": 2, "group_candidates": 1 << 10, "sparse_candidates": 1 << 12},
 ]
