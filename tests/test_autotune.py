@@ -20,7 +20,7 @@ def bowl(target):
 def test_descent_finds_the_minimum_of_a_separable_cost():
     target = {"dir_rows_log2": 2, "group_lanes": 4, "group_candidates": 1 << 19, "sparse_candidates": 1 << 24,
               "fused_rows_cap": 512, "level_ratio": 8, "levels": 4, "merge_items": 15, "bloom_bits": 12,
-              "merge_anti_ratio": 8, "sparse_items": 2}
+              "merge_anti_ratio": 4, "sparse_items": 2}
     best, cost, trials = autotune.coordinate_descent(bowl(target), START)
     assert best == target
     assert cost == 1.0
