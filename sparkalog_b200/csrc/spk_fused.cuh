@@ -43,6 +43,10 @@ struct FusedRoundArgs {
     const u32* keys32;
     const u32* rows;          // null: identity
     const u64* right;
+    // The right relation's second column alone (identity index on column 0,
+    // projecting that column): the gathers read 4-byte values from an array
+    // half the size of the rows, which L2 holds more of.
+    const u32* right_values;
     u32 v1_side;              // 0: DELTA column, 1: right column
     u32 v1_col;
     u32 v1_bits;              // significant bits of the second output column
@@ -322,6 +326,7 @@ __device__ __forceinline__ void fused_round(const FusedRoundArgs& a) {
                         rank[o] = static_cast<unsigned short>(rk - 1);
                         if (a.v1_side != 1) keys_a[o] = row;
                         else if (a.rows) cp_async_4(match_row + o, a.rows + first + k);
+                        else if (a.right_values) cp_async_4(match_row + o, a.right_values + first + k);
                         else cp_async_8(keys_a + o, a.right + first + k);
                     }
                     off += count;
@@ -348,7 +353,25 @@ __device__ __forceinline__ void fused_round(const FusedRoundArgs& a) {
             __syncthreads();
         }
         int long_run = 0;
-        {
+        if (a.v1_side == 1 && !a.rows && a.right_values) {
+            // The gathered values share keys_a's bytes: every thread reads
+            // its values before any thread writes a key.
+            constexpr int kPer = (CAP + THREADS - 1) / THREADS;
+            u32 vals[kPer];
+#pragma unroll
+            for (int i = 0; i < kPer; ++i) {
+                const u32 o = threadIdx.x + i * THREADS;
+                vals[i] = o < total ? match_row[o] : 0u;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < kPer; ++i) {
+                const u32 o = threadIdx.x + i * THREADS;
+                if (o < total) keys_a[o] = (static_cast<u64>(rank[o]) << 32) | vals[i];
+            }
+            for (u32 r = threadIdx.x; r < (ok ? runs : 0u); r += THREADS)
+                long_run |= run_off[r + 1] - run_off[r] > kRankRun ? 1 : 0;
+        } else {
             const u64* raw = (a.v1_side == 1 && a.rows) ? keys_b : keys_a;
             for (u32 o = threadIdx.x; o < total; o += THREADS)
                 keys_a[o] = (static_cast<u64>(rank[o]) << 32) | pair_col(raw[o], a.v1_col);
