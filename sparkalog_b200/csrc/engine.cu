@@ -654,7 +654,7 @@ struct IndexCache {
     u64 version = 0;
     u32 column = 0;
     DevArray offsets;   // u32[num_keys + 1] (dense index)
-    DevArray values;    // u32[n]: the second column, in row order (identity dense index)
+    u32* values_ptr = nullptr;  // u32[n] inside `offsets`: the second column in row order (identity)
     DevArray rows;      // u32[n] (empty when identity)
     bool identity = true;
     u64 num_keys = 0;
@@ -1073,8 +1073,12 @@ int build_index_impl(sparkalog_executor* ex, sparkalog_store* st, IndexCache& ic
         spk::max_run_kernel<<<simple_grid(n), 256, 0, s>>>(sorted_keys, n, maxdeg);
         SPK_CUDA(cudaGetLastError(), "max_run_kernel");
         ex->stats.total_launches += ic.identity ? 3 : 5;
+        ic.values_ptr = nullptr;
     } else {
-        SPK_CUDA(ic.offsets.ensure((ic.num_keys + 1) * 4, s), "cudaMallocAsync");
+        // An identity index keeps the second column right after the offsets.
+        const u64 off_bytes = spk::align_up((ic.num_keys + 1) * 4, 256);
+        SPK_CUDA(ic.offsets.ensure(off_bytes + (ic.identity ? n * 4 : 0), s), "cudaMallocAsync");
+        ic.values_ptr = ic.identity ? reinterpret_cast<u32*>(static_cast<char*>(ic.offsets.ptr) + off_bytes) : nullptr;
     }
     if (ic.bucketed) {
     } else if (n) {
@@ -1083,8 +1087,7 @@ int build_index_impl(sparkalog_executor* ex, sparkalog_store* st, IndexCache& ic
         SPK_CUDA(cudaGetLastError(), "dense_offsets_kernel");
         ex->stats.total_launches += ic.identity ? 1 : 3;
         if (ic.identity) {
-            SPK_CUDA(ic.values.ensure(n * 4, s), "cudaMallocAsync");
-            spk::low_words_kernel<<<simple_grid(n), 256, 0, s>>>(rows, n, ic.values.as<u32>());
+            spk::low_words_kernel<<<simple_grid(n), 256, 0, s>>>(rows, n, ic.values_ptr);
             SPK_CUDA(cudaGetLastError(), "low_words_kernel");
             ex->stats.total_launches += 1;
         }
@@ -1439,7 +1442,7 @@ int run_device_loop(sparkalog_executor* ex, sparkalog_store* st, size_t ti, u64 
     a.v1_side = p.proj_side[1];
     a.v1_col = p.proj_col[1];
     a.right_values = (ic.identity && !ic.bucketed && a.v1_side == 1 && a.v1_col == 1 && ic.num_keys)
-                         ? ic.values.as<u32>() : nullptr;
+                         ? ic.values_ptr : nullptr;
     a.v1_bits = static_cast<u32>(32 - __builtin_clz(st->max_value | 1));
     a.out = t.j_a.as<u64>();
     a.out_count = counts + 1;
@@ -2777,7 +2780,7 @@ int sparkalog_store_join(sparkalog_store* st, u32 left_id, u32 right_id, u32 lef
         rc = read_count(st, ops, ops.counts.as<u64>() + 3, &m);
         if (rc) return rc;
     }
-    for (DevArray* d : {&ic.offsets, &ic.values, &ic.rows, &ic.keys32, &ic.bucket_dir}) d->release(s);
+    for (DevArray* d : {&ic.offsets, &ic.rows, &ic.keys32, &ic.bucket_dir}) d->release(s);
     return store_sorted_unique(st, m, out_id, rows);
 }
 
@@ -3074,7 +3077,6 @@ void sparkalog_executor_destroy(sparkalog_executor* ex) {
     }
     for (auto& ic : ex->index) {
         ic.offsets.release(s);
-        ic.values.release(s);
         ic.rows.release(s);
         ic.keys32.release(s);
         ic.bucket_dir.release(s);
@@ -3542,7 +3544,7 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                     a.v1_side = p.proj_side[1];
                     a.v1_col = p.proj_col[1];
                     a.right_values = (ic.identity && !ic.bucketed && a.v1_side == 1 && a.v1_col == 1 && ic.num_keys)
-                                         ? ic.values.as<u32>() : nullptr;
+                                         ? ic.values_ptr : nullptr;
                     a.v1_bits = static_cast<u32>(32 - __builtin_clz(st->max_value | 1));
                     a.out = t.j_a.as<u64>();
                     a.out_count = jn;

@@ -379,21 +379,33 @@ __global__ void __launch_bounds__(THREADS) anti_merge_scan_kernel(const u64* n_p
     __shared__ u32 scratch[THREADS / kWarp + 1];
     const u64 nC = *n_ptr;
     const u64 num_tiles = nC == 0 ? 0 : (levels.count[partner] + nC + TILE - 1) / TILE;
-    const u64 per = (num_tiles + THREADS - 1) / THREADS;
-    const u64 b = threadIdx.x * per;
-    const u64 e = b + per < num_tiles ? b + per : num_tiles;
-    u32 sum = 0;
-    for (u64 t = b; t < e; ++t) sum += counts[t];
-    u32 total;
-    u32 run = block_exclusive_scan<THREADS>(sum, scratch, &total);
-    for (u64 t = b; t < e; ++t) {
-        const u32 c = counts[t];
-        counts[t] = run;
-        run += c;
+    // Chunks of THREADS * 16 counts: each thread loads its 16 consecutive
+    // counts at once (independent loads), the block scans the per-thread
+    // sums, and a running carry joins the chunks.
+    constexpr u64 kPer = 16;
+    u32 carry = 0;
+    for (u64 base = 0; base < num_tiles; base += THREADS * kPer) {
+        const u64 b = base + threadIdx.x * kPer;
+        u32 c[kPer];
+        u32 sum = 0;
+#pragma unroll
+        for (u64 i = 0; i < kPer; ++i) {
+            c[i] = b + i < num_tiles ? counts[b + i] : 0u;
+            sum += c[i];
+        }
+        u32 total;
+        u32 run = carry + block_exclusive_scan<THREADS>(sum, scratch, &total);
+#pragma unroll
+        for (u64 i = 0; i < kPer; ++i) {
+            if (b + i < num_tiles) counts[b + i] = run;
+            run += c[i];
+        }
+        carry += total;
+        __syncthreads();  // the scan's scratch is reused by the next chunk
     }
     if (threadIdx.x == 0) {
-        counts[num_tiles] = total;
-        *out_count = total;
+        counts[num_tiles] = carry;
+        *out_count = carry;
     }
 }
 
@@ -408,7 +420,16 @@ static __global__ void anti_merge_copy_kernel(const u64* n_ptr, Levels levels, i
         const u32 o = offsets[t], n = offsets[t + 1] - o;
         const u64* src = scratch + plan[t].j0;
         u64* dst = out + o;
-        for (u32 j = lane_id(); j < n; j += kWarp) dst[j] = src[j];
+        // Four independent loads in flight per lane before their stores.
+        for (u32 j = lane_id(); j < n; j += 4 * kWarp) {
+            u64 v[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                if (j + i * kWarp < n) v[i] = src[j + i * kWarp];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                if (j + i * kWarp < n) dst[j + i * kWarp] = v[i];
+        }
     }
 }
 
