@@ -185,8 +185,8 @@ constexpr int kSparseThreads = 256;  // anti-join of small candidate sets
 constexpr int kSparseItems = 4;
 constexpr int kSparseTile = kSparseThreads * kSparseItems;
 constexpr int kSparseMinTile = kSparseThreads * 2;  // the per-thread search's smallest tile (sparse_items 2)
-constexpr int kAntiMergeThreads = 256;  // merge-form anti-join: 11 merged rows per thread,
-constexpr int kAntiMergeItems = 11;     // 1,024 rows of side slices per stage
+constexpr int kAntiMergeThreads = 256;  // merge-form anti-join: 9 merged rows per thread,
+constexpr int kAntiMergeItems = 9;      // 1,024 rows of side slices per stage
 constexpr int kAntiMergeSide = 1024;
 constexpr int kAntiMergeTile = kAntiMergeThreads * kAntiMergeItems;
 constexpr int kWideThreads = 256;    // group-searched anti-join (lanes per candidate: tuning.group_lanes)

@@ -236,13 +236,23 @@ __global__ void __launch_bounds__(THREADS) anti_merge_kernel(const u64* buf_a, c
         }
     };
 
-    // Thread 0 keeps the plan entry of the tile after next in registers, so
-    // the issue of the next tile never waits on a plan load.
+    // Thread 0 fetches the plan entry of the tile after next into shared
+    // memory with asynchronous copies (plan_buf[(k + 1) & 1] holds the next
+    // tile's at iteration k), so the issue of the next tile never waits on a
+    // plan load and no thread holds a plan entry in registers.
     const u64 stride = gridDim.x;
-    AntiTile ahead{};
+    __shared__ __align__(16) AntiTile plan_buf[2];
+    static_assert(sizeof(AntiTile) % 16 == 0, "plan entries move in 16-byte pieces");
+    auto fetch_plan = [&](u64 t, int slot) {
+        const char* src = reinterpret_cast<const char*>(plan + t);
+        char* dst = reinterpret_cast<char*>(&plan_buf[slot]);
+#pragma unroll
+        for (int i = 0; i < static_cast<int>(sizeof(AntiTile) / 16); ++i) cp_async_16(dst + 16 * i, src + 16 * i);
+        cp_async_commit();
+    };
     if (threadIdx.x == 0) {
         issue(first_tile, plan[first_tile], 0);
-        if (first_tile + stride < num_tiles) ahead = plan[first_tile + stride];
+        if (first_tile + stride < num_tiles) fetch_plan(first_tile + stride, 1);
     }
     u32 parity = 0, pending = 1;
     int k = 0;
@@ -250,9 +260,10 @@ __global__ void __launch_bounds__(THREADS) anti_merge_kernel(const u64* buf_a, c
     for (u64 tile = first_tile; tile < num_tiles; tile += stride, ++k) {
         const int st = k & 1;
         if (threadIdx.x == 0 && tile + stride < num_tiles) {
-            issue(tile + stride, ahead, st ^ 1);
+            cp_async_wait<0>();
+            issue(tile + stride, plan_buf[(k + 1) & 1], st ^ 1);
             pending |= 1u << (st ^ 1);
-            if (tile + 2 * stride < num_tiles) ahead = plan[tile + 2 * stride];
+            if (tile + 2 * stride < num_tiles) fetch_plan(tile + 2 * stride, k & 1);
         }
         if (mbar_wait(&bars[st], (parity >> st) & 1u)) {
             parity ^= 1u << st;
@@ -280,23 +291,38 @@ __global__ void __launch_bounds__(THREADS) anti_merge_kernel(const u64* buf_a, c
         u64 v[ITEMS];
         u32 keep = 0;
         if (diag < len) {
-            const SmemKeys lk{Ls}, ck{Cs};
-            u32 ia = static_cast<u32>(merge_path(lk, nLs, ck, nCs, diag));
-            u32 ib = diag - ia;
+            // Merge-path split of this thread's diagonal (32-bit indices).
+            u32 ia, ib;
+            {
+                u32 lo = diag > nCs ? diag - nCs : 0u, hi = diag < nLs ? diag : nLs;
+                while (lo < hi) {
+                    const u32 mid = (lo + hi) >> 1;
+                    if (Cs[diag - 1 - mid] >= Ls[mid]) lo = mid + 1;
+                    else hi = mid;
+                }
+                ia = lo;
+                ib = diag - lo;
+            }
             bool l_ok = ia > 0 || has_l_prev, c_ok = ib > 0 || has_c_prev;
             u64 last_l = l_ok ? Ls[static_cast<int>(ia) - 1] : 0;
             u64 last_c = c_ok ? Cs[static_cast<int>(ib) - 1] : 0;
+            // The two heads stay in registers; only the side that advanced
+            // is read again.
+            u64 lh = ia < nLs ? Ls[ia] : 0, ch = ib < nCs ? Cs[ib] : 0;
 #pragma unroll
             for (int i = 0; i < ITEMS; ++i) {
                 v[i] = 0;
                 if (diag + i < len) {
-                    if (ib >= nCs || (ia < nLs && Ls[ia] <= Cs[ib])) {
-                        last_l = Ls[ia++];
+                    if (ib >= nCs || (ia < nLs && lh <= ch)) {
+                        last_l = lh;
                         l_ok = true;
+                        ++ia;
+                        lh = ia < nLs ? Ls[ia] : 0;
                     } else {
-                        const u64 c = Cs[ib++];
-                        const bool repeat = c_ok && c == last_c;
-                        if (!repeat) {
+                        const u64 c = ch;
+                        ++ib;
+                        ch = ib < nCs ? Cs[ib] : 0;
+                        if (!(c_ok && c == last_c)) {
                             ++unique_tally;
                             if (!(l_ok && c == last_l)) {
                                 keep |= 1u << i;

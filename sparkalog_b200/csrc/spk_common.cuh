@@ -38,6 +38,10 @@ __device__ __forceinline__ void cp_async_8(void* smem, const void* gmem) {
     const u32 s = static_cast<u32>(__cvta_generic_to_shared(smem));
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async_16(void* smem, const void* gmem) {
+    const u32 s = static_cast<u32>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_4(void* smem, const void* gmem) {
     const u32 s = static_cast<u32>(__cvta_generic_to_shared(smem));
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
