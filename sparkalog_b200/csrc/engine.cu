@@ -1976,6 +1976,7 @@ void sparkalog_store_destroy(sparkalog_store* st) {
     for (auto& kv : st->relations) {
         for (auto& l : kv.second.level) l.release(s);
         for (auto& d : kv.second.dir) d.release(s);
+        kv.second.bloom.release(s);
         kv.second.spare.release(s);
         kv.second.delta.release(s);
         kv.second.newt.release(s);
@@ -2661,7 +2662,7 @@ int sparkalog_store_drop(sparkalog_store* st, u32 id) {
     RelState& r = it->second;
     for (auto& l : r.level) l.release(s);
     for (auto& d : r.dir) d.release(s);
-    for (DevArray* d : {&r.spare, &r.delta, &r.newt, &r.member, &r.member_flag}) d->release(s);
+    for (DevArray* d : {&r.spare, &r.delta, &r.newt, &r.member, &r.member_flag, &r.bloom}) d->release(s);
     st->relations.erase(it);
     return 0;
 }
