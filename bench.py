@@ -312,7 +312,7 @@ def run_ours(args):
 
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     from sparkalog_b200 import generators
     from sparkalog_b200.recursion import DELTA, FULL, RecursiveExecutor, RelationStore, transitive_closure_scc
