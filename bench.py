@@ -125,6 +125,8 @@ def parse_args():
                    help="run warmup + steps fixpoints and print a summary (for profilers; no JSON contract line)")
     p.add_argument("--nodes", type=int, default=None, help="override the workload's node count (profiling)")
     p.add_argument("--edges", type=int, default=None, help="override the workload's edge count (profiling)")
+    p.add_argument("--pool-gb", type=int, default=None,
+                   help="device pool reserved before warm-up, in GB (profiling: keeps a capture's device memory small)")
     return p.parse_args()
 
 
@@ -324,7 +326,8 @@ def run_ours(args):
     src, dst = generators.er_edges(nodes, edges, seed)
     ps, pd = partition(src, dst, nodes, rank, world)
     stream = torch.cuda.current_stream()
-    pool_gb = grow_device_pool(min(48 << 30, max(2 << 30, 1600 * edges)))
+    pool_bytes = min(48 << 30, max(2 << 30, 1600 * edges)) if args.pool_gb is None else args.pool_gb << 30
+    pool_gb = grow_device_pool(pool_bytes)
     dev = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).cuda()
     e0, e1, s0, s1 = dev(src), dev(dst), dev(ps), dev(pd)
     path, edge = RelationId(1), RelationId(0)

@@ -418,6 +418,8 @@ typedef struct sparkalog_tuning {
     uint32_t merge_anti_ratio;    /* the merge-form anti-join runs while FULL rows <= ratio x the round's
                                      estimated candidates; 0: never (0-1024) */
     uint32_t sparse_items;        /* candidates per thread of the per-thread search: 2, 3 or 4 */
+    uint32_t compact_index;       /* 1: the fused join probes 4-bit match counts and one word per key
+                                     instead of CSR offsets; 0: offsets */
 } sparkalog_tuning;
 
 /* The built-in defaults (measured on a B200). */

@@ -130,6 +130,7 @@ class TuningC(ctypes.Structure):
         ("bloom_bits", ctypes.c_uint32),
         ("merge_anti_ratio", ctypes.c_uint32),
         ("sparse_items", ctypes.c_uint32),
+        ("compact_index", ctypes.c_uint32),
     ]
 
     def as_dict(self) -> dict:

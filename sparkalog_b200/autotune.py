@@ -54,6 +54,7 @@ SPACE: dict[str, list[int]] = {
     "bloom_bits": [0, 8, 12, 16],
     "merge_anti_ratio": [0, 2, 4, 8, 16],
     "sparse_items": [2, 3, 4],
+    "compact_index": [1, 0],
 }
 
 

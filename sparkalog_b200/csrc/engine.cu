@@ -211,6 +211,7 @@ sparkalog_tuning default_tuning() {
     t.bloom_bits = 0;
     t.merge_anti_ratio = 0;
     t.sparse_items = 3;
+    t.compact_index = 1;
     return t;
 }
 
@@ -220,7 +221,7 @@ bool tuning_valid(const sparkalog_tuning& t) {
            (t.merge_items == 7 || t.merge_items == 11 || t.merge_items == 15) && t.level_ratio >= 2 && t.level_ratio <= 64 && t.levels >= 2 &&
            t.levels <= static_cast<u32>(spk::kMaxLevels) && t.group_candidates <= t.sparse_candidates &&
            (t.bloom_bits == 0 || (t.bloom_bits >= 4 && t.bloom_bits <= 32)) && t.merge_anti_ratio <= 1024 &&
-           t.sparse_items >= 2 && t.sparse_items <= 4;
+           t.sparse_items >= 2 && t.sparse_items <= 4 && t.compact_index <= 1;
 }
 
 // A stream-ordered device allocation that only grows.
@@ -655,6 +656,12 @@ struct IndexCache {
     u32 column = 0;
     DevArray offsets;   // u32[num_keys + 1] (dense index)
     u32* values_ptr = nullptr;  // u32[n] inside `offsets`: the second column in row order (identity)
+    // Compact form of an identity dense index (tuning.compact_index): 4-bit
+    // match counts, eight keys to a word, then a word per key (its single
+    // match, else its first offset), both inside `compact`.
+    DevArray compact;
+    u32* key_class = nullptr;
+    u32* key_word = nullptr;
     DevArray rows;      // u32[n] (empty when identity)
     bool identity = true;
     u64 num_keys = 0;
@@ -1010,6 +1017,7 @@ int build_index(sparkalog_executor* ex, sparkalog_store* st, IndexCache& ic, u32
 
 int build_index_impl(sparkalog_executor* ex, sparkalog_store* st, IndexCache& ic, u32 relation, u32 column) {
     cudaStream_t s = st->stream;
+    ic.key_class = ic.key_word = nullptr;
     RelState* r = st->find(relation);
     if (!r) return fail(SPARKALOG_E_MISSING, "relation " + std::to_string(relation) + " is not registered");
     if (r->recursive) {
@@ -1089,6 +1097,16 @@ int build_index_impl(sparkalog_executor* ex, sparkalog_store* st, IndexCache& ic
         if (ic.identity) {
             spk::low_words_kernel<<<simple_grid(n), 256, 0, s>>>(rows, n, ic.values_ptr);
             SPK_CUDA(cudaGetLastError(), "low_words_kernel");
+            ex->stats.total_launches += 1;
+        }
+        if (ic.identity && ex->tuning.compact_index) {
+            const u64 class_bytes = spk::align_up((ic.num_keys + 7) / 8 * 4, 256);
+            SPK_CUDA(ic.compact.ensure(class_bytes + ic.num_keys * 4, s), "cudaMallocAsync");
+            ic.key_class = ic.compact.as<u32>();
+            ic.key_word = reinterpret_cast<u32*>(static_cast<char*>(ic.compact.ptr) + class_bytes);
+            spk::compact_index_kernel<<<simple_grid(ic.num_keys), 256, 0, s>>>(ic.offsets.as<u32>(), ic.values_ptr,
+                                                                              ic.num_keys, ic.key_class, ic.key_word);
+            SPK_CUDA(cudaGetLastError(), "compact_index_kernel");
             ex->stats.total_launches += 1;
         }
     } else {
@@ -1443,6 +1461,8 @@ int run_device_loop(sparkalog_executor* ex, sparkalog_store* st, size_t ti, u64 
     a.v1_col = p.proj_col[1];
     a.right_values = (ic.identity && !ic.bucketed && a.v1_side == 1 && a.v1_col == 1 && ic.num_keys)
                          ? ic.values_ptr : nullptr;
+    a.key_class = (a.right_values && ex->tuning.compact_index) ? ic.key_class : nullptr;
+    a.key_word = a.key_class ? ic.key_word : nullptr;
     a.v1_bits = static_cast<u32>(32 - __builtin_clz(st->max_value | 1));
     a.out = t.j_a.as<u64>();
     a.out_count = counts + 1;
@@ -2781,7 +2801,7 @@ int sparkalog_store_join(sparkalog_store* st, u32 left_id, u32 right_id, u32 lef
         rc = read_count(st, ops, ops.counts.as<u64>() + 3, &m);
         if (rc) return rc;
     }
-    for (DevArray* d : {&ic.offsets, &ic.rows, &ic.keys32, &ic.bucket_dir}) d->release(s);
+    for (DevArray* d : {&ic.offsets, &ic.rows, &ic.keys32, &ic.bucket_dir, &ic.compact}) d->release(s);
     return store_sorted_unique(st, m, out_id, rows);
 }
 
@@ -3081,6 +3101,7 @@ void sparkalog_executor_destroy(sparkalog_executor* ex) {
         ic.rows.release(s);
         ic.keys32.release(s);
         ic.bucket_dir.release(s);
+        ic.compact.release(s);
     }
     ex->seg_seen.release(s);
     ex->seg_new.release(s);
@@ -3546,6 +3567,8 @@ static int run_rounds(sparkalog_executor* ex, sparkalog_store* st, size_t max_it
                     a.v1_col = p.proj_col[1];
                     a.right_values = (ic.identity && !ic.bucketed && a.v1_side == 1 && a.v1_col == 1 && ic.num_keys)
                                          ? ic.values_ptr : nullptr;
+                    a.key_class = (a.right_values && ex->tuning.compact_index) ? ic.key_class : nullptr;
+                    a.key_word = a.key_class ? ic.key_word : nullptr;
                     a.v1_bits = static_cast<u32>(32 - __builtin_clz(st->max_value | 1));
                     a.out = t.j_a.as<u64>();
                     a.out_count = jn;

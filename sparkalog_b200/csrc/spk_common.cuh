@@ -256,6 +256,62 @@ __device__ __forceinline__ u64 warp_lookback_resolve(u64* status, u64 tile, u64 
     return exclusive;
 }
 
+// Look-back that does not wait: walks from *base (the closest predecessor not
+// yet summed, adding into *exclusive) while the predecessors' words are
+// published. Returns true, with the tile's inclusive prefix published, once
+// it reaches an inclusive word; returns false at the first unpublished word,
+// with the walk's state left in *base and *exclusive for a later call. Called
+// by all 32 lanes of one warp with identical state; tile 0 starts at base -1.
+__device__ __forceinline__ bool warp_lookback_try(u64* status, u64 tile, u64 aggregate, u32 epoch, long long* base,
+                                                  u64* exclusive) {
+    const u32 lane = lane_id();
+    for (;;) {
+        const long long t = *base - static_cast<long long>(lane);
+        u64 w = 0;
+        bool ready = true;
+        u64 flag = kFlagInclusive;  // before tile 0: a zero inclusive prefix
+        if (t >= 0) {
+            w = ld_volatile(status + t);
+            const u32 e = static_cast<u32>(w >> 40) & kEpochMask;
+            flag = (w >> kValueBits) & 3;
+            ready = (e == (epoch & kEpochMask)) && flag != 0;
+        }
+        const u32 incl = __ballot_sync(0xffffffffu, ready && flag == kFlagInclusive);
+        const u32 not_ready = __ballot_sync(0xffffffffu, !ready);
+        const u32 first_incl = incl ? (__ffs(incl) - 1) : 32;
+        const u32 first_wait = not_ready ? (__ffs(not_ready) - 1) : 32;
+        const bool blocked = first_wait < first_incl;
+        const u32 take = blocked ? first_wait : (first_incl < 32 ? first_incl + 1 : 32);
+        u64 v = (lane < take && t >= 0) ? (w & kValueMask) : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        *exclusive += v;
+        if (blocked) {
+            *base -= static_cast<long long>(first_wait);
+            return false;
+        }
+        if (first_incl < 32) {
+            if (lane == 0) st_volatile(status + tile, make_status(epoch, kFlagInclusive, *exclusive + aggregate));
+            return true;
+        }
+        *base -= 32;
+    }
+}
+
+// Completes a walk that warp_lookback_try left unfinished, waiting for the
+// predecessors still unpublished (capped; kErrLookbackTimeout past the cap).
+__device__ __forceinline__ void warp_lookback_finish(u64* status, u64 tile, u64 aggregate, u32 epoch, long long* base,
+                                                     u64* exclusive, u32* err) {
+    u32 spins = 0;
+    while (!warp_lookback_try(status, tile, aggregate, epoch, base, exclusive)) {
+        if (++spins > kSpinCap) {
+            if (lane_id() == 0) atomicOr(err, kErrLookbackTimeout);
+            return;
+        }
+        if (spins > 64) __nanosleep(64);
+    }
+}
+
 // Warp-cooperative look-back for a single channel (used by compaction
 // kernels): publish and resolve back to back. Must be called by all 32 lanes
 // of one warp; every lane gets the result.

@@ -250,7 +250,10 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_sparse_kernel(const 
                                                                           u32* err, unsigned long long* unique_count) {
     constexpr int kTile = THREADS * ITEMS;
     __shared__ CompactShared<THREADS> cs;
-    __shared__ u64 stage[kTile];
+    __shared__ u64 stage[2][kTile];
+    __shared__ long long walk_base;
+    __shared__ u64 walk_excl;
+    __shared__ int walk_done;
     const u64* keys = (final_sel && *final_sel) ? buf_b : buf_a;
     const u64 n = *n_ptr;
     const u64 num_tiles = (n + kTile - 1) / kTile;
@@ -259,6 +262,15 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_sparse_kernel(const 
         return;
     }
     u32 unique_tally = 0;
+    // A tile whose look-back met an unpublished predecessor waits in the
+    // other stage buffer, with its walk's state, while the CTA searches its
+    // next tile; it is finished (and written) after that tile's search.
+    bool pending = false;
+    u64 p_tile = 0;
+    u32 p_total = 0;
+    long long p_base = 0;
+    u64 p_excl = 0;
+    int cur = 0;
     for (;;) {
         if (threadIdx.x == 0) cs.tile = atomicAdd(tile_counter, 1u);
         __syncthreads();
@@ -324,16 +336,59 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_sparse_kernel(const 
                 }
             }
         }
-        u32 excl, total;
-        const u64 off = compact_offsets<THREADS>(__popc(keep), &excl, &total, tile, status, epoch, err, cs);
+        u32 total;
+        const u32 excl = block_exclusive_scan<THREADS>(static_cast<u32>(__popc(keep)), cs.scan_scratch, &total);
+        if (threadIdx.x == 0) lookback_publish(status, tile, total, epoch);
         u32 wpos = excl;
 #pragma unroll
         for (int i = 0; i < ITEMS; ++i)
-            if (keep & (1u << i)) stage[wpos++] = v[i];
+            if (keep & (1u << i)) stage[cur][wpos++] = v[i];
+        if (pending) {
+            // The waiting tile's predecessors had this tile's search to publish.
+            if (warp_id() == 0) {
+                warp_lookback_finish(status, p_tile, p_total, epoch, &p_base, &p_excl, err);
+                if (lane_id() == 0) cs.tile_offset = p_excl;
+            }
+            __syncthreads();
+            const u64 off = cs.tile_offset;
+            for (u32 j = threadIdx.x; j < p_total; j += THREADS) out[off + j] = stage[cur ^ 1][j];
+            if (p_tile == num_tiles - 1 && threadIdx.x == 0) *out_count = off + p_total;
+            pending = false;
+        }
+        if (warp_id() == 0) {
+            long long wb = static_cast<long long>(tile) - 1;
+            u64 we = 0;
+            const bool done = warp_lookback_try(status, tile, total, epoch, &wb, &we);
+            if (lane_id() == 0) {
+                walk_done = done ? 1 : 0;
+                walk_base = wb;
+                walk_excl = we;
+            }
+        }
         __syncthreads();
-        for (u32 j = threadIdx.x; j < total; j += THREADS) out[off + j] = stage[j];
-        if (tile == num_tiles - 1 && threadIdx.x == 0) *out_count = off + total;
+        if (walk_done) {
+            const u64 off = walk_excl;
+            for (u32 j = threadIdx.x; j < total; j += THREADS) out[off + j] = stage[cur][j];
+            if (tile == num_tiles - 1 && threadIdx.x == 0) *out_count = off + total;
+        } else {
+            pending = true;
+            p_tile = tile;
+            p_total = total;
+            p_base = walk_base;
+            p_excl = walk_excl;
+            cur ^= 1;
+        }
         __syncthreads();
+    }
+    if (pending) {
+        if (warp_id() == 0) {
+            warp_lookback_finish(status, p_tile, p_total, epoch, &p_base, &p_excl, err);
+            if (lane_id() == 0) cs.tile_offset = p_excl;
+        }
+        __syncthreads();
+        const u64 off = cs.tile_offset;
+        for (u32 j = threadIdx.x; j < p_total; j += THREADS) out[off + j] = stage[cur ^ 1][j];
+        if (p_tile == num_tiles - 1 && threadIdx.x == 0) *out_count = off + p_total;
     }
     flush_unique(unique_tally, unique_count);
 }
@@ -964,6 +1019,35 @@ static __global__ void dense_offsets_kernel(const u64* sorted, u64 n, u64 num_ke
         for (u64 k = threadIdx.x; k <= num_keys; k += blockDim.x) offsets[k] = 0;
     }
     atomicMax(max_degree, local_max);
+}
+
+// Compact form of a dense identity index, for joins that gather the right
+// relation's second column: per key a 4-bit match count (15 stands for
+// fifteen or more; the offsets then give the count), eight keys to a word,
+// and one 32-bit word per key that holds the key's single match when it has
+// one, else its first offset into `values`. A probe of a key without matches
+// reads only its count word (0.5 bytes per key: the count array stays in L2),
+// a key with one match one more word, and only keys with two or more matches
+// read `values`. Launched with blockDim a multiple of 32: each warp covers 32
+// consecutive keys, so groups of eight lanes pack one count word.
+static __global__ void compact_index_kernel(const u32* offsets, const u32* values, u64 num_keys, u32* key_class,
+                                            u32* key_word) {
+    const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+    const u32 lane = lane_id();
+    for (u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; i - lane < num_keys; i += stride) {
+        u32 nib = 0;
+        if (i < num_keys) {
+            const u32 lo = offsets[i], hi = offsets[i + 1];
+            const u32 deg = hi - lo;
+            nib = deg < 15u ? deg : 15u;
+            key_word[i] = deg == 1 ? values[lo] : lo;
+        }
+        u32 v = nib << ((lane & 7) * 4);
+        v |= __shfl_xor_sync(0xffffffffu, v, 1);
+        v |= __shfl_xor_sync(0xffffffffu, v, 2);
+        v |= __shfl_xor_sync(0xffffffffu, v, 4);
+        if ((lane & 7) == 0 && i < num_keys) key_class[i >> 3] = v;
+    }
 }
 
 }  // namespace spk

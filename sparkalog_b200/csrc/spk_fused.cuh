@@ -47,6 +47,12 @@ struct FusedRoundArgs {
     // projecting that column): the gathers read 4-byte values from an array
     // half the size of the rows, which L2 holds more of.
     const u32* right_values;
+    // Compact form of that index (with right_values): 4-bit match counts,
+    // eight keys to a word (15: read the offsets), and a word per key holding
+    // its single match, else its first offset into right_values. Keys without
+    // matches then cost a probe of the count words only, which L2 holds.
+    const u32* key_class;
+    const u32* key_word;
     u32 v1_side;              // 0: DELTA column, 1: right column
     u32 v1_col;
     u32 v1_bits;              // significant bits of the second output column
@@ -187,6 +193,10 @@ __device__ __forceinline__ int fused_sort_shifts(u32 v1_bits, u32 runs, int* shi
 // Runs with at most this many output rows are placed by rank.
 constexpr u32 kRankRun = 48;
 
+// DELTA rows a tile's window reaches past its nominal end, so that the x
+// boundary that ends the tile is usually found in shared memory.
+constexpr u64 kWindowExtra = 128;
+
 // Packed per-thread scan value: match count in the low kCountBits, x-run
 // starts above (a tile has fewer than 2048 rows, so starts fit in 11 bits).
 constexpr int kCountBits = 52;
@@ -231,18 +241,40 @@ __device__ __forceinline__ void fused_round(const FusedRoundArgs& a) {
         if (tile >= num_tiles) break;
 
         // 1. Rows [B(tile), B(tile + 1)): the first x boundary at or after each
-        // nominal start (warp 0: begin, warp 1: end), scanning <= ROWCAP rows.
+        // nominal start. The window [p0 - 1, p1 + extra) of DELTA rows comes
+        // into shared memory first (keys_b is free until the emitted keys are
+        // ordered) and both boundaries are found there (warp 0: begin, warp 1:
+        // end); only an x-run that reaches past the window sends a warp on to
+        // scan global memory, up to ROWCAP rows.
+        const u64 p0 = tile * R;
+        const u64 p1 = p0 + R < n ? p0 + R : n;
+        const u64 w0 = p0 > 0 ? p0 - 1 : 0;
+        const u64 extra = R + 1 + kWindowExtra <= static_cast<u64>(CAP) ? kWindowExtra
+                          : static_cast<u64>(CAP) > R + 1 ? CAP - 1 - R : 0;
+        const u64 w1 = p1 + extra < n ? p1 + extra : n;
+        u64* win = keys_b;
+        for (u32 r = threadIdx.x; r < w1 - w0; r += THREADS) cp_async_8(win + r, a.delta + w0 + r);
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncthreads();
         if (warp_id() < 2) {
-            const u64 p0 = (tile + warp_id()) * R;
+            const u64 p = warp_id() == 0 ? p0 : p1;
             u64 found = ~0ull;
-            if (p0 == 0) {
+            if (p == 0) {
                 found = 0;
-            } else if (p0 >= n) {
+            } else if (p >= n) {
                 found = n;
             } else {
-                for (u64 base = p0; base < p0 + ROWCAP && found == ~0ull; base += kWarp) {
-                    const u64 p = base + lane_id();
-                    const bool boundary = p >= n || (a.delta[p] >> 32) != (a.delta[p - 1] >> 32);
+                // p - 1 >= w0, so every row compared here lies in the window.
+                for (u64 base = p; base <= w1 && found == ~0ull; base += kWarp) {
+                    const u64 q = base + lane_id();
+                    const bool boundary = q < w1 ? (win[q - w0] >> 32) != (win[q - 1 - w0] >> 32) : (q == w1 && w1 == n);
+                    const u32 m = __ballot_sync(0xffffffffu, boundary);
+                    if (m) found = base + (__ffs(m) - 1);
+                }
+                for (u64 base = w1; base < p + ROWCAP && found == ~0ull; base += kWarp) {
+                    const u64 q = base + lane_id();
+                    const bool boundary = q >= n || (a.delta[q] >> 32) != (a.delta[q - 1] >> 32);
                     const u32 m = __ballot_sync(0xffffffffu, boundary);
                     if (m) found = base + (__ffs(m) - 1);
                 }
@@ -255,16 +287,42 @@ __device__ __forceinline__ void fused_round(const FusedRoundArgs& a) {
         const bool rows_ok = row0 != ~0ull && row1 != ~0ull && row1 - row0 <= static_cast<u64>(ROWCAP);
         const u32 nrows = rows_ok ? static_cast<u32>(row1 - row0) : 0u;
 
-        // 2. The tile's DELTA rows into shared memory (keys_b is free until
-        // the emitted keys are ordered), then every row's index range,
-        // gathered with asynchronous copies (each thread issues all of its
-        // gathers, then waits once).
-        u64* trow = keys_b;
-        for (u32 r = threadIdx.x; r < nrows; r += THREADS) cp_async_8(trow + r, a.delta + row0 + r);
-        cp_async_commit();
-        cp_async_wait<0>();
-        __syncthreads();
-        if (a.dense_offsets) {
+        // 2. The tile's DELTA rows: in the window already unless an x-run
+        // reached past it (then reloaded into keys_b). Then every row's index
+        // range, gathered with asynchronous copies (each thread issues all of
+        // its gathers, then waits once).
+        u64* trow = rows_ok ? win + (row0 - w0) : win;
+        if (rows_ok && row1 > w1) {
+            trow = keys_b;
+            for (u32 r = threadIdx.x; r < nrows; r += THREADS) cp_async_8(trow + r, a.delta + row0 + r);
+            cp_async_commit();
+            cp_async_wait<0>();
+            __syncthreads();
+        }
+        if (a.key_class) {
+            // Each thread probes its own rows (the ones it scans below): the
+            // counts first, then the words of the keys that have matches,
+            // still in flight during the scan.
+            const u32 r0 = threadIdx.x * kRowItems;
+            u32 key[kRowItems], cls[kRowItems];
+#pragma unroll
+            for (int i = 0; i < kRowItems; ++i) {
+                const u32 r = r0 + i;
+                key[i] = r < nrows ? pair_col(trow[r], a.left_key) : 0u;
+                cls[i] = (r < nrows && key[i] < a.dense_keys) ? __ldg(a.key_class + (key[i] >> 3)) : 0u;
+            }
+#pragma unroll
+            for (int i = 0; i < kRowItems; ++i) {
+                const u32 r = r0 + i;
+                if (r < nrows) {
+                    u32 c = (cls[i] >> ((key[i] & 7u) * 4u)) & 15u;
+                    if (c == 15u) c = a.dense_offsets[key[i] + 1] - a.dense_offsets[key[i]];
+                    range_hi[r] = c;
+                    if (c) cp_async_4(range_lo + r, a.key_word + key[i]);
+                }
+            }
+            cp_async_commit();
+        } else if (a.dense_offsets) {
             for (u32 r = threadIdx.x; r < nrows; r += THREADS) {
                 const u32 key = pair_col(trow[r], a.left_key);
                 if (key < a.dense_keys) {
@@ -297,7 +355,7 @@ __device__ __forceinline__ void fused_round(const FusedRoundArgs& a) {
             const u32 r = local0 + i;
             if (r < nrows) {
                 const u64 start = (r == 0 || (trow[r] >> 32) != (trow[r - 1] >> 32)) ? 1u : 0u;
-                packed += (start << kCountBits) + (range_hi[r] - range_lo[r]);
+                packed += (start << kCountBits) + (a.key_class ? range_hi[r] : range_hi[r] - range_lo[r]);
             }
         }
         u64 packed_total;
@@ -307,6 +365,7 @@ __device__ __forceinline__ void fused_round(const FusedRoundArgs& a) {
         const bool ok = rows_ok && total64 <= static_cast<u64>(CAP);
         const u32 total = ok ? static_cast<u32>(total64) : 0u;
         u32* match_row = reinterpret_cast<u32*>(keys_a) + CAP;  // row ids of an indexed right relation
+        if (a.key_class) cp_async_wait<0>();  // this thread's key words
         if (ok) {
             u32 off = static_cast<u32>(packed_excl & kCountMask);
             u32 rk = static_cast<u32>(packed_excl >> kCountBits);
@@ -320,12 +379,14 @@ __device__ __forceinline__ void fused_round(const FusedRoundArgs& a) {
                         run_off[rk] = off;
                         ++rk;
                     }
-                    const u32 first = range_lo[r], count = range_hi[r] - first;
+                    const u32 first = range_lo[r];
+                    const u32 count = a.key_class ? range_hi[r] : range_hi[r] - first;
                     for (u32 k = 0; k < count; ++k) {
                         const u32 o = off + k;
                         rank[o] = static_cast<unsigned short>(rk - 1);
                         if (a.v1_side != 1) keys_a[o] = row;
                         else if (a.rows) cp_async_4(match_row + o, a.rows + first + k);
+                        else if (a.key_class && count == 1) match_row[o] = first;
                         else if (a.right_values) cp_async_4(match_row + o, a.right_values + first + k);
                         else cp_async_8(keys_a + o, a.right + first + k);
                     }

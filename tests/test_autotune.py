@@ -7,7 +7,7 @@ from sparkalog_b200 import autotune
 
 START = {"dir_rows_log2": 6, "group_lanes": 8, "group_candidates": 1 << 17, "sparse_candidates": 1 << 26,
          "fused_rows_cap": 672, "level_ratio": 4, "levels": 3, "merge_items": 11, "bloom_bits": 0,
-         "merge_anti_ratio": 0, "sparse_items": 3}
+         "merge_anti_ratio": 0, "sparse_items": 3, "compact_index": 1}
 
 
 def bowl(target):
@@ -20,7 +20,7 @@ def bowl(target):
 def test_descent_finds_the_minimum_of_a_separable_cost():
     target = {"dir_rows_log2": 2, "group_lanes": 4, "group_candidates": 1 << 19, "sparse_candidates": 1 << 24,
               "fused_rows_cap": 512, "level_ratio": 8, "levels": 4, "merge_items": 15, "bloom_bits": 12,
-              "merge_anti_ratio": 4, "sparse_items": 2}
+              "merge_anti_ratio": 4, "sparse_items": 2, "compact_index": 0}
     best, cost, trials = autotune.coordinate_descent(bowl(target), START)
     assert best == target
     assert cost == 1.0

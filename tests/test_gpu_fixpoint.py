@@ -248,6 +248,20 @@ def test_fused_join_distinct_falls_back_on_hub(cuda):
     assert stats["classes"]["join"]["launches"] > 0
 
 
+@pytest.mark.parametrize("fan", [150, 300, 700])
+def test_fused_join_distinct_x_runs_past_the_window(cuda, fan):
+    # Hubs whose x-runs in DELTA are longer than the rows a tile's window
+    # reaches past its nominal end but fit a tile: the tile boundary is found
+    # by the scan beyond the window and the rows are reloaded, exactly.
+    hubs = np.repeat(np.array([0, 9000, 20000], dtype=np.uint32), fan)
+    targets = np.concatenate([np.arange(1, fan + 1), np.arange(9001, 9001 + fan),
+                              np.arange(20001, 20001 + fan)]).astype(np.uint32)
+    er0, er1 = generators.er_edges(30000, 24000, 29)
+    e0, e1 = oracle.btree_pairs(np.concatenate([hubs, er0]), np.concatenate([targets, er1]))
+    stats = _tc_with_stats(e0, e1)
+    assert stats["classes"]["join_distinct"]["launches"] > 0
+
+
 def test_fused_join_distinct_join_on_first_column(cuda):
     # p(x, y) :- p(x, z), e(x, y): the join key is DELTA's first column.
     from sparkalog_b200.relational import BinaryEqualityJoin, JoinInput, JoinProjection, RecursiveRulePlan
@@ -435,6 +449,7 @@ TUNINGS = [
     {"bloom_bits": 4, "levels": 4, "group_candidates": 1 << 12},
     {"merge_anti_ratio": 0, "sparse_items": 2, "levels": 4, "group_candidates": 1 << 10},
     {"sparse_items": 3, "group_candidates": 1 << 10},
+    {"compact_index": 0},
     {"merge_anti_ratio": 1024, "levels": 4, "level_ratio": 2},
     {"merge_anti_ratio": 1024, "levels": 2, "group_candidates": 1 << 10, "sparse_candidates": 1 << 12},
 ]
