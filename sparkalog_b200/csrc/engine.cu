@@ -210,7 +210,7 @@ sparkalog_tuning default_tuning() {
     t.levels = 3;
     t.bloom_bits = 0;
     t.merge_anti_ratio = 0;
-    t.sparse_items = 3;
+    t.sparse_items = 2;
     t.compact_index = 1;
     return t;
 }

@@ -249,11 +249,7 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_sparse_kernel(const 
                                                                           u64* status, u32* tile_counter, u32 epoch,
                                                                           u32* err, unsigned long long* unique_count) {
     constexpr int kTile = THREADS * ITEMS;
-    __shared__ CompactShared<THREADS> cs;
-    __shared__ u64 stage[2][kTile];
-    __shared__ long long walk_base;
-    __shared__ u64 walk_excl;
-    __shared__ int walk_done;
+    __shared__ DeferredShared<THREADS, kTile> ds;
     const u64* keys = (final_sel && *final_sel) ? buf_b : buf_a;
     const u64 n = *n_ptr;
     const u64 num_tiles = (n + kTile - 1) / kTile;
@@ -262,19 +258,13 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_sparse_kernel(const 
         return;
     }
     u32 unique_tally = 0;
-    // A tile whose look-back met an unpublished predecessor waits in the
-    // other stage buffer, with its walk's state, while the CTA searches its
-    // next tile; it is finished (and written) after that tile's search.
-    bool pending = false;
-    u64 p_tile = 0;
-    u32 p_total = 0;
-    long long p_base = 0;
-    u64 p_excl = 0;
-    int cur = 0;
+    // A tile whose look-back meets an unpublished predecessor waits while the
+    // CTA searches its next tile (deferred compaction).
+    DeferredState st;
     for (;;) {
-        if (threadIdx.x == 0) cs.tile = atomicAdd(tile_counter, 1u);
+        if (threadIdx.x == 0) ds.cs.tile = atomicAdd(tile_counter, 1u);
         __syncthreads();
-        const u64 tile = cs.tile;
+        const u64 tile = ds.cs.tile;
         if (tile >= num_tiles) break;
         const u64 base = tile * kTile + static_cast<u64>(threadIdx.x) * ITEMS;
         u64 v[ITEMS];
@@ -337,59 +327,14 @@ __global__ void __launch_bounds__(THREADS) anti_join_levels_sparse_kernel(const 
             }
         }
         u32 total;
-        const u32 excl = block_exclusive_scan<THREADS>(static_cast<u32>(__popc(keep)), cs.scan_scratch, &total);
-        if (threadIdx.x == 0) lookback_publish(status, tile, total, epoch);
-        u32 wpos = excl;
+        u32 wpos = deferred_scan<THREADS, kTile>(static_cast<u32>(__popc(keep)), &total, tile, status, epoch, ds);
 #pragma unroll
         for (int i = 0; i < ITEMS; ++i)
-            if (keep & (1u << i)) stage[cur][wpos++] = v[i];
-        if (pending) {
-            // The waiting tile's predecessors had this tile's search to publish.
-            if (warp_id() == 0) {
-                warp_lookback_finish(status, p_tile, p_total, epoch, &p_base, &p_excl, err);
-                if (lane_id() == 0) cs.tile_offset = p_excl;
-            }
-            __syncthreads();
-            const u64 off = cs.tile_offset;
-            for (u32 j = threadIdx.x; j < p_total; j += THREADS) out[off + j] = stage[cur ^ 1][j];
-            if (p_tile == num_tiles - 1 && threadIdx.x == 0) *out_count = off + p_total;
-            pending = false;
-        }
-        if (warp_id() == 0) {
-            long long wb = static_cast<long long>(tile) - 1;
-            u64 we = 0;
-            const bool done = warp_lookback_try(status, tile, total, epoch, &wb, &we);
-            if (lane_id() == 0) {
-                walk_done = done ? 1 : 0;
-                walk_base = wb;
-                walk_excl = we;
-            }
-        }
-        __syncthreads();
-        if (walk_done) {
-            const u64 off = walk_excl;
-            for (u32 j = threadIdx.x; j < total; j += THREADS) out[off + j] = stage[cur][j];
-            if (tile == num_tiles - 1 && threadIdx.x == 0) *out_count = off + total;
-        } else {
-            pending = true;
-            p_tile = tile;
-            p_total = total;
-            p_base = walk_base;
-            p_excl = walk_excl;
-            cur ^= 1;
-        }
-        __syncthreads();
+            if (keep & (1u << i)) ds.stage[st.cur][wpos++] = v[i];
+        deferred_flush<THREADS, kTile>(st, num_tiles, status, epoch, err, out, out_count, ds);
+        deferred_try<THREADS, kTile>(st, tile, total, num_tiles, status, epoch, out, out_count, ds);
     }
-    if (pending) {
-        if (warp_id() == 0) {
-            warp_lookback_finish(status, p_tile, p_total, epoch, &p_base, &p_excl, err);
-            if (lane_id() == 0) cs.tile_offset = p_excl;
-        }
-        __syncthreads();
-        const u64 off = cs.tile_offset;
-        for (u32 j = threadIdx.x; j < p_total; j += THREADS) out[off + j] = stage[cur ^ 1][j];
-        if (p_tile == num_tiles - 1 && threadIdx.x == 0) *out_count = off + p_total;
-    }
+    deferred_flush<THREADS, kTile>(st, num_tiles, status, epoch, err, out, out_count, ds);
     flush_unique(unique_tally, unique_count);
 }
 
@@ -410,8 +355,7 @@ __device__ __forceinline__ void anti_join_group(const u64* buf_a, const u64* buf
     // Each step shrinks a window of S > G rows to at most S / (G + 1) + 1;
     // 64 steps cover any u32 row range.
     constexpr int kMaxSteps = 64;
-    __shared__ CompactShared<THREADS> cs;
-    __shared__ u64 stage[kTile];
+    __shared__ DeferredShared<THREADS, kTile> ds;
     const u64* keys = (final_sel && *final_sel) ? buf_b : buf_a;
     const u64 n = *n_ptr;
     const u64 num_tiles = (n + kTile - 1) / kTile;
@@ -422,10 +366,11 @@ __device__ __forceinline__ void anti_join_group(const u64* buf_a, const u64* buf
     const u32 lane = threadIdx.x % G;
     const u32 group_mask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << (lane_id() / G * G);
     u32 unique_tally = 0;
+    DeferredState st;
     for (;;) {
-        if (threadIdx.x == 0) cs.tile = atomicAdd(tile_counter, 1u);
+        if (threadIdx.x == 0) ds.cs.tile = atomicAdd(tile_counter, 1u);
         __syncthreads();
-        const u64 tile = cs.tile;
+        const u64 tile = ds.cs.tile;
         if (tile >= num_tiles) break;
         const u64 idx = tile * kTile + threadIdx.x / G;
         u64 v = 0;
@@ -480,15 +425,13 @@ __device__ __forceinline__ void anti_join_group(const u64* buf_a, const u64* buf
             if (lane < hi[l] - lo[l] && levels.keys[l][lo[l] + lane] == v) found = true;
         found = (__ballot_sync(0xffffffffu, found) & group_mask) != 0;
         keep = keep && !found;
-        u32 excl, total;
-        const u64 off =
-            compact_offsets<THREADS>(lane == 0 && keep ? 1u : 0u, &excl, &total, tile, status, epoch, err, cs);
-        if (lane == 0 && keep) stage[excl] = v;
-        __syncthreads();
-        for (u32 j = threadIdx.x; j < total; j += THREADS) out[off + j] = stage[j];
-        if (tile == num_tiles - 1 && threadIdx.x == 0) *out_count = off + total;
-        __syncthreads();
+        u32 total;
+        const u32 excl = deferred_scan<THREADS, kTile>(lane == 0 && keep ? 1u : 0u, &total, tile, status, epoch, ds);
+        if (lane == 0 && keep) ds.stage[st.cur][excl] = v;
+        deferred_flush<THREADS, kTile>(st, num_tiles, status, epoch, err, out, out_count, ds);
+        deferred_try<THREADS, kTile>(st, tile, total, num_tiles, status, epoch, out, out_count, ds);
     }
+    deferred_flush<THREADS, kTile>(st, num_tiles, status, epoch, err, out, out_count, ds);
     flush_unique(unique_tally, unique_count);
 }
 

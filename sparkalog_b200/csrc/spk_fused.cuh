@@ -105,9 +105,13 @@ struct FusedLayout {
     static constexpr size_t kRunX = kRangeHi + ROWCAP * sizeof(u32);           // u32[ROWCAP]
     static constexpr size_t kRunOff = kRunX + ROWCAP * sizeof(u32);            // u32[ROWCAP + 4]
     static constexpr size_t kRank = kRunOff + (ROWCAP + 4) * sizeof(u32);      // u16[CAP]
-    static constexpr size_t kWarpCount = kRank + CAP * sizeof(unsigned short); // u16[kWarps][256]
-    static constexpr size_t kDigitStart = kWarpCount + kWarps * 256 * sizeof(unsigned short);
-    static constexpr size_t kBytes = kDigitStart + 256 * sizeof(u32);
+    // The radix sort's counters reuse the index ranges' bytes: the ranges are
+    // dead once the matches are emitted, before any sort.
+    static constexpr size_t kWarpCount = kRangeLo;                              // u16[kWarps][256]
+    static constexpr size_t kDigitStart = kWarpCount + kWarps * 256 * sizeof(unsigned short);  // u32[256]
+    static_assert(kWarps * 256 * sizeof(unsigned short) + 256 * sizeof(u32) <= 2 * ROWCAP * sizeof(u32),
+                  "sort counters fit the index ranges");
+    static constexpr size_t kBytes = kRank + CAP * sizeof(unsigned short);
 };
 
 // Stable LSD radix sort of n <= CAP keys in shared memory over the 8-bit

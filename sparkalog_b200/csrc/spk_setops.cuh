@@ -118,6 +118,91 @@ __device__ __forceinline__ u64 compact_offsets(u32 thread_count, u32* thread_exc
     return cs.tile_offset;
 }
 
+// Ordered compaction whose tiles do not wait on slow predecessors. A tile
+// publishes its kept count, stages its kept rows, and tries its look-back
+// without waiting; if a predecessor has not published yet, the tile stays in
+// the other stage buffer, with its walk's state, while the CTA works on its
+// next tile, and is finished and written after that tile's rows are staged.
+// A CTA publishes its current tile's count before it waits on its waiting
+// tile, so every wait ends: a claimed tile's count never depends on a wait.
+template <int THREADS, int TILE>
+struct DeferredShared {
+    CompactShared<THREADS> cs;
+    u64 stage[2][TILE];
+    long long walk_base;
+    u64 walk_excl;
+    int walk_done;
+};
+
+struct DeferredState {
+    bool pending = false;
+    u64 tile = 0;
+    u32 total = 0;
+    long long base = 0;
+    u64 excl = 0;
+    int cur = 0;
+};
+
+// Block scan of the per-thread keep counts; publishes the tile's count and
+// returns the thread's offset within the tile (rows go to stage[st.cur]).
+template <int THREADS, int TILE>
+__device__ __forceinline__ u32 deferred_scan(u32 thread_count, u32* tile_total, u64 tile, u64* status, u32 epoch,
+                                             DeferredShared<THREADS, TILE>& ds) {
+    const u32 excl = block_exclusive_scan<THREADS>(thread_count, ds.cs.scan_scratch, tile_total);
+    if (threadIdx.x == 0) lookback_publish(status, tile, *tile_total, epoch);
+    return excl;
+}
+
+// Finishes and writes the waiting tile, if any. All threads.
+template <int THREADS, int TILE>
+__device__ __forceinline__ void deferred_flush(DeferredState& st, u64 num_tiles, u64* status, u32 epoch, u32* err,
+                                               u64* out, u64* out_count, DeferredShared<THREADS, TILE>& ds) {
+    if (!st.pending) return;
+    if (warp_id() == 0) {
+        warp_lookback_finish(status, st.tile, st.total, epoch, &st.base, &st.excl, err);
+        if (lane_id() == 0) ds.cs.tile_offset = st.excl;
+    }
+    __syncthreads();
+    const u64 off = ds.cs.tile_offset;
+    const u64* rows = ds.stage[st.cur ^ 1];
+    for (u32 j = threadIdx.x; j < st.total; j += THREADS) out[off + j] = rows[j];
+    if (st.tile == num_tiles - 1 && threadIdx.x == 0) *out_count = off + st.total;
+    st.pending = false;
+}
+
+// Tries the current tile's look-back once: writes it now, or leaves it
+// waiting. Call after deferred_flush; ends with a barrier. All threads.
+template <int THREADS, int TILE>
+__device__ __forceinline__ void deferred_try(DeferredState& st, u64 tile, u32 total, u64 num_tiles, u64* status,
+                                             u32 epoch, u64* out, u64* out_count,
+                                             DeferredShared<THREADS, TILE>& ds) {
+    if (warp_id() == 0) {
+        long long base = static_cast<long long>(tile) - 1;
+        u64 excl = 0;
+        const bool done = warp_lookback_try(status, tile, total, epoch, &base, &excl);
+        if (lane_id() == 0) {
+            ds.walk_done = done ? 1 : 0;
+            ds.walk_base = base;
+            ds.walk_excl = excl;
+        }
+    }
+    __syncthreads();
+    if (ds.walk_done) {
+        const u64 off = ds.walk_excl;
+        const u64* rows = ds.stage[st.cur];
+        for (u32 j = threadIdx.x; j < total; j += THREADS) out[off + j] = rows[j];
+        if (tile == num_tiles - 1 && threadIdx.x == 0) *out_count = off + total;
+    } else {
+        st.pending = true;
+        st.tile = tile;
+        st.total = total;
+        st.base = ds.walk_base;
+        st.excl = ds.walk_excl;
+        st.cur ^= 1;
+    }
+    __syncthreads();
+}
+
 // ---------------------------------------------------------------------------
 // Unique + unpack of sorted packed keys (the end of distinct).
 // ---------------------------------------------------------------------------
