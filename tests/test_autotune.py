@@ -60,3 +60,18 @@ def test_library_defaults_are_inside_the_search_space():
     d = autotune.defaults()
     assert set(autotune.SPACE) <= set(d)
     assert autotune.valid(d)
+
+
+def test_shipped_tunings_are_points_of_the_search_space():
+    from sparkalog_b200 import _native
+
+    fields = {name for name, _ in _native.TuningC._fields_}
+    shipped = sorted(autotune.SHIPPED_DIR.glob("*.json"))
+    assert shipped
+    for path in shipped:
+        t = json.loads(path.read_text())["tuning"]
+        assert set(t) <= fields, path.name
+        merged = {**autotune.defaults(), **t}
+        assert autotune.valid(merged), path.name
+        for name, values in autotune.SPACE.items():
+            assert merged[name] in values, (path.name, name, merged[name])
